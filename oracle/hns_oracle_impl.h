@@ -1,0 +1,474 @@
+/* Precision-generic body of the CPU oracle (test infrastructure only).
+ *
+ * Included twice by hns_oracle.c, with R = float / S = _f32 and R = double / S = _f64.
+ * Each function restates one reference kernel; the citation is on the function. The
+ * arithmetic follows the reference's operation order so that the float build matches the
+ * reference to rounding; the double build is the FP64 oracle the error statements use.
+ */
+#define CAT2(a, b) a##b
+#define CAT(a, b) CAT2(a, b)
+#define FN(name) CAT(name, S)
+
+/* Nearest read, 0 outside the domain: IndexSampler<T,0> (src/Utils/Stencils.hpp:74-93). */
+static inline R FN(near_s)(const hnso_topo* t, const R* d, int32_t i, int32_t j, int32_t k) {
+    const uint64_t off = hnso_offset(t, i, j, k);
+    return off == 0 ? (R)0 : d[off - 1];
+}
+
+static inline void FN(near_v)(const hnso_topo* t, const R* d, int32_t i, int32_t j, int32_t k, R v[3]) {
+    const uint64_t off = hnso_offset(t, i, j, k);
+    if (off == 0) {
+        v[0] = v[1] = v[2] = (R)0;
+    } else {
+        v[0] = d[3 * (off - 1)];
+        v[1] = d[3 * (off - 1) + 1];
+        v[2] = d[3 * (off - 1) + 2];
+    }
+}
+
+static inline R FN(lerp)(R a, R b, R w) { return a + w * (b - a); }
+
+/* Trilinear sample: floor, fractional part, then lerp along z, y, x
+ * (TrilinearSampler::sample, src/Utils/Stencils.hpp:118-153). */
+static R FN(tri_s)(const hnso_topo* t, const R* d, R x, R y, R z) {
+    const int32_t i = (int32_t)floor(x), j = (int32_t)floor(y), k = (int32_t)floor(z);
+    const R tx = x - (R)i, ty = y - (R)j, tz = z - (R)k;
+    const R v000 = FN(near_s)(t, d, i, j, k), v001 = FN(near_s)(t, d, i, j, k + 1);
+    const R v010 = FN(near_s)(t, d, i, j + 1, k), v011 = FN(near_s)(t, d, i, j + 1, k + 1);
+    const R v100 = FN(near_s)(t, d, i + 1, j, k), v101 = FN(near_s)(t, d, i + 1, j, k + 1);
+    const R v110 = FN(near_s)(t, d, i + 1, j + 1, k), v111 = FN(near_s)(t, d, i + 1, j + 1, k + 1);
+    const R z0 = FN(lerp)(v000, v001, tz), z1 = FN(lerp)(v010, v011, tz);
+    const R z2 = FN(lerp)(v100, v101, tz), z3 = FN(lerp)(v110, v111, tz);
+    const R y0 = FN(lerp)(z0, z1, ty), y1 = FN(lerp)(z2, z3, ty);
+    return FN(lerp)(y0, y1, tx);
+}
+
+static void FN(tri_v)(const hnso_topo* t, const R* d, R x, R y, R z, R out[3]) {
+    const int32_t i = (int32_t)floor(x), j = (int32_t)floor(y), k = (int32_t)floor(z);
+    const R tx = x - (R)i, ty = y - (R)j, tz = z - (R)k;
+    R v[2][2][2][3];
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) FN(near_v)(t, d, i + a, j + b, k + c, v[a][b][c]);
+    for (int q = 0; q < 3; ++q) {
+        const R z0 = FN(lerp)(v[0][0][0][q], v[0][0][1][q], tz), z1 = FN(lerp)(v[0][1][0][q], v[0][1][1][q], tz);
+        const R z2 = FN(lerp)(v[1][0][0][q], v[1][0][1][q], tz), z3 = FN(lerp)(v[1][1][0][q], v[1][1][1][q], tz);
+        const R y0 = FN(lerp)(z0, z1, ty), y1 = FN(lerp)(z2, z3, ty);
+        out[q] = FN(lerp)(y0, y1, tx);
+    }
+}
+
+void FN(hnso_sample_trilinear_scalar)(const hnso_topo* t, const R* data, const R* xyz, int64_t n, R* out) {
+    for (int64_t q = 0; q < n; ++q) out[q] = FN(tri_s)(t, data, xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]);
+}
+
+void FN(hnso_sample_trilinear_vec3)(const hnso_topo* t, const R* data, const R* xyz, int64_t n, R* out) {
+    for (int64_t q = 0; q < n; ++q) FN(tri_v)(t, data, xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2], out + 3 * q);
+}
+
+static inline void FN(coord_of)(const hnso_topo* t, int64_t slot, int32_t* i, int32_t* j, int32_t* k) {
+    const int32_t* o = hnso_leaf_origin(t, slot >> 9);
+    const int32_t n = (int32_t)(slot & 511);
+    *i = o[0] + ((n >> 6) & 7);
+    *j = o[1] + ((n >> 3) & 7);
+    *k = o[2] + (n & 7);
+}
+
+static inline R FN(fmin_)(R a, R b) { return a < b ? a : (b < a ? b : (a != a ? b : a)); }
+static inline R FN(fmax_)(R a, R b) { return a > b ? a : (b > a ? b : (a != a ? b : a)); }
+
+/* advect_vector (src/Cuda/Kernel.cu:349-426), no collision: MacCormack back/forward trace
+ * with trilinear velocity, clamped to [min,max] of centre, 6 face neighbours and the
+ * forward sample. */
+void FN(hnso_advect_vector)(const hnso_topo* t, const R* vel, R* out, R dt, R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R sdt = dt * inv_dx;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        R vo[3], vf[3], vb[3], back[3], fwd[3], corr[3], mn[3], mx[3];
+        FN(near_v)(t, vel, i, j, k, vo);
+        back[0] = (R)i - vo[0] * sdt;
+        back[1] = (R)j - vo[1] * sdt;
+        back[2] = (R)k - vo[2] * sdt;
+        FN(tri_v)(t, vel, back[0], back[1], back[2], vf);
+        for (int q = 0; q < 3; ++q) fwd[q] = back[q] + vf[q] * sdt;
+        FN(tri_v)(t, vel, fwd[0], fwd[1], fwd[2], vb);
+        for (int q = 0; q < 3; ++q) {
+            corr[q] = vf[q] + (R)0.5 * (vo[q] - vb[q]);
+            mn[q] = mx[q] = vo[q];
+        }
+        for (int dim = 0; dim < 3; ++dim) {
+            for (int off = -1; off <= 1; off += 2) {
+                R vn[3];
+                FN(near_v)(t, vel, i + (dim == 0 ? off : 0), j + (dim == 1 ? off : 0), k + (dim == 2 ? off : 0), vn);
+                for (int q = 0; q < 3; ++q) {
+                    mn[q] = FN(fmin_)(mn[q], vn[q]);
+                    mx[q] = FN(fmax_)(mx[q], vn[q]);
+                }
+            }
+        }
+        for (int q = 0; q < 3; ++q) {
+            mn[q] = FN(fmin_)(mn[q], vf[q]);
+            mx[q] = FN(fmax_)(mx[q], vf[q]);
+            out[3 * s + q] = FN(fmax_)(mn[q], FN(fmin_)(corr[q], mx[q]));
+        }
+    }
+}
+
+/* Index of a tap for advect_scalars: offset 0 (outside the domain) reads array index 0,
+ * i.e. slot 0's value, not zero (src/Cuda/Kernel.cu:229-230, 256-257). */
+static inline int64_t FN(tap)(const hnso_topo* t, int32_t i, int32_t j, int32_t k) {
+    const uint64_t off = hnso_offset(t, i, j, k);
+    return off == 0 ? 0 : (int64_t)(off - 1);
+}
+
+static void FN(interp_setup)(const hnso_topo* t, R x, R y, R z, int64_t idx[8], R w[8]) {
+    const int32_t i0 = (int32_t)floor(x), j0 = (int32_t)floor(y), k0 = (int32_t)floor(z);
+    const int32_t i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+    const R tx = x - (R)i0, ty = y - (R)j0, tz = z - (R)k0;
+    const R itx = (R)1 - tx, ity = (R)1 - ty, itz = (R)1 - tz;
+    const R w00 = itx * ity, w10 = tx * ity, w01 = itx * ty, w11 = tx * ty;
+    w[0] = w00 * itz;
+    w[1] = w10 * itz;
+    w[2] = w01 * itz;
+    w[3] = w11 * itz;
+    w[4] = w00 * tz;
+    w[5] = w10 * tz;
+    w[6] = w01 * tz;
+    w[7] = w11 * tz;
+    idx[0] = FN(tap)(t, i0, j0, k0);
+    idx[1] = FN(tap)(t, i1, j0, k0);
+    idx[2] = FN(tap)(t, i0, j1, k0);
+    idx[3] = FN(tap)(t, i1, j1, k0);
+    idx[4] = FN(tap)(t, i0, j0, k1);
+    idx[5] = FN(tap)(t, i1, j0, k1);
+    idx[6] = FN(tap)(t, i0, j1, k1);
+    idx[7] = FN(tap)(t, i1, j1, k1);
+}
+
+/* advect_scalars (src/Cuda/Kernel.cu:163-289), no collision: the back-trace uses the
+ * voxel's own velocity, the re-trace the weight-sum trilinear velocity; per field a
+ * fused-multiply-add weight sum, MacCormack correction and 7+1 point clamp. */
+void FN(hnso_advect_scalars)(const hnso_topo* t, const R* vel, const R* const* in, R* const* out, int nfields, R dt,
+                             R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R sdt = dt * inv_dx;
+    static const int offs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const int64_t orig = FN(tap)(t, i, j, k);
+        const R* vc = vel + 3 * orig;
+        const R back[3] = {(R)i - vc[0] * sdt, (R)j - vc[1] * sdt, (R)k - vc[2] * sdt};
+        int64_t bi[8], fi[8], nb[6];
+        R bw[8], fw[8];
+        FN(interp_setup)(t, back[0], back[1], back[2], bi, bw);
+        R vf[3] = {0, 0, 0};
+        for (int q = 0; q < 8; ++q)
+            for (int c = 0; c < 3; ++c) vf[c] = vf[c] + vel[3 * bi[q] + c] * bw[q];
+        const R fwd[3] = {back[0] + vf[0] * sdt, back[1] + vf[1] * sdt, back[2] + vf[2] * sdt};
+        FN(interp_setup)(t, fwd[0], fwd[1], fwd[2], fi, fw);
+        for (int q = 0; q < 6; ++q) nb[q] = FN(tap)(t, i + offs[q][0], j + offs[q][1], k + offs[q][2]);
+        for (int f = 0; f < nfields; ++f) {
+            const R* d = in[f];
+            const R po = d[orig];
+            R pf = 0, pb = 0;
+            for (int q = 0; q < 8; ++q) {
+                pf = FMA(d[bi[q]], bw[q], pf);
+                pb = FMA(d[fi[q]], fw[q], pb);
+            }
+            const R corr = FMA((R)0.5, po - pb, pf);
+            R mn = po, mx = po;
+            for (int q = 0; q < 6; ++q) {
+                mn = FN(fmin_)(mn, d[nb[q]]);
+                mx = FN(fmax_)(mx, d[nb[q]]);
+            }
+            mn = FN(fmin_)(mn, pf);
+            mx = FN(fmax_)(mx, pf);
+            out[f][s] = FN(fmax_)(mn, FN(fmin_)(corr, mx));
+        }
+    }
+}
+
+/* advect_scalar (src/Cuda/Kernel.cu:294-344), the HNanoAdvect kernel: samplers read 0
+ * outside the domain; lerp-chain trilinear for the field and the velocity. */
+void FN(hnso_advect_scalar)(const hnso_topo* t, const R* vel, const R* in, R* out, R dt, R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R sdt = dt * inv_dx;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const R po = FN(near_s)(t, in, i, j, k);
+        R vc[3], vf[3];
+        FN(near_v)(t, vel, i, j, k, vc);
+        const R back[3] = {(R)i - vc[0] * sdt, (R)j - vc[1] * sdt, (R)k - vc[2] * sdt};
+        const R pf = FN(tri_s)(t, in, back[0], back[1], back[2]);
+        FN(tri_v)(t, vel, back[0], back[1], back[2], vf);
+        const R fwd[3] = {back[0] + vf[0] * sdt, back[1] + vf[1] * sdt, back[2] + vf[2] * sdt};
+        const R pb = FN(tri_s)(t, in, fwd[0], fwd[1], fwd[2]);
+        const R corr = pf + (R)0.5 * (po - pb);
+        R mn = po, mx = po;
+        for (int dim = 0; dim < 3; ++dim) {
+            for (int off = -1; off <= 1; off += 2) {
+                const R v = FN(near_s)(t, in, i + (dim == 0 ? off : 0), j + (dim == 1 ? off : 0), k + (dim == 2 ? off : 0));
+                mn = FN(fmin_)(mn, v);
+                mx = FN(fmax_)(mx, v);
+            }
+        }
+        mn = FN(fmin_)(mn, pf);
+        mx = FN(fmax_)(mx, pf);
+        out[s] = FN(fmax_)(mn, FN(fmin_)(corr, mx));
+    }
+}
+
+/* divergence (src/Cuda/Kernel.cu:432-453): central difference written through face
+ * averages, velocity 0 outside the domain. */
+void FN(hnso_divergence)(const hnso_topo* t, const R* vel, R* div, R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const R* c = vel + 3 * s;
+        R n[3];
+        FN(near_v)(t, vel, i + 1, j, k, n);
+        const R xp = (c[0] + n[0]) * (R)0.5;
+        FN(near_v)(t, vel, i - 1, j, k, n);
+        const R xm = (c[0] + n[0]) * (R)0.5;
+        FN(near_v)(t, vel, i, j + 1, k, n);
+        const R yp = (c[1] + n[1]) * (R)0.5;
+        FN(near_v)(t, vel, i, j - 1, k, n);
+        const R ym = (c[1] + n[1]) * (R)0.5;
+        FN(near_v)(t, vel, i, j, k + 1, n);
+        const R zp = (c[2] + n[2]) * (R)0.5;
+        FN(near_v)(t, vel, i, j, k - 1, n);
+        const R zm = (c[2] + n[2]) * (R)0.5;
+        div[s] = (xp - xm + yp - ym + zp - zm) * inv_dx;
+    }
+}
+
+/* One colour of redBlackGaussSeidelUpdate (src/Cuda/Kernel.cu:459-489): colour
+ * (i+j+k)&1, pressure 0 outside the domain with a fixed 1/6 (Dirichlet-0 walls). */
+void FN(hnso_rbgs_sweep)(const hnso_topo* t, const R* div, R* p, R dx, int color, R omega) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R dx2 = dx * dx;
+    const R inv6 = (R)INV6;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        if (((i + j + k) & 1) != color) continue;
+        const R sum = FN(near_s)(t, p, i + 1, j, k) + FN(near_s)(t, p, i - 1, j, k) + FN(near_s)(t, p, i, j + 1, k) +
+                      FN(near_s)(t, p, i, j - 1, k) + FN(near_s)(t, p, i, j, k + 1) + FN(near_s)(t, p, i, j, k - 1);
+        const R pgs = (sum - div[s] * dx2) * inv6;
+        const R pold = p[s];
+        p[s] = pold + omega * (pgs - pold);
+    }
+}
+
+/* The pressure loop of HNS_Advance (src/Cuda/HNanoSolver.cu:366-373): iterations x
+ * (colour 0, colour 1). */
+void FN(hnso_rbgs)(const hnso_topo* t, const R* div, R* p, R dx, int iterations, R omega) {
+    for (int it = 0; it < iterations; ++it) {
+        FN(hnso_rbgs_sweep)(t, div, p, dx, 0, omega);
+        FN(hnso_rbgs_sweep)(t, div, p, dx, 1, omega);
+    }
+}
+
+/* Poisson residual of the system the sweeps relax, accumulated in double:
+ * r = div*dx^2 - (sum of 6 neighbours - 6 p), with p = 0 outside. Returns sum r^2 and
+ * sum (div*dx^2)^2. */
+void FN(hnso_residual)(const hnso_topo* t, const R* div, const R* p, R dx, double* r2, double* b2) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const double h2 = (double)dx * (double)dx;
+    double sr = 0.0, sb = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : sr, sb)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const double lap = (double)FN(near_s)(t, p, i + 1, j, k) + (double)FN(near_s)(t, p, i - 1, j, k) +
+                           (double)FN(near_s)(t, p, i, j + 1, k) + (double)FN(near_s)(t, p, i, j - 1, k) +
+                           (double)FN(near_s)(t, p, i, j, k + 1) + (double)FN(near_s)(t, p, i, j, k - 1) -
+                           6.0 * (double)p[s];
+        const double b = (double)div[s] * h2;
+        sr += (b - lap) * (b - lap);
+        sb += b * b;
+    }
+    *r2 = sr;
+    *b2 = sb;
+}
+
+/* subtractPressureGradient (src/Cuda/Kernel.cu:495-541), no collision: u = u* - grad p,
+ * central differences, p = 0 outside. */
+void FN(hnso_subtract_gradient)(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R h = (R)0.5 * inv_dx;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const R gx = (FN(near_s)(t, p, i + 1, j, k) - FN(near_s)(t, p, i - 1, j, k)) * h;
+        const R gy = (FN(near_s)(t, p, i, j + 1, k) - FN(near_s)(t, p, i, j - 1, k)) * h;
+        const R gz = (FN(near_s)(t, p, i, j, k + 1) - FN(near_s)(t, p, i, j, k - 1)) * h;
+        out[3 * s] = vel[3 * s] - gx;
+        out[3 * s + 1] = vel[3 * s + 1] - gy;
+        out[3 * s + 2] = vel[3 * s + 2] - gz;
+    }
+}
+
+/* computeVorticityMag (src/Cuda/Utils.cuh:226-243): |curl u| at a voxel. */
+static R FN(vort_mag)(const hnso_topo* t, const R* vel, int32_t i, int32_t j, int32_t k, R factor) {
+    R px[3], mx[3], py[3], my[3], pz[3], mz[3];
+    FN(near_v)(t, vel, i + 1, j, k, px);
+    FN(near_v)(t, vel, i - 1, j, k, mx);
+    FN(near_v)(t, vel, i, j + 1, k, py);
+    FN(near_v)(t, vel, i, j - 1, k, my);
+    FN(near_v)(t, vel, i, j, k + 1, pz);
+    FN(near_v)(t, vel, i, j, k - 1, mz);
+    const R ox = ((py[2] - my[2]) - (pz[1] - mz[1])) * factor;
+    const R oy = ((pz[0] - mz[0]) - (px[2] - mx[2])) * factor;
+    const R oz = ((px[1] - mx[1]) - (py[0] - my[0])) * factor;
+    return SQRT(ox * ox + oy * oy + oz * oz);
+}
+
+/* vorticityConfinement (src/Cuda/Kernel.cu:682-727), out of place. The |omega| gradient is
+ * taken at offsets of int(factor_scale) voxels: the reference builds a Coord from the float
+ * (Kernel.cu:707-712), which truncates toward zero, so 0.5 gives a zero force. */
+void FN(hnso_vorticity_confinement)(const hnso_topo* t, const R* vel, R* out, R dt, R inv_dx, R scale, R factor_scale) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R factor = (R)0.5 * inv_dx;
+    const int32_t fs = (int32_t)factor_scale;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        R px[3], mx[3], py[3], my[3], pz[3], mz[3];
+        FN(near_v)(t, vel, i + 1, j, k, px);
+        FN(near_v)(t, vel, i - 1, j, k, mx);
+        FN(near_v)(t, vel, i, j + 1, k, py);
+        FN(near_v)(t, vel, i, j - 1, k, my);
+        FN(near_v)(t, vel, i, j, k + 1, pz);
+        FN(near_v)(t, vel, i, j, k - 1, mz);
+        const R ox = ((py[2] - my[2]) - (pz[1] - mz[1])) * factor;
+        const R oy = ((pz[0] - mz[0]) - (px[2] - mx[2])) * factor;
+        const R oz = ((px[1] - mx[1]) - (py[0] - my[0])) * factor;
+        const R mpx = FN(vort_mag)(t, vel, i + fs, j, k, factor), mmx = FN(vort_mag)(t, vel, i - fs, j, k, factor);
+        const R mpy = FN(vort_mag)(t, vel, i, j + fs, k, factor), mmy = FN(vort_mag)(t, vel, i, j - fs, k, factor);
+        const R mpz = FN(vort_mag)(t, vel, i, j, k + fs, factor), mmz = FN(vort_mag)(t, vel, i, j, k - fs, factor);
+        const R gx = (mpx - mmx) * (R)0.5 * inv_dx;
+        const R gy = (mpy - mmy) * (R)0.5 * inv_dx;
+        const R gz = (mpz - mmz) * (R)0.5 * inv_dx;
+        const R glen = SQRT(gx * gx + gy * gy + gz * gz) + (R)1e-5f;
+        const R nx = gx / glen, ny = gy / glen, nz = gz / glen;
+        const R fx = scale * (ny * oz - nz * oy), fy = scale * (nz * ox - nx * oz), fz = scale * (nx * oy - ny * ox);
+        out[3 * s] = vel[3 * s] + fx * dt;
+        out[3 * s + 1] = vel[3 * s + 1] + fy * dt;
+        out[3 * s + 2] = vel[3 * s + 2] + fz * dt;
+    }
+}
+
+/* temperature_buoyancy (src/Cuda/Kernel.cu:546-563): v.y += max(0,(T-Tamb)*beta)*dt where
+ * T > Tamb; otherwise the velocity passes through. */
+void FN(hnso_temperature_buoyancy)(int64_t n, const R* vel, const R* temp, R* out, R dt, R ambient, R strength) {
+    for (int64_t s = 0; s < n; ++s) {
+        const R T = temp[s];
+        out[3 * s] = vel[3 * s];
+        out[3 * s + 2] = vel[3 * s + 2];
+        if (T <= ambient) {
+            out[3 * s + 1] = vel[3 * s + 1];
+        } else {
+            const R f = FN(fmax_)((R)0, (T - ambient) * strength);
+            out[3 * s] = vel[3 * s] + (R)0 * dt;
+            out[3 * s + 1] = vel[3 * s + 1] + f * dt;
+            out[3 * s + 2] = vel[3 * s + 2] + (R)0 * dt;
+        }
+    }
+}
+
+/* combustion (src/Cuda/Kernel.cu:568-588): burn min(fuel, rate*dt) where fuel > 0 and
+ * T >= ignition; heat release raises T. */
+void FN(hnso_combustion)(int64_t n, const R* fuel, const R* temp, R* out_fuel, R* out_temp, R dt, R ignition, R rate,
+                         R heat) {
+    for (int64_t s = 0; s < n; ++s) {
+        R f = fuel[s], T = temp[s];
+        if (f > (R)0 && T >= ignition) {
+            const R burned = FN(fmin_)(f, rate * dt);
+            f -= burned;
+            T += burned * heat;
+        }
+        out_fuel[s] = f;
+        out_temp[s] = T;
+    }
+}
+
+/* combustion_oxygen (src/Cuda/Kernel.cu:641-677): oxygen = 1 - fuel - waste, burn =
+ * min(oxygen, fuel); waste += 2 burn; flame = max(flame, min(1, 10 burn)); T += burn*gain;
+ * div += burn*expansion. Fuel below 1e-3 counts as 0. */
+void FN(hnso_combustion_oxygen)(int64_t n, const R* fuel, const R* waste, const R* temp, R* div, const R* flame,
+                                R* o_fuel, R* o_waste, R* o_temp, R* o_flame, R gain, R expansion) {
+    for (int64_t s = 0; s < n; ++s) {
+        R f = fuel[s];
+        const R w = waste[s], T = temp[s], fl = flame[s];
+        if (f < (R)0.001f) f = 0;
+        const R ox = (R)1 - f - w;
+        if (ox < (R)0) {
+            o_fuel[s] = f;
+            o_waste[s] = w;
+            o_temp[s] = T;
+            o_flame[s] = fl;
+            continue;
+        }
+        const R burn = FN(fmin_)(ox, f);
+        o_fuel[s] = f - burn;
+        o_waste[s] = w + burn * (R)2;
+        o_temp[s] = T + burn * gain;
+        div[s] += burn * expansion;
+        o_flame[s] = FN(fmax_)(fl, FN(fmin_)((R)1, burn * (R)10));
+    }
+}
+
+/* add_scalar_source / add_velocity_source(_xyz) / add_gravity
+ * (src/Cuda/Kernel.cu:732-755, 834-838). */
+void FN(hnso_add_scalar_source)(int64_t n, R* field, const R* src, R dt) {
+    for (int64_t s = 0; s < n; ++s) field[s] += dt * src[s];
+}
+
+void FN(hnso_add_velocity_source)(int64_t n, R* vel, const R* src, R dt) {
+    for (int64_t s = 0; s < 3 * n; ++s) vel[s] += src[s] * dt;
+}
+
+void FN(hnso_add_velocity_source_xyz)(int64_t n, R* vel, const R* sx, const R* sy, const R* sz, R dt) {
+    for (int64_t s = 0; s < n; ++s) {
+        vel[3 * s] += dt * sx[s];
+        vel[3 * s + 1] += dt * sy[s];
+        vel[3 * s + 2] += dt * sz[s];
+    }
+}
+
+void FN(hnso_add_gravity)(int64_t n, R* vel, R g, R dt) {
+    for (int64_t s = 0; s < n; ++s) vel[3 * s + 1] -= g * dt;
+}
+
+/* HNanoProjectNonDivergent (src/Cuda/PressureProjection.cu:9-78): divergence, p = 0,
+ * iterations x (red, black), gradient subtraction back into the velocity. omega < 0 selects
+ * that path's 2/(1+sin(3.14159*dx)) evaluated in double (PressureProjection.cu:53). */
+void FN(hnso_project)(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterations, R omega) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R inv_dx = (R)1 / dx;
+    if (omega < (R)0) omega = (R)(2.0f / (1.0f + sin(3.14159 * (double)dx)));
+    FN(hnso_divergence)(t, vel, div, inv_dx);
+    for (int64_t s = 0; s < N; ++s) p[s] = 0;
+    FN(hnso_rbgs)(t, div, p, dx, iterations, omega);
+    R* tmp = (R*)malloc(sizeof(R) * 3 * (size_t)N);
+    memcpy(tmp, vel, sizeof(R) * 3 * (size_t)N);
+    FN(hnso_subtract_gradient)(t, tmp, p, vel, inv_dx);
+    free(tmp);
+}
+
+#undef FN
+#undef CAT
+#undef CAT2
