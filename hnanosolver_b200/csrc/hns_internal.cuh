@@ -1,0 +1,174 @@
+// Internal declarations of libhns: the context, the device topology view and error
+// plumbing. Not installed; the public surface is include/hns.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "hns.h"
+
+namespace hns {
+
+// ---- errors --------------------------------------------------------------------------------
+
+struct Error : std::runtime_error {
+    hns_status status;
+    Error(hns_status s, const std::string& msg) : std::runtime_error(msg), status(s) {}
+};
+
+[[noreturn]] void fail(hns_status s, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what, const char* file, int line);
+#define HNS_CUDA(call) ::hns::cuda_check((call), #call, __FILE__, __LINE__)
+#define HNS_LAUNCHED() ::hns::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+
+hns_status record_error(hns_status s, const std::string& msg);
+void clear_error();
+
+// Runs `body` and turns any exception into a status (no exception crosses the C ABI).
+template <typename F>
+hns_status guarded(F&& body) {
+    try {
+        clear_error();
+        body();
+        return HNS_OK;
+    } catch (const Error& e) {
+        return record_error(e.status, e.what());
+    } catch (const std::bad_alloc&) {
+        return record_error(HNS_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return record_error(HNS_ERR_INVALID_ARG, e.what());
+    }
+}
+
+// ---- device memory -------------------------------------------------------------------------
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t n) { alloc(n); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr, o.bytes = 0; }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        if (this != &o) {
+            reset();
+            ptr = o.ptr, bytes = o.bytes;
+            o.ptr = nullptr, o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DeviceBuffer() { reset(); }
+    void alloc(size_t n);
+    void reset() noexcept;
+    template <typename T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+// ---- topology ------------------------------------------------------------------------------
+
+// Device view of the leaf table. A coordinate's leaf is found either through the 27-leaf
+// neighbourhood of the leaf being processed (staged in shared memory by the kernels) or
+// through `lookup`, a dense table over the leaves' bounding box in leaf units.
+struct TopoView {
+    int64_t num_leaves;
+    const int4* origin;   // [L] leaf origins (w unused)
+    const int* nbr27;     // [L][27] neighbour leaf indices, -1 = none; index (dx+1)*9+(dy+1)*3+(dz+1)
+    const int* lookup;    // dense leaf table, -1 = none
+    int lo_x, lo_y, lo_z; // table origin in leaf units (coordinate >> 3)
+    int dim_x, dim_y, dim_z;
+};
+
+struct Topology {
+    int64_t num_leaves = 0;
+    std::vector<int32_t> origins;  // host copy, 3 per leaf
+    DeviceBuffer d_origin, d_nbr27, d_lookup;
+    TopoView view{};
+    bool nanovdb_order = false;
+    void build(const int32_t* leaf_origins, int64_t n, cudaStream_t stream);
+};
+
+bool leaves_in_nanovdb_order(const int32_t* origins, int64_t n);
+void sort_leaves_nanovdb(int32_t* origins, int64_t n);
+
+// ---- context ------------------------------------------------------------------------------
+
+struct Context {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    float dx = 0.f;
+    Topology topo;
+    // Scratch owned by the context, grown on demand and reused across calls.
+    std::map<std::string, DeviceBuffer> scratch;
+    DeviceBuffer d_reduce;  // FP64 reduction accumulators
+
+    int64_t num_voxels() const { return topo.num_leaves * 512; }
+    float* scratch_f32(const std::string& name, size_t count);
+    double* reduce_slots(int count);
+};
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+};
+
+Context* check_ctx(hns_ctx* ctx);
+const Context* check_ctx(const hns_ctx* ctx);
+
+// ---- kernels (hns_kernels.cu) --------------------------------------------------------------
+
+constexpr int kMaxAdvectFields = 16;
+
+struct FieldSet {
+    const float* in[kMaxAdvectFields];
+    float* out[kMaxAdvectFields];
+    int count;
+};
+
+// Velocity (vel_out, may be null) and HNanoAdvect scalars (f) along one shared trace.
+void launch_advect_fused(const Context& c, const float* vel, float* vel_out, const FieldSet& f, float dt);
+void launch_advect_scalars(const Context& c, const float* vel, const FieldSet& f, float dt);
+void launch_divergence(const Context& c, const float* vel, float* div);
+// One fused red+black iteration: p_in -> p_out (ping-pong). p_in == nullptr means p = 0.
+// check/tol2: skip when check[0] <= tol2 * check[1]; resid_out: accumulate the residual of
+// p_in (FP64 {sum r^2, sum b^2}).
+void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in, float* p_out, float omega,
+                           unsigned flags, const double* check = nullptr, double tol2 = 0.0,
+                           double* resid_out = nullptr);
+void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out);
+void launch_vorticity(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale);
+// acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).
+void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags);
+void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint64_t* out);
+
+// Runs `iterations` fused RBGS iterations from `p` (or zero) and leaves the result in `p`.
+void rbgs_solve(Context& c, const float* div, float* p, int iterations, float omega, unsigned flags);
+
+// Convergence-checked solve: at most `max_iterations` (rounded up to even) iterations; the
+// FP64 residual of the iterate is evaluated inside the sweep every `check_every` iterations
+// and the remaining launches return at once when ||r|| <= tol ||b||. Enqueues only; the
+// check slots (2 doubles per check, from c.reduce_slots) are read by solve_result().
+struct SolvePlan {
+    int max_iterations = 0;
+    int check_every = 0;
+    int num_checks = 0;
+    double tol = 0.0;
+    double* slots = nullptr;
+};
+SolvePlan rbgs_solve_checked(Context& c, const float* div, float* p, int max_iterations, float omega, unsigned flags,
+                             double tol, int check_every);
+// Host readback (synchronizes): iterations run and the last evaluated relative residual.
+void solve_result(Context& c, const SolvePlan& plan, int* iterations, double* residual);
+
+}  // namespace hns
+
+struct hns_ctx {
+    hns::Context impl;
+};

@@ -1,0 +1,216 @@
+// Device-side helpers shared by the solver kernels: leaf lookup, slot addressing and the
+// samplers of the reference (src/Utils/Stencils.hpp) restated over the leaf table.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hns_internal.cuh"
+
+namespace hns {
+namespace dev {
+
+constexpr float kInv6 = 0.166666667f;  // the reference's constant (src/Cuda/Kernel.cu:475)
+
+__device__ __forceinline__ int local_offset(int i, int j, int k) { return ((i & 7) << 6) | ((j & 7) << 3) | (k & 7); }
+
+// Leaf index of the voxel (i,j,k) through the dense leaf table, -1 outside the domain.
+__device__ __forceinline__ int leaf_from_table(const TopoView& t, int i, int j, int k) {
+    const int a = (i >> 3) - t.lo_x, b = (j >> 3) - t.lo_y, c = (k >> 3) - t.lo_z;
+    if ((unsigned)a >= (unsigned)t.dim_x || (unsigned)b >= (unsigned)t.dim_y || (unsigned)c >= (unsigned)t.dim_z) return -1;
+    return __ldg(t.lookup + ((int64_t)a * t.dim_y + b) * t.dim_z + c);
+}
+
+// The 27-leaf neighbourhood of the leaf a CTA works on, staged in shared memory.
+struct LeafNbhd {
+    int nb[27];
+    int lx, ly, lz;  // leaf coordinates (origin >> 3)
+};
+
+__device__ __forceinline__ void load_nbhd(LeafNbhd& L, const TopoView& t, int64_t leaf) {
+    if (threadIdx.x < 27) L.nb[threadIdx.x] = __ldg(t.nbr27 + leaf * 27 + threadIdx.x);
+    if (threadIdx.x == 27) {
+        const int4 o = t.origin[leaf];
+        L.lx = o.x >> 3;
+        L.ly = o.y >> 3;
+        L.lz = o.z >> 3;
+    }
+}
+
+__device__ __forceinline__ int leaf_of(const TopoView& t, const LeafNbhd& L, int i, int j, int k) {
+    const int a = (i >> 3) - L.lx + 1, b = (j >> 3) - L.ly + 1, c = (k >> 3) - L.lz + 1;
+    if ((unsigned)a < 3u && (unsigned)b < 3u && (unsigned)c < 3u) return L.nb[a * 9 + b * 3 + c];
+    return leaf_from_table(t, i, j, k);
+}
+
+// Slot of voxel (i,j,k), -1 outside the domain.
+__device__ __forceinline__ int64_t slot_of(const TopoView& t, const LeafNbhd& L, int i, int j, int k) {
+    const int l = leaf_of(t, L, i, j, k);
+    return l < 0 ? -1 : ((int64_t)l << 9) + local_offset(i, j, k);
+}
+
+__device__ __forceinline__ float3 ld3(const float* __restrict__ v, int64_t s) {
+    return make_float3(__ldg(v + 3 * s), __ldg(v + 3 * s + 1), __ldg(v + 3 * s + 2));
+}
+
+__device__ __forceinline__ void st3(float* __restrict__ v, int64_t s, float3 a) {
+    v[3 * s] = a.x;
+    v[3 * s + 1] = a.y;
+    v[3 * s + 2] = a.z;
+}
+
+// Nearest reads, 0 outside the domain (IndexSampler<T,0>, src/Utils/Stencils.hpp:74-93).
+__device__ __forceinline__ float near_s(const TopoView& t, const LeafNbhd& L, const float* __restrict__ d, int i, int j, int k) {
+    const int64_t s = slot_of(t, L, i, j, k);
+    return s < 0 ? 0.f : __ldg(d + s);
+}
+
+__device__ __forceinline__ float3 near_v(const TopoView& t, const LeafNbhd& L, const float* __restrict__ d, int i, int j, int k) {
+    const int64_t s = slot_of(t, L, i, j, k);
+    return s < 0 ? make_float3(0.f, 0.f, 0.f) : ld3(d, s);
+}
+
+__device__ __forceinline__ float lerp1(float a, float b, float w) { return fmaf(w, b - a, a); }
+
+// Trilinear sample, 0 outside the domain: floor, fractional part, lerp along z, then y,
+// then x (TrilinearSampler::sample, src/Utils/Stencils.hpp:118-153).
+__device__ __forceinline__ float tri_s(const TopoView& t, const LeafNbhd& L, const float* __restrict__ d, float x, float y, float z) {
+    const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
+    const float tx = x - (float)i, ty = y - (float)j, tz = z - (float)k;
+    const float v000 = near_s(t, L, d, i, j, k), v001 = near_s(t, L, d, i, j, k + 1);
+    const float v010 = near_s(t, L, d, i, j + 1, k), v011 = near_s(t, L, d, i, j + 1, k + 1);
+    const float v100 = near_s(t, L, d, i + 1, j, k), v101 = near_s(t, L, d, i + 1, j, k + 1);
+    const float v110 = near_s(t, L, d, i + 1, j + 1, k), v111 = near_s(t, L, d, i + 1, j + 1, k + 1);
+    const float z0 = lerp1(v000, v001, tz), z1 = lerp1(v010, v011, tz);
+    const float z2 = lerp1(v100, v101, tz), z3 = lerp1(v110, v111, tz);
+    return lerp1(lerp1(z0, z1, ty), lerp1(z2, z3, ty), tx);
+}
+
+__device__ __forceinline__ float3 tri_v(const TopoView& t, const LeafNbhd& L, const float* __restrict__ d, float x, float y, float z) {
+    const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
+    const float tx = x - (float)i, ty = y - (float)j, tz = z - (float)k;
+    const float3 v000 = near_v(t, L, d, i, j, k), v001 = near_v(t, L, d, i, j, k + 1);
+    const float3 v010 = near_v(t, L, d, i, j + 1, k), v011 = near_v(t, L, d, i, j + 1, k + 1);
+    const float3 v100 = near_v(t, L, d, i + 1, j, k), v101 = near_v(t, L, d, i + 1, j, k + 1);
+    const float3 v110 = near_v(t, L, d, i + 1, j + 1, k), v111 = near_v(t, L, d, i + 1, j + 1, k + 1);
+    float3 r;
+#define HNS_TRI_COMP(c)                                                                   \
+    {                                                                                     \
+        const float z0 = lerp1(v000.c, v001.c, tz), z1 = lerp1(v010.c, v011.c, tz);       \
+        const float z2 = lerp1(v100.c, v101.c, tz), z3 = lerp1(v110.c, v111.c, tz);       \
+        r.c = lerp1(lerp1(z0, z1, ty), lerp1(z2, z3, ty), tx);                            \
+    }
+    HNS_TRI_COMP(x)
+    HNS_TRI_COMP(y)
+    HNS_TRI_COMP(z)
+#undef HNS_TRI_COMP
+    return r;
+}
+
+// The eight taps of a trilinear sample at (x,y,z): slots (-1 outside the domain) of the
+// corners v[a][b][c] = (i+a, j+b, k+c) and the fractional position. Computing them once
+// lets several fields be sampled at the same point with shared addressing.
+struct Taps {
+    int64_t s[8];  // index a*4 + b*2 + c
+    float tx, ty, tz;
+};
+
+__device__ __forceinline__ void taps_at(Taps& T, const TopoView& t, const LeafNbhd& L, float x, float y, float z) {
+    const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
+    T.tx = x - (float)i;
+    T.ty = y - (float)j;
+    T.tz = z - (float)k;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) T.s[q] = slot_of(t, L, i + (q >> 2), j + ((q >> 1) & 1), k + (q & 1));
+}
+
+__device__ __forceinline__ float tap_s(const float* __restrict__ d, int64_t s) { return s < 0 ? 0.f : __ldg(d + s); }
+
+__device__ __forceinline__ float3 tap_v(const float* __restrict__ d, int64_t s) {
+    return s < 0 ? make_float3(0.f, 0.f, 0.f) : ld3(d, s);
+}
+
+// Lerp along z, then y, then x of the staged corners (TrilinearSampler::sample order).
+__device__ __forceinline__ float tri_lerp(const Taps& T, const float v[8]) {
+    const float z0 = lerp1(v[0], v[1], T.tz), z1 = lerp1(v[2], v[3], T.tz);
+    const float z2 = lerp1(v[4], v[5], T.tz), z3 = lerp1(v[6], v[7], T.tz);
+    return lerp1(lerp1(z0, z1, T.ty), lerp1(z2, z3, T.ty), T.tx);
+}
+
+__device__ __forceinline__ float tri_s(const Taps& T, const float* __restrict__ d) {
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = tap_s(d, T.s[q]);
+    return tri_lerp(T, v);
+}
+
+__device__ __forceinline__ float3 tri_v(const Taps& T, const float* __restrict__ d) {
+    float x[8], y[8], z[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const float3 a = tap_v(d, T.s[q]);
+        x[q] = a.x, y[q] = a.y, z[q] = a.z;
+    }
+    return make_float3(tri_lerp(T, x), tri_lerp(T, y), tri_lerp(T, z));
+}
+
+// Slot for the multi-field advection's taps: out-of-domain reads slot 0
+// (src/Cuda/Kernel.cu:229-230, 256-257).
+__device__ __forceinline__ int64_t tap_slot(const TopoView& t, const LeafNbhd& L, int i, int j, int k) {
+    const int64_t s = slot_of(t, L, i, j, k);
+    return s < 0 ? 0 : s;
+}
+
+// Eight taps and weights of the multi-field advection's weight-sum trilinear
+// (setupInterpolation, src/Cuda/Kernel.cu:204-233).
+__device__ __forceinline__ void interp_setup(const TopoView& t, const LeafNbhd& L, float x, float y, float z, int64_t idx[8], float w[8]) {
+    const int i0 = __float2int_rd(x), j0 = __float2int_rd(y), k0 = __float2int_rd(z);
+    const int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+    const float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+    const float itx = 1.0f - tx, ity = 1.0f - ty, itz = 1.0f - tz;
+    const float w00 = itx * ity, w10 = tx * ity, w01 = itx * ty, w11 = tx * ty;
+    w[0] = w00 * itz;
+    w[1] = w10 * itz;
+    w[2] = w01 * itz;
+    w[3] = w11 * itz;
+    w[4] = w00 * tz;
+    w[5] = w10 * tz;
+    w[6] = w01 * tz;
+    w[7] = w11 * tz;
+    idx[0] = tap_slot(t, L, i0, j0, k0);
+    idx[1] = tap_slot(t, L, i1, j0, k0);
+    idx[2] = tap_slot(t, L, i0, j1, k0);
+    idx[3] = tap_slot(t, L, i1, j1, k0);
+    idx[4] = tap_slot(t, L, i0, j0, k1);
+    idx[5] = tap_slot(t, L, i1, j0, k1);
+    idx[6] = tap_slot(t, L, i0, j1, k1);
+    idx[7] = tap_slot(t, L, i1, j1, k1);
+}
+
+// |curl u| at a voxel (computeVorticityMag, src/Cuda/Utils.cuh:226-243).
+__device__ __forceinline__ float vort_mag(const TopoView& t, const LeafNbhd& L, const float* __restrict__ v, int i, int j, int k, float factor) {
+    const float3 px = near_v(t, L, v, i + 1, j, k), mx = near_v(t, L, v, i - 1, j, k);
+    const float3 py = near_v(t, L, v, i, j + 1, k), my = near_v(t, L, v, i, j - 1, k);
+    const float3 pz = near_v(t, L, v, i, j, k + 1), mz = near_v(t, L, v, i, j, k - 1);
+    const float ox = ((py.z - my.z) - (pz.y - mz.y)) * factor;
+    const float oy = ((pz.x - mz.x) - (px.z - mx.z)) * factor;
+    const float oz = ((px.y - mx.y) - (py.x - my.x)) * factor;
+    return __fsqrt_rn(ox * ox + oy * oy + oz * oz);
+}
+
+// Voxel handled by this thread in the "two CTAs per leaf" kernels.
+struct VoxelIdx {
+    int64_t leaf;
+    int n;  // local slot 0..511
+};
+
+__device__ __forceinline__ VoxelIdx voxel_of_block() {
+    VoxelIdx v;
+    v.leaf = (int64_t)(blockIdx.x >> 1);
+    v.n = (int)(((blockIdx.x & 1u) << 8) | threadIdx.x);
+    return v;
+}
+
+}  // namespace dev
+}  // namespace hns

@@ -163,3 +163,34 @@ def smoothed_fields(origins: np.ndarray, seed: int = 0, box_passes: int = 3):
     vel = rng.uniform(-1.0, 1.0, size=(len(coords), 3)).astype(np.float32)
     vel = box_filter(vel, coords, box_passes)
     return np.ascontiguousarray(dens, dtype=np.float32), np.ascontiguousarray(vel, dtype=np.float32)
+
+
+def value_noise_leaves(origins: np.ndarray, seed: int = 0) -> np.ndarray:
+    """value_noise(leaf_dense_coords(origins), seed) with the 8-voxel lattice, computed per
+    leaf: every leaf lies in one lattice cell, so its 512 values are a fixed 512x8 weight
+    matrix applied to the cell's 8 corner values."""
+    o = np.asarray(origins, dtype=np.int64).reshape(-1, 3)
+    lo = o.min(axis=0)
+    cell = (o - lo) // 8
+    shape = tuple(int(v) + 2 for v in cell.max(axis=0))
+    rng = np.random.default_rng(seed)
+    lat = rng.random(shape, dtype=np.float32)
+    t = local_offsets().astype(np.float32) / 8.0
+    w = np.empty((512, 8), dtype=np.float32)
+    corners = np.empty((len(o), 8), dtype=np.float32)
+    q = 0
+    for a in (0, 1):
+        for b in (0, 1):
+            for c in (0, 1):
+                w[:, q] = (t[:, 0] if a else 1 - t[:, 0]) * (t[:, 1] if b else 1 - t[:, 1]) * (t[:, 2] if c else 1 - t[:, 2])
+                corners[:, q] = lat[cell[:, 0] + a, cell[:, 1] + b, cell[:, 2] + c]
+                q += 1
+    return (corners @ w.T).reshape(-1)
+
+
+def noise_fields(origins: np.ndarray, seed: int = 0):
+    """Cheap smooth fields for the large workloads: density = value noise in [0, 1]; each
+    velocity component = 2 * (independent value noise) - 1. Shapes (N,) and (N, 3)."""
+    dens = value_noise_leaves(origins, seed)
+    vel = np.stack([2.0 * value_noise_leaves(origins, seed + 1 + k) - 1.0 for k in range(3)], axis=1)
+    return np.ascontiguousarray(dens, dtype=np.float32), np.ascontiguousarray(vel, dtype=np.float32)

@@ -1,0 +1,141 @@
+/* hns.h -- C ABI of the B200 sparse smoke/fire solver (libhns.so).
+ *
+ * Plain C: opaque context, status codes, raw pointers and sizes. No exception crosses this
+ * boundary and no C++ or torch type appears in it. The C++ surface that mirrors the
+ * reference's own entry points (HNS_EnsureContext, AdvectIndexGrid, ...) is declared in
+ * hns_legacy.hpp and is implemented on top of these functions.
+ *
+ * Data layout (the reference's "indexed" layout, src/Utils/GridBuilder.hpp:164-174,
+ * 231-251): the domain is a set of 8^3 leaves; leaf i owns slots [512 i, 512 i + 512) and
+ * slot 512 i + n holds the voxel at origin_i + ((n>>6)&7, (n>>3)&7, n&7). A voxel's
+ * NanoVDB ValueOnIndex offset is 1 + slot, and 0 outside the domain
+ * (externals/nanovdb/NanoVDB.h:4219-4227, 4598-4601). Scalar fields are float[N]; vec3
+ * fields are float[3N] interleaved x,y,z per slot (the reference's nanovdb::Vec3f arrays).
+ *
+ * Unless a function says otherwise, field pointers are DEVICE pointers on the context's
+ * device and work is enqueued on the context's stream; every entry point returns after
+ * its work is enqueued (call hns_synchronize to wait). All functions are thread-safe for
+ * distinct contexts; one context must not be used from two threads at once.
+ */
+#ifndef HNS_H
+#define HNS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define HNS_API __declspec(dllexport)
+#else
+#define HNS_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HNS_ABI_VERSION 1
+
+typedef enum hns_status {
+    HNS_OK = 0,
+    HNS_ERR_INVALID_ARG = 1,   /* null pointer, bad size, bad enum value */
+    HNS_ERR_CUDA = 2,          /* a CUDA runtime call failed; see hns_last_error() */
+    HNS_ERR_OUT_OF_MEMORY = 3, /* device allocation failed */
+    HNS_ERR_NOT_FOUND = 4,     /* named field does not exist */
+    HNS_ERR_LAYOUT = 5,        /* coordinates are not leaf-dense / leaves not 8-aligned or repeated */
+    HNS_ERR_NOT_CONVERGED = 6, /* iterative solve hit its iteration cap above the tolerance */
+    HNS_ERR_UNSUPPORTED = 7,   /* valid request this build does not support (see message) */
+    HNS_ERR_TIMEOUT = 8        /* a bounded device-side wait gave up */
+} hns_status;
+
+typedef struct hns_ctx hns_ctx;
+
+HNS_API int hns_abi_version(void);
+HNS_API const char* hns_status_string(hns_status status);
+/* Message of the last failing call on this thread ("" if none). */
+HNS_API const char* hns_last_error(void);
+
+/* ---- topology --------------------------------------------------------------------------
+ * Replaces CreateIndexGrid (src/Cuda/HNanoSolver.cu:498-510, which builds a NanoVDB
+ * ValueOnIndex grid with voxelsToGrid) and the per-context setup of HNS_EnsureContext
+ * (src/Cuda/HNanoSolver.cu:58-156). The caller's slot order is authoritative: leaf i of
+ * `leaf_origins` owns slots [512 i, 512 i + 512). When the leaves are in NanoVDB order
+ * (hns_sort_leaves_nanovdb) every voxel's offset equals the reference grid's. */
+
+/* leaf_origins: host int32[3 * num_leaves], each a multiple of 8, no repeats.
+ * device: CUDA device ordinal. The context creates its own non-blocking stream. */
+HNS_API hns_status hns_create(hns_ctx** out, const int32_t* leaf_origins, int64_t num_leaves, float voxel_size,
+                              int device);
+/* coords: host int32[3 * num_voxels] in the leaf-dense layout above (num_voxels a multiple
+ * of 512); HNS_ERR_LAYOUT otherwise. This is the coordinate block of GridIndexedData. */
+HNS_API hns_status hns_create_from_coords(hns_ctx** out, const int32_t* coords, int64_t num_voxels,
+                                          float voxel_size, int device);
+HNS_API hns_status hns_destroy(hns_ctx* ctx);
+/* Use a caller-owned cudaStream_t (NULL restores the context's own stream). */
+HNS_API hns_status hns_set_stream(hns_ctx* ctx, void* cuda_stream);
+HNS_API void* hns_get_stream(const hns_ctx* ctx);
+HNS_API hns_status hns_synchronize(hns_ctx* ctx);
+HNS_API int64_t hns_num_voxels(const hns_ctx* ctx);
+HNS_API int64_t hns_num_leaves(const hns_ctx* ctx);
+HNS_API float hns_voxel_size(const hns_ctx* ctx);
+/* Host int32[3 * num_leaves]. */
+HNS_API hns_status hns_leaf_origins(const hns_ctx* ctx, int32_t* out);
+/* ValueOnIndex offsets (0 outside the domain, else 1 + slot) of host ijk[3n], computed on
+ * the device; out is host uint64[n]. Synchronous. */
+HNS_API hns_status hns_index_offsets(hns_ctx* ctx, const int32_t* ijk, int64_t n, uint64_t* out);
+/* Sorts host leaf origins in place into NanoVDB leaf order. */
+HNS_API hns_status hns_sort_leaves_nanovdb(int32_t* leaf_origins, int64_t num_leaves);
+/* *out = 1 if the context's leaves are in NanoVDB order, else 0. */
+HNS_API hns_status hns_is_nanovdb_order(const hns_ctx* ctx, int* out);
+
+/* ---- operators on device arrays ---------------------------------------------------------
+ * One call = one pass of the corresponding reference kernel over every slot, with the
+ * context's voxel size. Inputs and outputs must not alias unless stated. */
+
+/* MacCormack vec3 advection (advect_vector, src/Cuda/Kernel.cu:349-426): vel -> out. */
+HNS_API hns_status hns_advect_vec3(hns_ctx* ctx, const float* vel, float* out, float dt);
+/* Single-field MacCormack advection (advect_scalar, src/Cuda/Kernel.cu:294-344; the kernel
+ * behind HNanoAdvect): samplers read 0 outside the domain. */
+HNS_API hns_status hns_advect_scalar(hns_ctx* ctx, const float* vel, const float* in, float* out, float dt);
+/* Multi-field advection of HNS_Advance (advect_scalars, src/Cuda/Kernel.cu:163-289): the
+ * back-trace uses the voxel's own velocity and out-of-domain taps read slot 0.
+ * in/out: HOST arrays of nfields device pointers. */
+HNS_API hns_status hns_advect_scalars(hns_ctx* ctx, const float* vel, const float* const* in, float* const* out,
+                                      int nfields, float dt);
+/* Central divergence (divergence, src/Cuda/Kernel.cu:432-453). */
+HNS_API hns_status hns_divergence(hns_ctx* ctx, const float* vel, float* div);
+
+/* Flags of the pressure solve. */
+#define HNS_SOLVE_ZERO_INIT 1u   /* start from p = 0 (p is not read; the reference's memset) */
+#define HNS_SOLVE_NEUMANN 2u     /* zero-gradient walls instead of the reference's p = 0 outside */
+
+/* `iterations` red-black SOR iterations on div (redBlackGaussSeidelUpdate,
+ * src/Cuda/Kernel.cu:459-489, looped as src/Cuda/HNanoSolver.cu:366-373): colour
+ * (i+j+k)&1, p = 0 outside, fixed 1/6. p: device float[N], in/out. */
+HNS_API hns_status hns_rbgs(hns_ctx* ctx, const float* div, float* p, int iterations, float omega, unsigned flags);
+/* u = u* - grad p (subtractPressureGradient, src/Cuda/Kernel.cu:495-541). */
+HNS_API hns_status hns_subtract_gradient(hns_ctx* ctx, const float* vel, const float* p, float* out);
+/* Vorticity confinement (vorticityConfinement, src/Cuda/Kernel.cu:682-727), out of place.
+ * The |omega| gradient is taken int(factor_scale) voxels away, as the reference's Coord
+ * construction truncates the float. */
+HNS_API hns_status hns_vorticity_confinement(hns_ctx* ctx, const float* vel, float* out, float dt, float scale,
+                                             float factor_scale);
+
+/* Result of a pressure solve. */
+typedef struct hns_solve_info {
+    int iterations;           /* red-black iterations run */
+    double residual;          /* ||b - A p||_2 / ||b||_2 in FP64 after the solve (b = div dx^2) */
+    double initial_residual;  /* same for the initial p */
+} hns_solve_info;
+
+/* HNanoProjectNonDivergent (src/Cuda/PressureProjection.cu:9-78): divergence of vel,
+ * p = 0, `iterations` red-black iterations, vel -= grad p in place. omega <= 0 selects the
+ * reference's 2/(1+sin(3.14159 dx)). `info` may be NULL; when given, the FP64 residuals
+ * are computed (two extra reduction passes) and the call synchronizes. */
+HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float omega, unsigned flags,
+                               hns_solve_info* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HNS_H */
