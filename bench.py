@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of one solver step on a seeded synthetic sparse grid, on 1..N GPUs.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload shell512] [--precision fp32]
+
+A step is one pass of the hot path over the grid: the SOP operator chain
+HNanoAdvect + HNanoAdvectVelocity + HNanoProjectNonDivergent (scalars and velocity advected
+along one MacCormack trace, divergence, red-black SOR to a relative FP64 Poisson residual of
+1e-5, gradient subtraction), through the C ABI of libhns.so. The metric is active
+voxel-steps/s. Under torchrun every rank runs an independent replica of the workload
+(the solver does not shard a grid across GPUs), so scaling is weak.
+
+--impl reference times the reference's own CPU implementation of the same step (its
+src/Cuda/Kernel.cu kernels compiled as host C++, oracle/_ref, all host threads) on a
+bounded sample of the same workload: every launch of the step runs an evenly spaced subset
+of its thread blocks, with the red-black iteration count the GPU solve needed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+# Workloads: the grid, the step parameters and the red-black iteration count the FP32 solve
+# needs to reach the tolerance on it (the reference arm runs that fixed count: its operator
+# takes an iteration count, not a tolerance).
+WORKLOADS = {
+    "shell512": dict(desc="512^3 box, 16-voxel band (+ leaf half-diagonal) around a seeded radius-200 sphere, "
+                          "fields: value-noise density, value-noise velocity in (-1,1)",
+                     dx=0.1, dt=0.1, omega=1.9, tolerance=1e-5, cap=2000, check_every=10, fp32_iterations=None),
+    "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60",
+                     dx=0.1, dt=1.0 / 24.0, omega=1.9, tolerance=1e-5, cap=2000, check_every=10, fp32_iterations=None),
+    "box64": dict(desc="64^3 box fully active (512 leaves)", dx=0.1, dt=0.1, omega=1.0, tolerance=0.0, cap=40,
+                  check_every=0, fp32_iterations=40),
+}
+RBGS_BYTES_PER_VOXEL = 12  # one fused red+black iteration: read p, read div, write p (FP32)
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per launch of the red-black kernel from the committed ncu summary
+    (profiles/rbgs_iteration_<workload>.md, line `dram_bytes_per_launch: <int>`), or None."""
+    path = os.path.join(ROOT, "profiles", f"rbgs_iteration_{workload}.md")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.strip().startswith("dram_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1].strip().split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def reference_arm(args, wl):
+    """Reference CPU implementation of the step on a bounded sample (rank 0 only)."""
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    from hnanosolver_b200 import synth
+    from oracle import binding
+
+    ref = binding.RefOracle()
+    cores = ref.lib.ref_num_threads()
+    origins = synth.topology(args.workload)
+    dens, vel = synth.noise_fields(origins, seed=0)
+    g = ref.grid(synth.leaf_dense_coords(origins))
+    iters = wl["fp32_iterations"] or 200
+    n = len(dens)
+    blocks = (n + 255) // 256
+    stride = max(1, blocks // 4096)
+    ref.lib.ref_set_block_stride(stride)
+    scratch = None
+    for _ in range(args.warmup):
+        scratch = g.plain_step(vel, [dens], wl["dt"], wl["dx"], iters, wl["omega"], scratch)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        scratch = g.plain_step(vel, [dens], wl["dt"], wl["dx"], iters, wl["omega"], scratch)
+        times.append(time.perf_counter() - t0)
+    ref.lib.ref_set_block_stride(1)
+    sampled = (blocks + stride - 1) // stride * 256
+    t = sum(times) / len(times)
+    value = sampled / t
+    sample = (f"every launch of the step over 1/{stride} of its 256-voxel blocks ({sampled} of {n} voxels), "
+              f"{iters} red-black iterations, {args.steps} steps")
+    line = {
+        "impl": "reference", "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "voxels": n, "leaves": len(origins), "red_black_iterations": iters},
+        "cpu_baseline": {"value": value, "unit": "voxel-steps/s", "cores": cores, "kind": "reference",
+                         "sample": sample, "cpu": binding.cpu_model(), "library": os.path.basename(ref.path)},
+        "e2e": {"value": value, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args, wl, iters):
+    """The reference's CPU step on a bounded sample, for the cpu_baseline key of our line."""
+    from hnanosolver_b200 import synth
+    from oracle import binding
+
+    ref = binding.RefOracle()
+    origins = synth.topology(args.workload)
+    dens, vel = synth.noise_fields(origins, seed=0)
+    g = ref.grid(synth.leaf_dense_coords(origins))
+    n = len(dens)
+    blocks = (n + 255) // 256
+    stride = max(1, blocks // 4096)
+    ref.lib.ref_set_block_stride(stride)
+    scratch = g.plain_step(vel, [dens], wl["dt"], wl["dx"], iters, wl["omega"])
+    reps, t0 = 0, time.perf_counter()
+    while reps < 3 and (reps == 0 or time.perf_counter() - t0 < 15.0):
+        scratch = g.plain_step(vel, [dens], wl["dt"], wl["dx"], iters, wl["omega"], scratch)
+        reps += 1
+    t = (time.perf_counter() - t0) / reps
+    ref.lib.ref_set_block_stride(1)
+    sampled = (blocks + stride - 1) // stride * 256
+    return {"value": sampled / t, "unit": "voxel-steps/s", "cores": ref.lib.ref_num_threads(), "kind": "reference",
+            "sample": f"{reps} steps, every launch over 1/{stride} of its 256-voxel blocks ({sampled} of {n} voxels), "
+                      f"{iters} red-black iterations", "cpu": binding.cpu_model()}
+
+
+def ours(args, wl):
+    import torch
+
+    from hnanosolver_b200 import lib as hl
+    from hnanosolver_b200 import synth
+
+    rank, world, local = dist_info()
+    dist = world > 1
+    if dist:
+        import datetime
+
+        import torch.distributed as td
+
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    origins = synth.topology(args.workload)
+    dens, vel = synth.noise_fields(origins, seed=rank)
+    n = len(dens)
+    g = hl.Grid(origins, voxel_size=wl["dx"], device=local)
+    stream = torch.cuda.Stream(device=dev)
+    g.set_stream(stream.cuda_stream)
+    v = [torch.from_numpy(vel).to(dev), torch.empty((n, 3), device=dev)]
+    d = [torch.from_numpy(dens).to(dev), torch.empty(n, device=dev)]
+    torch.cuda.synchronize()
+
+    def desc(cap):
+        return hl.StepDesc(dt=wl["dt"], max_iterations=cap, omega=wl["omega"], tolerance=wl["tolerance"],
+                           check_every=wl["check_every"], flags=0)
+
+    # Iterations the solve needs on this grid: one checked solve, then a cap with a margin
+    # of two check periods so that few launches are skipped at the end of each solve.
+    info = g.step_plain(v[0], v[1], [d[0]], [d[1]], desc(wl["cap"]), info=True)
+    need = info.iterations
+    cap = need if wl["tolerance"] == 0 else need + 2 * max(2, wl["check_every"])
+    st = desc(cap)
+    state = 1
+
+    def step():
+        nonlocal state
+        g.step_plain(v[state], v[1 - state], [d[state]], [d[1 - state]], st)
+        state = 1 - state
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    clocks = ClockSampler(torch.cuda.current_device() if not os.environ.get("CUDA_VISIBLE_DEVICES") else local)
+    clocks.start()
+    g.profile_read()
+    g.profile_enable(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        td.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    g.profile_enable(False)
+    prof = g.profile_read()
+    last = g.last_solve()
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * n * args.steps / (ms / 1e3)
+
+    # Dominant kernel: the fused red-black iteration. Average duration of the launches that ran
+    # inside the timed region (solve-phase events / device launch counter).
+    solve_ms = prof.phase_ms[hl.PHASES["solve"]]
+    launches = max(1, prof.solver_launches)
+    rbgs_ms = solve_ms / launches
+    peak, peak_kind = measured_peak_gbs()
+    achieved = RBGS_BYTES_PER_VOXEL * n / (rbgs_ms / 1e3) / 1e9
+    traffic = profiled_traffic(args.workload)
+
+    # End to end through the C ABI with host buffers: each step uploads the velocity and
+    # density from pinned host memory, steps, and downloads both.
+    hv = torch.from_numpy(vel).pin_memory().numpy()
+    hd = torch.from_numpy(dens).pin_memory().numpy()
+    e2e_steps = max(1, min(args.steps, 5))
+    g.step_plain_host(hv, [hd], st)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        g.step_plain_host(hv, [hd], st)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, wl, need)
+
+    if rank == 0:
+        phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
+        line = {
+            "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": wl["desc"], "voxels": n, "leaves": len(origins),
+                       "precision": args.precision, "dt": wl["dt"], "dx": wl["dx"], "omega": wl["omega"],
+                       "tolerance": wl["tolerance"], "red_black_iterations": last.iterations,
+                       "iterations_needed_at_start": need, "iteration_cap": cap,
+                       "last_checked_residual": last.residual, "residual_at_start": info.residual,
+                       "l2": "inputs larger than L2 (state %.0f MB per GPU)" % ((16 * 2 + 8) * n / 1e6),
+                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+                       "phase_ms_per_step": phase_ms},
+            "roofline": {"kernel": "rbgs_iteration_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": RBGS_BYTES_PER_VOXEL * n, "launch_ms": rbgs_ms,
+                         "launches_timed": int(prof.solver_launches)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": 16 * n,
+                    "d2h_bytes_per_step": 16 * n, "steps": e2e_steps,
+                    "path": "hns_step_plain_host (C ABI, pinned host buffers)"},
+            "gpu_launches": args.steps * (3 + cap),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        td.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="shell512")
+    ap.add_argument("--precision", choices=["fp32"], default="fp32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        reference_arm(args, wl)
+    else:
+        ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

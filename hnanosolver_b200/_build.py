@@ -31,5 +31,19 @@ def build(verbose: bool = False, extra=()) -> str:
     return LIB
 
 
+def build_legacy_test() -> str:
+    """The C++ program that drives the reference-named entry points (tests/legacy)."""
+    src = os.path.join(ROOT, "tests", "legacy", "legacy_api_test.cpp")
+    out_dir = os.path.join(ROOT, "tests", "legacy", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, "legacy_api_test")
+    cuda = os.path.dirname(os.path.dirname(os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")))
+    cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", os.path.join(cuda, "include"), src,
+           "-o", exe, "-L", PKG, "-lhns", "-L", os.path.join(cuda, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN/../../../hnanosolver_b200", "-Wl,-rpath," + os.path.join(cuda, "lib64")]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
 if __name__ == "__main__":
     build(verbose=True, extra=sys.argv[1:])

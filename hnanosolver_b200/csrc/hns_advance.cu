@@ -1,0 +1,369 @@
+// The all-in-one solver step of the HNanoSolver SOP (HNS_Advance,
+// src/Cuda/HNanoSolver.cu:223-456) over the context's named fields, and the field store
+// that replaces the reference's SimContext maps (src/Cuda/HNanoSolver.cu:27-48).
+//
+// Per substep the reference runs about 2*iterations + 15 launches, with cudaMalloc'd
+// temporaries, memsets and device-to-device copies. Here:
+//   advect_fused          velocity -> adv                       (advect_vector)
+//   confine_sources       adv -> adv2, + sources, gravity       (vorticityConfinement out of
+//                                                                place, add_velocity_source(_xyz),
+//                                                                add_scalar_source, add_gravity)
+//   div_combust_buoy      adv2 -> div, fields, adv3             (divergence, combustion_oxygen,
+//                                                                temperature_buoyancy)
+//   rbgs x iterations     div -> p                              (redBlackGaussSeidelUpdate)
+//   [divergence, rbgs x max(2, iterations/2)]  when disturbanceEnable > 0
+//   subtract_gradient     adv3, p -> velocity
+//   advect_scalars        the persistent scalars, with the projected velocity
+// Each fusion applies the reference's per-voxel operations in the reference's order, so
+// every output equals the reference's (the confinement race aside: it runs out of place).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hns_internal.cuh"
+#include "hns_stencil.cuh"
+
+namespace hns {
+namespace {
+
+using namespace dev;
+
+constexpr int kThreads = 256;
+
+struct ScalarSources {
+    float* dst[3];
+    const float* src[3];
+    int count;
+};
+
+// vorticityConfinement (src/Cuda/Kernel.cu:682-727) out of place, then the velocity source
+// (add_velocity_source / add_velocity_source_xyz, Kernel.cu:739-755), gravity (add_gravity,
+// Kernel.cu:834-838) and the scalar sources (add_scalar_source, Kernel.cu:732-737), in the
+// order HNS_Advance launches them (src/Cuda/HNanoSolver.cu:279-318).
+__global__ void __launch_bounds__(kThreads) confine_sources_kernel(TopoView t, const float* __restrict__ vel,
+                                                                    float* __restrict__ out, float dt, float inv_dx,
+                                                                    float scale, int fs, const float* __restrict__ src_v3,
+                                                                    const float* __restrict__ sx, const float* __restrict__ sy,
+                                                                    const float* __restrict__ sz, float gravity,
+                                                                    ScalarSources ss) {
+    __shared__ LeafNbhd L;
+    const VoxelIdx v = voxel_of_block();
+    load_nbhd(L, t, v.leaf);
+    __syncthreads();
+    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
+    const int64_t s = (v.leaf << 9) + v.n;
+    const float factor = 0.5f * inv_dx;
+    const float3 px = near_v(t, L, vel, i + 1, j, k), mx = near_v(t, L, vel, i - 1, j, k);
+    const float3 py = near_v(t, L, vel, i, j + 1, k), my = near_v(t, L, vel, i, j - 1, k);
+    const float3 pz = near_v(t, L, vel, i, j, k + 1), mz = near_v(t, L, vel, i, j, k - 1);
+    const float ox = ((py.z - my.z) - (pz.y - mz.y)) * factor;
+    const float oy = ((pz.x - mz.x) - (px.z - mx.z)) * factor;
+    const float oz = ((px.y - mx.y) - (py.x - my.x)) * factor;
+    const float mpx = vort_mag(t, L, vel, i + fs, j, k, factor), mmx = vort_mag(t, L, vel, i - fs, j, k, factor);
+    const float mpy = vort_mag(t, L, vel, i, j + fs, k, factor), mmy = vort_mag(t, L, vel, i, j - fs, k, factor);
+    const float mpz = vort_mag(t, L, vel, i, j, k + fs, factor), mmz = vort_mag(t, L, vel, i, j, k - fs, factor);
+    const float gx = (mpx - mmx) * 0.5f * inv_dx;
+    const float gy = (mpy - mmy) * 0.5f * inv_dx;
+    const float gz = (mpz - mmz) * 0.5f * inv_dx;
+    const float glen = sqrtf(gx * gx + gy * gy + gz * gz) + 1e-5f;
+    const float nx = gx / glen, ny = gy / glen, nz = gz / glen;
+    const float3 u = ld3(vel, s);
+    const float fx = scale * (ny * oz - nz * oy), fy = scale * (nz * ox - nx * oz), fz = scale * (nx * oy - ny * ox);
+    float3 r = make_float3(u.x + fx * dt, u.y + fy * dt, u.z + fz * dt);
+    if (src_v3 != nullptr) {
+        const float3 a = ld3(src_v3, s);
+        r.x += a.x * dt;
+        r.y += a.y * dt;
+        r.z += a.z * dt;
+    } else if (sx != nullptr && sy != nullptr && sz != nullptr) {
+        r.x += dt * __ldg(sx + s);
+        r.y += dt * __ldg(sy + s);
+        r.z += dt * __ldg(sz + s);
+    }
+    if (gravity != 0.0f) r.y -= gravity * dt;
+    st3(out, s, r);
+    for (int q = 0; q < ss.count; ++q) ss.dst[q][s] += dt * __ldg(ss.src[q] + s);
+}
+
+// divergence (Kernel.cu:432-453) of the forced velocity, combustion_oxygen
+// (Kernel.cu:641-677) in place on fuel/waste/temperature/flame with the expansion added to
+// that divergence, then temperature_buoyancy (Kernel.cu:546-563) from the burned temperature
+// into a separate velocity buffer (neighbouring threads still read `vel`).
+__global__ void __launch_bounds__(kThreads) div_combust_buoy_kernel(TopoView t, const float* __restrict__ vel,
+                                                                     float* __restrict__ vel_out, float* __restrict__ div,
+                                                                     float inv_dx, float* __restrict__ fuel,
+                                                                     float* __restrict__ waste, float* __restrict__ temp,
+                                                                     float* __restrict__ flame, float gain, float expansion,
+                                                                     float dt, float ambient, float strength) {
+    __shared__ LeafNbhd L;
+    const VoxelIdx v = voxel_of_block();
+    load_nbhd(L, t, v.leaf);
+    __syncthreads();
+    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
+    const int64_t s = (v.leaf << 9) + v.n;
+    const float3 c = ld3(vel, s);
+    const float xp = (c.x + near_v(t, L, vel, i + 1, j, k).x) * 0.5f;
+    const float xm = (c.x + near_v(t, L, vel, i - 1, j, k).x) * 0.5f;
+    const float yp = (c.y + near_v(t, L, vel, i, j + 1, k).y) * 0.5f;
+    const float ym = (c.y + near_v(t, L, vel, i, j - 1, k).y) * 0.5f;
+    const float zp = (c.z + near_v(t, L, vel, i, j, k + 1).z) * 0.5f;
+    const float zm = (c.z + near_v(t, L, vel, i, j, k - 1).z) * 0.5f;
+    float dv = (xp - xm + yp - ym + zp - zm) * inv_dx;
+
+    float f = fuel[s];
+    const float w = waste[s], T = temp[s], fl = flame[s];
+    if (f < 0.001f) f = 0.0f;
+    const float oxy = 1.0f - f - w;
+    float Tn = T;
+    if (oxy < 0.0f) {
+        fuel[s] = f;
+    } else {
+        const float burn = fminf(oxy, f);
+        fuel[s] = f - burn;
+        waste[s] = w + burn * 2.0f;
+        Tn = T + burn * gain;
+        temp[s] = Tn;
+        dv += burn * expansion;
+        flame[s] = fmaxf(fl, fminf(1.0f, burn * 10.0f));
+    }
+    div[s] = dv;
+    if (Tn <= ambient) {
+        st3(vel_out, s, c);
+    } else {
+        const float by = fmaxf(0.0f, (Tn - ambient) * strength);
+        st3(vel_out, s, make_float3(c.x + 0.0f * dt, c.y + by * dt, c.z + 0.0f * dt));
+    }
+}
+
+unsigned leaf_blocks(const Context& c) { return (unsigned)(c.topo.num_leaves * 2); }
+
+bool is_source(const std::string& n) { return n.rfind("src_", 0) == 0; }
+
+}  // namespace
+
+// ---- field store -----------------------------------------------------------------------------
+
+Field* Context::find_field(const std::string& name) {
+    for (auto& f : fields)
+        if (f.name == name) return &f;
+    return nullptr;
+}
+
+Field& Context::ensure_field(const std::string& name, int components, bool zero) {
+    Field* f = find_field(name);
+    if (f && f->components != components) fail(HNS_ERR_INVALID_ARG, "field '" + name + "' exists with another component count");
+    if (!f) {
+        fields.push_back(Field{name, components, DeviceBuffer()});
+        f = &fields.back();
+        f->buf.alloc(sizeof(float) * (size_t)components * (size_t)num_voxels());
+        if (zero) HNS_CUDA(cudaMemsetAsync(f->buf.ptr, 0, f->buf.bytes, stream));
+    }
+    return *f;
+}
+
+void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& P) {
+    const size_t n = (size_t)c.num_voxels();
+    const float dx = c.dx;
+    const float inv_dx = 1.0f / dx;
+    const int subs = std::max(1, P.substeps);
+    const float dt_sub = dt / (float)subs;
+
+    // Velocity: "velocity", else the first vec3 field (src/Cuda/HNanoSolver.cu:99-108).
+    Field* velf = c.find_field("velocity");
+    if (!velf || velf->components != 3) {
+        velf = nullptr;
+        for (auto& f : c.fields)
+            if (f.components == 3 && !is_source(f.name)) {
+                velf = &f;
+                break;
+            }
+    }
+    if (!velf) fail(HNS_ERR_NOT_FOUND, "no vec3 velocity field in the context");
+    const std::string vel_name = velf->name;
+    // Persistent scalars present when the call starts are the ones advected (:247-250).
+    std::vector<std::string> adv_names;
+    for (auto& f : c.fields)
+        if (f.components == 1 && !is_source(f.name) && f.name != "collision_sdf") adv_names.push_back(f.name);
+
+    float* adv = c.scratch_f32("advance_adv", 3 * n);
+    float* adv2 = c.scratch_f32("advance_adv2", 3 * n);
+    float* adv3 = c.scratch_f32("advance_adv3", 3 * n);
+    float* div = c.scratch_f32("advance_div", n);
+    float* p = c.scratch_f32("advance_p", n);
+    const float omega = 2.0f / (1.0f + sinf(3.14159f * dx));  // host sinf, as :365
+
+    for (int s = 0; s < subs; ++s) {
+        float* vel = c.find_field(vel_name)->buf.as<float>();
+        c.phase_begin(HNS_PHASE_ADVECT);
+        FieldSet none{};
+        launch_advect_fused(c, vel, adv, none, dt_sub);
+        c.phase_end();
+
+        Field* sv = c.find_field("src_vel");
+        Field* sx = c.find_field("src_vel_x");
+        Field* sy = c.find_field("src_vel_y");
+        Field* sz = c.find_field("src_vel_z");
+        ScalarSources ss{};
+        static const char* pairs[3][2] = {{"src_temperature", "temperature"}, {"src_density", "density"}, {"src_fuel", "fuel"}};
+        for (auto& pr : pairs) {
+            Field* src = c.find_field(pr[0]);
+            Field* dst = c.find_field(pr[1]);
+            if (src && dst && src->components == 1 && dst->components == 1) {
+                ss.src[ss.count] = src->buf.as<float>();
+                ss.dst[ss.count] = dst->buf.as<float>();
+                ++ss.count;
+            }
+        }
+        c.phase_begin(HNS_PHASE_FORCES);
+        confine_sources_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+            c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, (int)P.factorScale,
+            (sv && sv->components == 3) ? sv->buf.as<float>() : nullptr,
+            (sx && sx->components == 1) ? sx->buf.as<float>() : nullptr, (sy && sy->components == 1) ? sy->buf.as<float>() : nullptr,
+            (sz && sz->components == 1) ? sz->buf.as<float>() : nullptr, P.gravity, ss);
+        HNS_LAUNCHED();
+
+        // fuel/waste/temperature/flame are created zero-filled on first use (:326-338).
+        float* fuel = c.ensure_field("fuel", 1, true).buf.as<float>();
+        float* waste = c.ensure_field("waste", 1, true).buf.as<float>();
+        float* temp = c.ensure_field("temperature", 1, true).buf.as<float>();
+        float* flame = c.ensure_field("flame", 1, true).buf.as<float>();
+        div_combust_buoy_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+            c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, P.temperatureRelease, P.expansionRate, dt_sub,
+            P.ambientTemp, P.buoyancyStrength);
+        HNS_LAUNCHED();
+        c.phase_end();
+
+        c.phase_begin(HNS_PHASE_SOLVE);
+        rbgs_solve(c, div, p, iterations, omega, HNS_SOLVE_ZERO_INIT);
+        if (P.disturbanceEnable > 0.0f) {
+            // The disturbance injection is commented out in the reference; what remains is a
+            // second, shorter solve of the divergence without the expansion (:377-403).
+            launch_divergence(c, adv3, div);
+            rbgs_solve(c, div, p, std::max(2, iterations / 2), omega, HNS_SOLVE_ZERO_INIT);
+        }
+        c.phase_end();
+        c.phase_begin(HNS_PHASE_GRADIENT);
+        vel = c.find_field(vel_name)->buf.as<float>();
+        launch_subtract_gradient(c, adv3, p, vel);
+        c.phase_end();
+
+        if (!adv_names.empty()) {
+            c.phase_begin(HNS_PHASE_ADVECT);
+            // Each field has a twin buffer in the scratch store: the advection writes the twin
+            // and the two are swapped, so no step allocates or copies.
+            for (size_t base = 0; base < adv_names.size(); base += kMaxAdvectFields) {
+                FieldSet f{};
+                f.count = (int)std::min<size_t>(kMaxAdvectFields, adv_names.size() - base);
+                for (int q = 0; q < f.count; ++q) {
+                    f.in[q] = c.find_field(adv_names[base + q])->buf.as<float>();
+                    f.out[q] = c.scratch_f32("advance_twin:" + adv_names[base + q], n);
+                }
+                launch_advect_scalars(c, vel, f, dt_sub);
+            }
+            for (const auto& name : adv_names) std::swap(c.find_field(name)->buf, c.scratch["advance_twin:" + name]);
+            c.phase_end();
+        }
+    }
+}
+
+}  // namespace hns
+
+using namespace hns;
+
+extern "C" {
+
+HNS_API hns_status hns_field_set(hns_ctx* ctx, const char* name, int components, const float* data, int on_device) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!name || !*name) fail(HNS_ERR_INVALID_ARG, "empty field name");
+        if (components != 1 && components != 3) fail(HNS_ERR_INVALID_ARG, "components must be 1 or 3");
+        DeviceGuard g(c->device);
+        Field* f = c->find_field(name);
+        if (f && f->components != components) {
+            c->fields.erase(c->fields.begin() + (f - c->fields.data()));
+            f = nullptr;
+        }
+        Field& fld = c->ensure_field(name, components, data == nullptr);
+        if (data)
+            HNS_CUDA(cudaMemcpyAsync(fld.buf.ptr, data, fld.buf.bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                     c->stream));
+        if (!on_device) HNS_CUDA(cudaStreamSynchronize(c->stream));  // host buffer may be reused on return
+    });
+}
+
+HNS_API hns_status hns_field_get(hns_ctx* ctx, const char* name, float* out, int on_device) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!name || !out) fail(HNS_ERR_INVALID_ARG, "null argument");
+        Field* f = c->find_field(name);
+        if (!f) fail(HNS_ERR_NOT_FOUND, std::string("no field '") + name + "'");
+        DeviceGuard g(c->device);
+        HNS_CUDA(cudaMemcpyAsync(out, f->buf.ptr, f->buf.bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                 c->stream));
+        if (!on_device) HNS_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+HNS_API hns_status hns_field_ptr(hns_ctx* ctx, const char* name, float** dev_ptr, int* components) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!name || !dev_ptr) fail(HNS_ERR_INVALID_ARG, "null argument");
+        Field* f = c->find_field(name);
+        if (!f) fail(HNS_ERR_NOT_FOUND, std::string("no field '") + name + "'");
+        *dev_ptr = f->buf.as<float>();
+        if (components) *components = f->components;
+    });
+}
+
+HNS_API hns_status hns_field_remove(hns_ctx* ctx, const char* name) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!name) fail(HNS_ERR_INVALID_ARG, "null name");
+        Field* f = c->find_field(name);
+        if (!f) fail(HNS_ERR_NOT_FOUND, std::string("no field '") + name + "'");
+        DeviceGuard g(c->device);
+        HNS_CUDA(cudaStreamSynchronize(c->stream));
+        c->fields.erase(c->fields.begin() + (f - c->fields.data()));
+    });
+}
+
+HNS_API int hns_field_count(const hns_ctx* ctx) { return ctx ? (int)ctx->impl.fields.size() : 0; }
+
+HNS_API hns_status hns_field_info(const hns_ctx* ctx, int index, char* name, size_t name_len, int* components) {
+    return guarded([&] {
+        const Context* c = check_ctx(ctx);
+        if (index < 0 || index >= (int)c->fields.size()) fail(HNS_ERR_INVALID_ARG, "field index out of range");
+        const Field& f = c->fields[(size_t)index];
+        if (name && name_len > 0) {
+            const size_t m = std::min(name_len - 1, f.name.size());
+            std::memcpy(name, f.name.data(), m);
+            name[m] = '\0';
+        }
+        if (components) *components = f.components;
+    });
+}
+
+HNS_API hns_status hns_advance(hns_ctx* ctx, int iterations, float dt, const hns_combustion_params* params) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!params) fail(HNS_ERR_INVALID_ARG, "null params");
+        if (iterations < 0) fail(HNS_ERR_INVALID_ARG, "negative iteration count");
+        DeviceGuard g(c->device);
+        run_advance(*c, iterations, dt, *params);
+    });
+}
+
+HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!out) fail(HNS_ERR_INVALID_ARG, "null output");
+        // build_activity_mask writes 1 for every slot (src/Cuda/Kernel.cu:75).
+        std::memset(out, 1, (size_t)c->num_voxels());
+    });
+}
+
+}  // extern "C"

@@ -190,9 +190,23 @@ float* Context::scratch_f32(const std::string& name, size_t count) {
 }
 
 double* Context::reduce_slots(int count) {
-    const size_t bytes = sizeof(double) * (size_t)count;
-    if (d_reduce.bytes < bytes) d_reduce.alloc(std::max<size_t>(bytes, 64 * sizeof(double)));
+    if (count > kReduceSlots) fail(HNS_ERR_UNSUPPORTED, "more than " + std::to_string(kMaxChecks) + " convergence checks");
+    if (!d_reduce.ptr) d_reduce.alloc(sizeof(double) * kReduceSlots);
     return d_reduce.as<double>();
+}
+
+void Context::phase_begin(int phase) {
+    if (!profiling) return;
+    PhaseEvent e{phase, nullptr, nullptr};
+    HNS_CUDA(cudaEventCreate(&e.start));
+    HNS_CUDA(cudaEventCreate(&e.stop));
+    HNS_CUDA(cudaEventRecord(e.start, stream));
+    phase_events.push_back(e);
+}
+
+void Context::phase_end() {
+    if (!profiling || phase_events.empty()) return;
+    HNS_CUDA(cudaEventRecord(phase_events.back().stop, stream));
 }
 
 Context* check_ctx(hns_ctx* ctx) {
@@ -264,6 +278,10 @@ hns_status create_impl(hns_ctx** out, const int32_t* origins, int64_t num_leaves
         c.stream = c.own_stream;
         try {
             c.topo.build(origins, num_leaves, c.stream);
+            c.d_counters.alloc(sizeof(unsigned long long) * 8);
+            c.counters = c.d_counters.as<unsigned long long>();
+            HNS_CUDA(cudaMemsetAsync(c.counters, 0, c.d_counters.bytes, c.stream));
+            c.reduce_slots(1);
         } catch (...) {
             (void)cudaStreamDestroy(c.own_stream);
             c.own_stream = nullptr;
@@ -331,6 +349,11 @@ HNS_API hns_status hns_destroy(hns_ctx* ctx) {
         Context& c = ctx->impl;
         DeviceGuard g(c.device);
         if (c.stream) (void)cudaStreamSynchronize(c.stream);
+        for (auto& e : c.phase_events) {
+            (void)cudaEventDestroy(e.start);
+            (void)cudaEventDestroy(e.stop);
+        }
+        c.phase_events.clear();
         if (c.own_stream) (void)cudaStreamDestroy(c.own_stream);
         delete ctx;
     });
@@ -356,6 +379,37 @@ HNS_API hns_status hns_synchronize(hns_ctx* ctx) {
 HNS_API int64_t hns_num_voxels(const hns_ctx* ctx) { return ctx ? ctx->impl.num_voxels() : 0; }
 HNS_API int64_t hns_num_leaves(const hns_ctx* ctx) { return ctx ? ctx->impl.topo.num_leaves : 0; }
 HNS_API float hns_voxel_size(const hns_ctx* ctx) { return ctx ? ctx->impl.dx : 0.f; }
+
+HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        c->profiling = enable != 0;
+    });
+}
+
+HNS_API hns_status hns_profile_read(hns_ctx* ctx, hns_profile_data* out) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        check_ptr(out, "output");
+        DeviceGuard g(c->device);
+        std::memset(out, 0, sizeof(*out));
+        HNS_CUDA(cudaStreamSynchronize(c->stream));
+        for (auto& e : c->phase_events) {
+            float ms = 0.f;
+            HNS_CUDA(cudaEventElapsedTime(&ms, e.start, e.stop));
+            if (e.phase >= 0 && e.phase < HNS_NUM_PHASES) {
+                out->phase_ms[e.phase] += ms;
+                out->phase_count[e.phase] += 1;
+            }
+            (void)cudaEventDestroy(e.start);
+            (void)cudaEventDestroy(e.stop);
+        }
+        c->phase_events.clear();
+        HNS_CUDA(cudaMemcpy(&out->solver_launches, c->counters, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        HNS_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(unsigned long long), c->stream));
+        HNS_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
 
 HNS_API hns_status hns_leaf_origins(const hns_ctx* ctx, int32_t* out) {
     return guarded([&] {
@@ -509,7 +563,6 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
         if (!(omega > 0.f)) omega = (float)(2.0f / (1.0f + std::sin(3.14159 * (double)c->dx)));
         float* div = c->scratch_f32("project_div", n);
         float* p = c->scratch_f32("project_p", n);
-        float* ustar = c->scratch_f32("project_vel", 3 * n);
         launch_divergence(*c, vel, div);
         double* acc = nullptr;
         if (info) {
@@ -520,8 +573,7 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
         }
         rbgs_solve(*c, div, p, iterations, omega, flags | HNS_SOLVE_ZERO_INIT);
         if (info) launch_residual(*c, div, p, acc + 2, flags);
-        HNS_CUDA(cudaMemcpyAsync(ustar, vel, 3 * n * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
-        launch_subtract_gradient(*c, ustar, p, vel);
+        launch_subtract_gradient(*c, vel, p, vel);  // pointwise in vel: safe in place
         if (info) {
             double h[4];
             HNS_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));

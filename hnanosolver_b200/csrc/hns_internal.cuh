@@ -98,6 +98,26 @@ void sort_leaves_nanovdb(int32_t* origins, int64_t n);
 
 // ---- context ------------------------------------------------------------------------------
 
+// A named device field of the context (the reference's SimContext d_state / d_src maps).
+struct Field {
+    std::string name;
+    int components;  // 1 or 3 (vec3 interleaved)
+    DeviceBuffer buf;
+};
+
+// Schedule of one convergence-checked pressure solve (see rbgs_solve_checked).
+struct SolvePlan {
+    int max_iterations = 0;
+    int check_every = 0;
+    int num_checks = 0;
+    double tol = 0.0;
+    double* slots = nullptr;
+};
+
+// FP64 accumulators per context: 8 scratch doubles + 2 per convergence check.
+constexpr int kMaxChecks = 4096;
+constexpr int kReduceSlots = 8 + 2 * kMaxChecks;
+
 struct Context {
     int device = 0;
     cudaStream_t own_stream = nullptr;
@@ -106,7 +126,23 @@ struct Context {
     Topology topo;
     // Scratch owned by the context, grown on demand and reused across calls.
     std::map<std::string, DeviceBuffer> scratch;
-    DeviceBuffer d_reduce;  // FP64 reduction accumulators
+    DeviceBuffer d_reduce;  // FP64 reduction accumulators, allocated once (kReduceSlots doubles)
+    SolvePlan last_solve;   // schedule of the most recent checked solve (hns_last_solve)
+    // Profiling (hns_profile_*): device counters and per-phase events on the stream.
+    DeviceBuffer d_counters;
+    unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
+    bool profiling = false;
+    struct PhaseEvent {
+        int phase;
+        cudaEvent_t start, stop;
+    };
+    std::vector<PhaseEvent> phase_events;
+    void phase_begin(int phase);
+    void phase_end();
+    // Named fields in insertion order.
+    std::vector<Field> fields;
+    Field* find_field(const std::string& name);
+    Field& ensure_field(const std::string& name, int components, bool zero);
 
     int64_t num_voxels() const { return topo.num_leaves * 512; }
     float* scratch_f32(const std::string& name, size_t count);
@@ -148,6 +184,9 @@ void launch_vorticity(const Context& c, const float* vel, float* out, float dt, 
 void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags);
 void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint64_t* out);
 
+// HNS_Advance over the context's fields (hns_advance.cu).
+void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& params);
+
 // Runs `iterations` fused RBGS iterations from `p` (or zero) and leaves the result in `p`.
 void rbgs_solve(Context& c, const float* div, float* p, int iterations, float omega, unsigned flags);
 
@@ -155,13 +194,7 @@ void rbgs_solve(Context& c, const float* div, float* p, int iterations, float om
 // FP64 residual of the iterate is evaluated inside the sweep every `check_every` iterations
 // and the remaining launches return at once when ||r|| <= tol ||b||. Enqueues only; the
 // check slots (2 doubles per check, from c.reduce_slots) are read by solve_result().
-struct SolvePlan {
-    int max_iterations = 0;
-    int check_every = 0;
-    int num_checks = 0;
-    double tol = 0.0;
-    double* slots = nullptr;
-};
+
 SolvePlan rbgs_solve_checked(Context& c, const float* div, float* p, int max_iterations, float omega, unsigned flags,
                              double tol, int check_every);
 // Host readback (synchronizes): iterations run and the last evaluated relative residual.

@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
                                                                    const float* __restrict__ p_in,
                                                                    float* __restrict__ p_out, float dx2, float omega,
                                                                    const double* __restrict__ check, double tol2,
-                                                                   double* __restrict__ resid_out) {
+                                                                   double* __restrict__ resid_out,
+                                                                   unsigned long long* __restrict__ executed) {
     __shared__ float sp[PT * PT * PT];
     __shared__ float sb[RT * RT * RT];
     __shared__ int nb[27];
@@ -189,6 +190,7 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
     if (check != nullptr && check[0] <= tol2 * check[1]) return;
     const int64_t leaf = blockIdx.x;
     const int tid = threadIdx.x;
+    if (executed != nullptr && leaf == 0 && tid == 0) atomicAdd(executed, 1ull);
     if (tid < 27) nb[tid] = __ldg(t.nbr27 + leaf * 27 + tid);
     __syncthreads();
     for (int c = tid; c < PT * PT * PT; c += kThreads) {
@@ -394,7 +396,7 @@ void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in
                            unsigned flags, const double* check, double tol2, double* resid_out) {
     if (flags & HNS_SOLVE_NEUMANN) fail(HNS_ERR_UNSUPPORTED, "Neumann walls are not supported by this solver build");
     rbgs_iteration_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
-        c.topo.view, div, p_in, p_out, c.dx * c.dx, omega, check, tol2, resid_out);
+        c.topo.view, div, p_in, p_out, c.dx * c.dx, omega, check, tol2, resid_out, c.counters);
     HNS_LAUNCHED();
 }
 

@@ -39,6 +39,32 @@ class SolveInfo(ctypes.Structure):
     _fields_ = [("iterations", _i), ("residual", ctypes.c_double), ("initial_residual", ctypes.c_double)]
 
 
+class StepDesc(ctypes.Structure):
+    _fields_ = [("dt", _f), ("max_iterations", _i), ("omega", _f), ("tolerance", ctypes.c_double),
+                ("check_every", _i), ("flags", _u)]
+
+
+class CombustionParams(ctypes.Structure):
+    """hns_combustion_params: the layout of the reference's CombustionParams."""
+
+    _fields_ = [
+        ("expansionRate", _f), ("temperatureRelease", _f), ("buoyancyStrength", _f), ("ambientTemp", _f),
+        ("vorticityScale", _f), ("factorScale", _f), ("disturbanceEnable", _f), ("disturbanceStrength", _f),
+        ("disturbanceSwirl", _f), ("disturbanceThreshold", _f), ("disturbanceGain", _f),
+        ("disturbanceFrequency", _f), ("substeps", _i), ("gravity", _f), ("maskDensityMin", _f),
+        ("maskDensityMax", _f), ("downloadVel", _i), ("simReset", _i),
+    ]
+
+
+NUM_PHASES = 8
+PHASES = {"advect": 0, "divergence": 1, "solve": 2, "gradient": 3, "forces": 4}
+
+
+class ProfileData(ctypes.Structure):
+    _fields_ = [("phase_ms", ctypes.c_double * NUM_PHASES), ("phase_count", _i * NUM_PHASES),
+                ("solver_launches", ctypes.c_ulonglong)]
+
+
 def _sig(lib, name, res, *args):
     fn = getattr(lib, name)
     fn.restype = res
@@ -73,6 +99,19 @@ def _load():
     _sig(lib, "hns_subtract_gradient", _i, _p, _p, _p, _p)
     _sig(lib, "hns_vorticity_confinement", _i, _p, _p, _p, _f, _f, _f)
     _sig(lib, "hns_project", _i, _p, _p, _i, _f, _u, ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_step_plain", _i, _p, _p, _p, _p, _p, _i, ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_step_plain_host", _i, _p, _p, _p, _i, ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_last_solve", _i, _p, ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_field_set", _i, _p, ctypes.c_char_p, _i, _p, _i)
+    _sig(lib, "hns_field_get", _i, _p, ctypes.c_char_p, _p, _i)
+    _sig(lib, "hns_field_ptr", _i, _p, ctypes.c_char_p, ctypes.POINTER(_p), ctypes.POINTER(_i))
+    _sig(lib, "hns_field_remove", _i, _p, ctypes.c_char_p)
+    _sig(lib, "hns_field_count", _i, _p)
+    _sig(lib, "hns_field_info", _i, _p, _i, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_i))
+    _sig(lib, "hns_advance", _i, _p, _i, _f, ctypes.POINTER(CombustionParams))
+    _sig(lib, "hns_active_mask", _i, _p, _p)
+    _sig(lib, "hns_profile_enable", _i, _p, _i)
+    _sig(lib, "hns_profile_read", _i, _p, ctypes.POINTER(ProfileData))
     return lib
 
 
@@ -181,3 +220,73 @@ class Grid:
         si = SolveInfo()
         check(lib.hns_project(self._h, _dptr(vel), iterations, omega, flags, ctypes.byref(si) if info else None))
         return si if info else None
+
+    # ---- steps ----
+    def step_plain(self, vel_in, vel_out, scalars_in, scalars_out, desc: StepDesc, info=False):
+        n = len(scalars_in)
+        pin = (_p * max(1, n))(*[_dptr(t) for t in scalars_in])
+        pout = (_p * max(1, n))(*[_dptr(t) for t in scalars_out])
+        si = SolveInfo()
+        check(lib.hns_step_plain(self._h, _dptr(vel_in), _dptr(vel_out), pin, pout, n, ctypes.byref(desc),
+                                 ctypes.byref(si) if info else None))
+        return si if info else None
+
+    def step_plain_host(self, vel: np.ndarray, scalars, desc: StepDesc, info=False):
+        """vel (N,3) float32 and scalars (N,) float32 host arrays, updated in place."""
+        for a in [vel, *scalars]:
+            if a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("host fields must be contiguous float32")
+        ptrs = (_p * max(1, len(scalars)))(*[a.ctypes.data for a in scalars])
+        si = SolveInfo()
+        check(lib.hns_step_plain_host(self._h, vel.ctypes.data, ptrs, len(scalars), ctypes.byref(desc),
+                                      ctypes.byref(si) if info else None))
+        return si if info else None
+
+    def last_solve(self) -> SolveInfo:
+        si = SolveInfo()
+        check(lib.hns_last_solve(self._h, ctypes.byref(si)))
+        return si
+
+    def profile_enable(self, on: bool = True):
+        check(lib.hns_profile_enable(self._h, 1 if on else 0))
+
+    def profile_read(self) -> ProfileData:
+        d = ProfileData()
+        check(lib.hns_profile_read(self._h, ctypes.byref(d)))
+        return d
+
+    # ---- named fields and the all-in-one step ----
+    def field_set(self, name: str, data: np.ndarray | None = None, components: int | None = None):
+        """Host numpy data ((N,) or (N,3) float32) or None for a zero field."""
+        if data is not None:
+            data = np.ascontiguousarray(data, dtype=np.float32)
+            components = 3 if data.ndim == 2 else 1
+        check(lib.hns_field_set(self._h, name.encode(), components or 1,
+                                None if data is None else data.ctypes.data, 0))
+
+    def field_get(self, name: str) -> np.ndarray:
+        ptr, comps = _p(), _i()
+        check(lib.hns_field_ptr(self._h, name.encode(), ctypes.byref(ptr), ctypes.byref(comps)))
+        out = np.zeros((self.num_voxels, 3) if comps.value == 3 else self.num_voxels, np.float32)
+        check(lib.hns_field_get(self._h, name.encode(), out.ctypes.data, 0))
+        return out
+
+    def field_names(self):
+        out = []
+        buf = ctypes.create_string_buffer(256)
+        comps = _i()
+        for q in range(lib.hns_field_count(self._h)):
+            check(lib.hns_field_info(self._h, q, buf, 256, ctypes.byref(comps)))
+            out.append(buf.value.decode())
+        return out
+
+    def field_remove(self, name: str):
+        check(lib.hns_field_remove(self._h, name.encode()))
+
+    def advance(self, iterations: int, dt: float, params: CombustionParams):
+        check(lib.hns_advance(self._h, iterations, dt, ctypes.byref(params)))
+
+    def active_mask(self) -> np.ndarray:
+        out = np.zeros(self.num_voxels, np.uint8)
+        check(lib.hns_active_mask(self._h, out.ctypes.data))
+        return out

@@ -134,6 +134,110 @@ typedef struct hns_solve_info {
 HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float omega, unsigned flags,
                                hns_solve_info* info);
 
+/* ---- one solver step ------------------------------------------------------------------- */
+
+typedef struct hns_step_desc {
+    float dt;
+    int max_iterations; /* red-black iteration cap (rounded up to even when tolerance > 0) */
+    float omega;        /* SOR factor; <= 0 selects 2/(1+sin(3.14159 dx)) */
+    double tolerance;   /* target ||b - A p|| / ||b|| (FP64); 0 runs exactly max_iterations */
+    int check_every;    /* iterations between residual checks (rounded up to even; 0 = 10) */
+    unsigned flags;     /* HNS_SOLVE_* (HNS_SOLVE_ZERO_INIT is implied) */
+} hns_step_desc;
+
+/* One step of the SOP operator chain HNanoAdvect + HNanoAdvectVelocity +
+ * HNanoProjectNonDivergent (src/SOP/Advection/SOP_VDBAdvect.hpp:66,
+ * src/SOP/VelocityAdvection/SOP_VDBAdvectVelocity.hpp:60,
+ * src/SOP/ProjectNonDivergent/SOP_VDBProjectNonDivergent.hpp:69): vel_in and every
+ * scalars_in[i] are advected along the same MacCormack trace into vel_out / scalars_out[i]
+ * (advect_vector and advect_scalar semantics), then vel_out is projected in place. The
+ * solve starts from p = 0 and, with a tolerance, stops on the device once the residual
+ * test passes. Device pointers; scalars_in/out are host arrays of device pointers.
+ * info may be NULL (no synchronization); with info the call synchronizes, reports the
+ * exact FP64 residual and returns HNS_ERR_NOT_CONVERGED if the tolerance was not met. */
+HNS_API hns_status hns_step_plain(hns_ctx* ctx, const float* vel_in, float* vel_out, const float* const* scalars_in,
+                                  float* const* scalars_out, int nscalars, const hns_step_desc* desc,
+                                  hns_solve_info* info);
+/* hns_step_plain on HOST buffers updated in place (uploads, step, downloads; synchronous):
+ * the host-memory form of the SOP-facing operators. */
+HNS_API hns_status hns_step_plain_host(hns_ctx* ctx, float* vel, float* const* scalars, int nscalars,
+                                       const hns_step_desc* desc, hns_solve_info* info);
+/* Iterations and last checked residual of the most recent convergence-checked solve
+ * (synchronizes). residual is -1 when that solve ran without a tolerance. */
+HNS_API hns_status hns_last_solve(hns_ctx* ctx, hns_solve_info* info);
+
+/* ---- named fields and the all-in-one step -----------------------------------------------
+ * The context keeps named device fields, as the reference's SimContext keeps d_state and
+ * d_src (src/Cuda/HNanoSolver.cu:27-48): "velocity" (3 components), persistent scalars,
+ * sources named "src_*" (src_vel or src_vel_x/y/z, src_temperature, src_density,
+ * src_fuel). Fields live across calls; the simulation state stays on the device. */
+
+/* Creates or overwrites a field from `data` (host, or device if on_device); data NULL
+ * creates a zero field. components: 1 or 3. Host uploads complete before return. */
+HNS_API hns_status hns_field_set(hns_ctx* ctx, const char* name, int components, const float* data, int on_device);
+/* Copies a field to `out` (host, or device if on_device); host copies complete before return. */
+HNS_API hns_status hns_field_get(hns_ctx* ctx, const char* name, float* out, int on_device);
+/* Device pointer of a field (valid until the field is removed or the next hns_advance). */
+HNS_API hns_status hns_field_ptr(hns_ctx* ctx, const char* name, float** dev_ptr, int* components);
+HNS_API hns_status hns_field_remove(hns_ctx* ctx, const char* name);
+HNS_API int hns_field_count(const hns_ctx* ctx);
+/* Name (truncated to name_len-1 chars) and component count of field `index`. */
+HNS_API hns_status hns_field_info(const hns_ctx* ctx, int index, char* name, size_t name_len, int* components);
+
+/* Parameters of the all-in-one step; same layout as the reference's CombustionParams
+ * (src/Cuda/Kernels.cuh:5-24). */
+typedef struct hns_combustion_params {
+    float expansionRate;
+    float temperatureRelease;
+    float buoyancyStrength;
+    float ambientTemp;
+    float vorticityScale;
+    float factorScale;
+    float disturbanceEnable;
+    float disturbanceStrength;
+    float disturbanceSwirl;
+    float disturbanceThreshold;
+    float disturbanceGain;
+    float disturbanceFrequency;
+    int substeps;
+    float gravity;
+    float maskDensityMin;
+    float maskDensityMax;
+    int downloadVel;
+    int simReset;
+} hns_combustion_params;
+
+/* HNS_Advance (src/Cuda/HNanoSolver.cu:223-456) on the context's fields, without collision:
+ * per substep advect the velocity, vorticity confinement (out of place), velocity and scalar
+ * sources, gravity, divergence, oxygen combustion, buoyancy, `iterations` red-black
+ * iterations from p = 0 with omega = 2/(1+sin(3.14159 dx)), the re-solve of the reference's
+ * disturbance branch when disturbanceEnable > 0, gradient subtraction, and advection of the
+ * scalars present at the call's start with the projected velocity. fuel, waste, temperature
+ * and flame are created zero-filled when missing. */
+HNS_API hns_status hns_advance(hns_ctx* ctx, int iterations, float dt, const hns_combustion_params* params);
+/* host uint8[num_voxels]: the activity mask of the last step (the reference's
+ * build_activity_mask marks every slot active, src/Cuda/Kernel.cu:75). */
+HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out);
+
+/* ---- profiling --------------------------------------------------------------------------
+ * While enabled, the step entry points record CUDA events on the context's stream around
+ * each phase; hns_profile_read sums them (synchronizes) and resets. */
+#define HNS_PHASE_ADVECT 0
+#define HNS_PHASE_DIVERGENCE 1
+#define HNS_PHASE_SOLVE 2
+#define HNS_PHASE_GRADIENT 3
+#define HNS_PHASE_FORCES 4
+#define HNS_NUM_PHASES 8
+
+typedef struct hns_profile_data {
+    double phase_ms[HNS_NUM_PHASES];        /* device time per phase since the last read */
+    int phase_count[HNS_NUM_PHASES];        /* phase executions since the last read */
+    unsigned long long solver_launches;     /* red-black launches that ran (not skipped) */
+} hns_profile_data;
+
+HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable);
+HNS_API hns_status hns_profile_read(hns_ctx* ctx, hns_profile_data* out);
+
 #ifdef __cplusplus
 }
 #endif

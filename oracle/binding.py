@@ -287,6 +287,7 @@ class RefOracle:
         _sig(lib, "ref_project", None, _p, _p, _i64, _p, _p, _p, _f, _i, _f)
         _sig(lib, "ref_hns_advance", None, _p, _p, ctypes.POINTER(AdvanceFields), _f, _i, _f,
              ctypes.POINTER(CombustionParams))
+        _sig(lib, "ref_plain_step", None, _p, _p, _i64, _p, _p, _i, _f, _f, _i, _f, _p)
 
     def grid(self, coords) -> "RefGrid":
         return RefGrid(self, coords)
@@ -389,6 +390,15 @@ class RefGrid:
         p = np.zeros(self.n, np.float32)
         self.lib.ref_project(self.h, ptr(self.coords), self.n, ptr(vel), ptr(div), ptr(p), dx, iterations, omega)
         return vel, div, p
+
+    def plain_step(self, vel, scalars, dt, dx, iterations, omega, scratch=None):
+        """In place on vel (N,3) and the scalar arrays; returns the scratch buffer for reuse."""
+        if scratch is None:
+            scratch = np.zeros(5 * self.n, np.float32)
+        ptrs = (_p * max(1, len(scalars)))(*[a.ctypes.data for a in scalars])
+        self.lib.ref_plain_step(self.h, ptr(self.coords), self.n, ptr(vel), ptrs, len(scalars), dt, dx, iterations,
+                                omega, ptr(scratch))
+        return scratch
 
     def hns_advance(self, velocity, scalars: dict, sources: dict, dx, iteration, dt, params: CombustionParams):
         vel = np.ascontiguousarray(velocity, dtype=np.float32).copy()

@@ -251,6 +251,34 @@ void ref_project(void* g, const int32_t* coords, int64_t n, float* vel, float* d
     ref_subtract_gradient(g, coords, n, tmp.data(), p, vel, inv_dx);
 }
 
+// One step of the SOP operator chain HNanoAdvect + HNanoAdvectVelocity +
+// HNanoProjectNonDivergent with the reference's kernels (the SOP bodies are commented out in
+// the reference, src/Cuda/Advection.cu:13-166 and src/Cuda/PressureProjection.cu:9-78): the
+// scalars and the velocity are advected with the old velocity, then the velocity is
+// projected with `iterations` red-black sweeps from p = 0. `scratch` holds 5n floats.
+// With a block stride > 1 (ref_set_block_stride) every launch runs a subset of its blocks:
+// the timed CPU baseline's bounded sample.
+void ref_plain_step(void* g, const int32_t* coords, int64_t n, float* vel, float* const* scalars, int nscalars, float dt,
+                    float dx, int iterations, float omega, float* scratch) {
+    const IndexGrid* grid = static_cast<RefGrid*>(g)->grid;
+    const float inv_dx = 1.0f / dx;
+    float* adv = scratch;          // 3n
+    float* div = scratch + 3 * n;  // n
+    float* p = scratch + 4 * n;    // n
+    std::vector<float> tmp(nscalars > 0 ? n : 0);
+    for (int q = 0; q < nscalars; ++q) {
+        float* in = scalars[q];
+        float* out = tmp.data();
+        launch(n, [&] { advect_scalar(grid, C(coords), V(vel), in, out, nullptr, false, (size_t)n, dt, inv_dx, nullptr); });
+        std::copy(tmp.begin(), tmp.end(), in);
+    }
+    launch(n, [&] { advect_vector(grid, C(coords), V(vel), V(adv), nullptr, false, nullptr, (size_t)n, dt, inv_dx); });
+    launch(n, [&] { divergence(grid, C(coords), V(adv), div, inv_dx, nullptr, (size_t)n); });
+    std::fill(p, p + n, 0.0f);
+    ref_rbgs(g, coords, n, div, p, dx, iterations, omega);
+    launch(n, [&] { subtractPressureGradient(grid, C(coords), (size_t)n, V(adv), p, V(vel), nullptr, false, inv_dx, nullptr); });
+}
+
 // Field set for the HNS_Advance restatement. `names`/`scalars` are the persistent scalar
 // fields present when the call starts (the context's d_state, HNanoSolver.cu:113-119):
 // exactly these are advected (advNames is taken before the substep loop, :247-250).
