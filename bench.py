@@ -38,7 +38,7 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "shell512": dict(desc="512^3 box, 16-voxel band (+ leaf half-diagonal) around a seeded radius-200 sphere, "
                           "fields: value-noise density, value-noise velocity in (-1,1)",
-                     dx=0.1, dt=0.1, omega=1.9, tolerance=1e-5, cap=2000, check_every=10, fp32_iterations=None),
+                     dx=0.1, dt=0.1, omega=1.8, tolerance=1e-5, cap=3000, check_every=10, fp32_iterations=800),
     "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60",
                      dx=0.1, dt=1.0 / 24.0, omega=1.9, tolerance=1e-5, cap=2000, check_every=10, fp32_iterations=None),
     "box64": dict(desc="64^3 box fully active (512 leaves)", dx=0.1, dt=0.1, omega=1.0, tolerance=0.0, cap=40,
@@ -146,7 +146,7 @@ def reference_arm(args, wl):
     iters = wl["fp32_iterations"] or 200
     n = len(dens)
     blocks = (n + 255) // 256
-    stride = max(1, blocks // 4096)
+    stride = max(1, blocks // 2048)
     ref.lib.ref_set_block_stride(stride)
     scratch = None
     for _ in range(args.warmup):
@@ -185,7 +185,7 @@ def cpu_baseline(args, wl, iters):
     g = ref.grid(synth.leaf_dense_coords(origins))
     n = len(dens)
     blocks = (n + 255) // 256
-    stride = max(1, blocks // 4096)
+    stride = max(1, blocks // 2048)
     ref.lib.ref_set_block_stride(stride)
     scratch = g.plain_step(vel, [dens], wl["dt"], wl["dx"], iters, wl["omega"])
     reps, t0 = 0, time.perf_counter()
@@ -233,7 +233,12 @@ def ours(args, wl):
 
     # Iterations the solve needs on this grid: one checked solve, then a cap with a margin
     # of two check periods so that few launches are skipped at the end of each solve.
-    info = g.step_plain(v[0], v[1], [d[0]], [d[1]], desc(wl["cap"]), info=True)
+    try:
+        info = g.step_plain(v[0], v[1], [d[0]], [d[1]], desc(wl["cap"]), info=True)
+    except hl.HnsError as e:
+        if e.status != 6:  # HNS_ERR_NOT_CONVERGED: the FP32 floor; keep the cap
+            raise
+        info = g.last_solve()
     need = info.iterations
     cap = need if wl["tolerance"] == 0 else need + 2 * max(2, wl["check_every"])
     st = desc(cap)
@@ -317,7 +322,7 @@ def ours(args, wl):
                        "l2": "inputs larger than L2 (state %.0f MB per GPU)" % ((16 * 2 + 8) * n / 1e6),
                        "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                        "phase_ms_per_step": phase_ms},
-            "roofline": {"kernel": "rbgs_iteration_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"kernel": "rbgs_bulk_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": RBGS_BYTES_PER_VOXEL * n, "launch_ms": rbgs_ms,
                          "launches_timed": int(prof.solver_launches)},

@@ -380,6 +380,34 @@ HNS_API int64_t hns_num_voxels(const hns_ctx* ctx) { return ctx ? ctx->impl.num_
 HNS_API int64_t hns_num_leaves(const hns_ctx* ctx) { return ctx ? ctx->impl.topo.num_leaves : 0; }
 HNS_API float hns_voxel_size(const hns_ctx* ctx) { return ctx ? ctx->impl.dx : 0.f; }
 
+HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (option == HNS_OPT_RBGS_KERNEL) {
+            if (value != HNS_RBGS_PLAIN && value != HNS_RBGS_BULK) fail(HNS_ERR_INVALID_ARG, "unknown red-black kernel");
+            c->rbgs_kernel = value;
+        } else {
+            fail(HNS_ERR_INVALID_ARG, "unknown option");
+        }
+    });
+}
+
+HNS_API hns_status hns_device_status(hns_ctx* ctx) {
+    unsigned long long flag = 0;
+    const hns_status s = guarded([&] {
+        Context* c = check_ctx(ctx);
+        DeviceGuard g(c->device);
+        HNS_CUDA(cudaStreamSynchronize(c->stream));
+        HNS_CUDA(cudaMemcpy(&flag, c->counters + 1, sizeof(flag), cudaMemcpyDeviceToHost));
+        if (flag) {
+            HNS_CUDA(cudaMemsetAsync(c->counters + 1, 0, sizeof(flag), c->stream));
+            HNS_CUDA(cudaStreamSynchronize(c->stream));
+        }
+    });
+    if (s != HNS_OK) return s;
+    return flag ? record_error(HNS_ERR_TIMEOUT, "a device-side wait gave up (bulk copy did not complete)") : HNS_OK;
+}
+
 HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable) {
     return guarded([&] {
         Context* c = check_ctx(ctx);

@@ -132,6 +132,7 @@ struct Context {
     DeviceBuffer d_counters;
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
+    int rbgs_kernel = HNS_RBGS_BULK;  // hns_set_option(HNS_OPT_RBGS_KERNEL)
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -178,6 +179,10 @@ void launch_divergence(const Context& c, const float* vel, float* div);
 void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in, float* p_out, float omega,
                            unsigned flags, const double* check = nullptr, double tol2 = 0.0,
                            double* resid_out = nullptr);
+// The bulk-copy form of the iteration (hns_rbgs.cu); needs 16-byte aligned arrays.
+bool rbgs_bulk_eligible(const float* div, const float* p_in, const float* p_out);
+void launch_rbgs_bulk(const Context& c, const float* div, const float* p_in, float* p_out, float omega,
+                      const double* check, double tol2, double* resid_out);
 void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out);
 void launch_vorticity(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale);
 // acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).

@@ -395,6 +395,10 @@ void launch_divergence(const Context& c, const float* vel, float* div) {
 void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in, float* p_out, float omega,
                            unsigned flags, const double* check, double tol2, double* resid_out) {
     if (flags & HNS_SOLVE_NEUMANN) fail(HNS_ERR_UNSUPPORTED, "Neumann walls are not supported by this solver build");
+    if (c.rbgs_kernel == HNS_RBGS_BULK && rbgs_bulk_eligible(div, p_in, p_out)) {
+        launch_rbgs_bulk(c, div, p_in, p_out, omega, check, tol2, resid_out);
+        return;
+    }
     rbgs_iteration_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
         c.topo.view, div, p_in, p_out, c.dx * c.dx, omega, check, tol2, resid_out, c.counters);
     HNS_LAUNCHED();

@@ -59,10 +59,12 @@ std::string single_velocity_block(const HNS::GridIndexedData& data) {
 // build their grid on every call, as the reference's did).
 struct ScopedCtx {
     hns_ctx* c = nullptr;
+    cudaStream_t s = nullptr;  // the stream every copy and kernel of the call goes on
     ScopedCtx(const HNS::GridIndexedData& data, float voxelSize, cudaStream_t stream) {
         const std::vector<int32_t> o = leaves_of(data);
         ok(hns_create(&c, o.data(), (int64_t)o.size() / 3, voxelSize, current_device()), "create");
         if (stream) ok(hns_set_stream(c, stream), "set_stream");
+        s = static_cast<cudaStream_t>(hns_get_stream(c));
     }
     ~ScopedCtx() {
         if (c) (void)hns_destroy(c);
@@ -235,12 +237,12 @@ HNS_API void AdvectIndexGrid(HNS::GridIndexedData& data, float dt, float voxelSi
     const size_t n = data.size();
     ScopedCtx c(data, voxelSize, stream);
     DevArray dv(3 * n), din(n), dout(n);
-    upload(dv.p, data.pValues<HNS::Vec3f>(vel), 3 * n, stream);
+    upload(dv.p, data.pValues<HNS::Vec3f>(vel), 3 * n, c.s);
     for (const auto& name : floats) {
         float* h = data.pValues<float>(name);
-        upload(din.p, h, n, stream);
+        upload(din.p, h, n, c.s);
         ok(hns_advect_scalar(c.c, dv.p, din.p, dout.p, dt), "AdvectIndexGrid");
-        download(h, dout.p, n, stream);
+        download(h, dout.p, n, c.s);
     }
     ok(hns_synchronize(c.c), "AdvectIndexGrid");
 }
@@ -251,9 +253,9 @@ HNS_API void AdvectIndexGridVelocity(HNS::GridIndexedData& data, float dt, float
     ScopedCtx c(data, voxelSize, stream);
     DevArray dv(3 * n), dout(3 * n);
     float* h = reinterpret_cast<float*>(data.pValues<HNS::Vec3f>(vel));
-    upload(dv.p, h, 3 * n, stream);
+    upload(dv.p, h, 3 * n, c.s);
     ok(hns_advect_vec3(c.c, dv.p, dout.p, dt), "AdvectIndexGridVelocity");
-    download(h, dout.p, 3 * n, stream);
+    download(h, dout.p, 3 * n, c.s);
     ok(hns_synchronize(c.c), "AdvectIndexGridVelocity");
 }
 
@@ -263,9 +265,9 @@ HNS_API void ProjectNonDivergent(HNS::GridIndexedData& data, size_t iteration, f
     ScopedCtx c(data, voxelSize, stream);
     DevArray dv(3 * n);
     float* h = reinterpret_cast<float*>(data.pValues<HNS::Vec3f>(vel));
-    upload(dv.p, h, 3 * n, stream);
+    upload(dv.p, h, 3 * n, c.s);
     ok(hns_project(c.c, dv.p, (int)iteration, -1.0f, 0u, nullptr), "ProjectNonDivergent");
-    download(h, dv.p, 3 * n, stream);
+    download(h, dv.p, 3 * n, c.s);
     ok(hns_synchronize(c.c), "ProjectNonDivergent");
 }
 
@@ -276,9 +278,9 @@ HNS_API void Divergence(HNS::GridIndexedData& data, float voxelSize, const cudaS
     const size_t n = data.size();
     ScopedCtx c(data, voxelSize, stream);
     DevArray dv(3 * n), dd(n);
-    upload(dv.p, data.pValues<HNS::Vec3f>(vel), 3 * n, stream);
+    upload(dv.p, data.pValues<HNS::Vec3f>(vel), 3 * n, c.s);
     ok(hns_divergence(c.c, dv.p, dd.p), "Divergence");
-    download(hdiv, dd.p, n, stream);
+    download(hdiv, dd.p, n, c.s);
     ok(hns_synchronize(c.c), "Divergence");
 }
 

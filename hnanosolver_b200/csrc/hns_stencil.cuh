@@ -71,7 +71,9 @@ __device__ __forceinline__ float3 near_v(const TopoView& t, const LeafNbhd& L, c
     return s < 0 ? make_float3(0.f, 0.f, 0.f) : ld3(d, s);
 }
 
-__device__ __forceinline__ float lerp1(float a, float b, float w) { return fmaf(w, b - a, a); }
+// a + w (b - a), rounded after each operation (the reference's sampler lerp,
+// src/Utils/Stencils.hpp:137-140; the library is built without implicit FMA contraction).
+__device__ __forceinline__ float lerp1(float a, float b, float w) { return a + w * (b - a); }
 
 // Trilinear sample, 0 outside the domain: floor, fractional part, lerp along z, then y,
 // then x (TrilinearSampler::sample, src/Utils/Stencils.hpp:118-153).

@@ -19,6 +19,8 @@ STATUS_NAMES = {
     0: "HNS_OK", 1: "HNS_ERR_INVALID_ARG", 2: "HNS_ERR_CUDA", 3: "HNS_ERR_OUT_OF_MEMORY", 4: "HNS_ERR_NOT_FOUND",
     5: "HNS_ERR_LAYOUT", 6: "HNS_ERR_NOT_CONVERGED", 7: "HNS_ERR_UNSUPPORTED", 8: "HNS_ERR_TIMEOUT",
 }
+OPT_RBGS_KERNEL = 1
+RBGS_PLAIN, RBGS_BULK = 0, 1
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 
@@ -110,6 +112,8 @@ def _load():
     _sig(lib, "hns_field_info", _i, _p, _i, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_i))
     _sig(lib, "hns_advance", _i, _p, _i, _f, ctypes.POINTER(CombustionParams))
     _sig(lib, "hns_active_mask", _i, _p, _p)
+    _sig(lib, "hns_set_option", _i, _p, _i, _i)
+    _sig(lib, "hns_device_status", _i, _p)
     _sig(lib, "hns_profile_enable", _i, _p, _i)
     _sig(lib, "hns_profile_read", _i, _p, ctypes.POINTER(ProfileData))
     return lib
@@ -290,3 +294,9 @@ class Grid:
         out = np.zeros(self.num_voxels, np.uint8)
         check(lib.hns_active_mask(self._h, out.ctypes.data))
         return out
+
+    def set_option(self, option: int, value: int):
+        check(lib.hns_set_option(self._h, option, value))
+
+    def device_status(self):
+        check(lib.hns_device_status(self._h))

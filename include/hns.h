@@ -219,6 +219,16 @@ HNS_API hns_status hns_advance(hns_ctx* ctx, int iterations, float dt, const hns
  * build_activity_mask marks every slot active, src/Cuda/Kernel.cu:75). */
 HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out);
 
+/* ---- options ----------------------------------------------------------------------------- */
+#define HNS_OPT_RBGS_KERNEL 1 /* which red-black kernel: */
+#define HNS_RBGS_PLAIN 0      /*   plain loads into a padded halo tile */
+#define HNS_RBGS_BULK 1       /*   bulk async copies of the contiguous leaf payload (default;
+                                   used when div and p are 16-byte aligned) */
+HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
+/* Device-side error flags raised since the last call (bounded waits that gave up): returns
+ * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */
+HNS_API hns_status hns_device_status(hns_ctx* ctx);
+
 /* ---- profiling --------------------------------------------------------------------------
  * While enabled, the step entry points record CUDA events on the context's stream around
  * each phase; hns_profile_read sums them (synchronizes) and resets. */

@@ -49,3 +49,7 @@ def rel_err(got, ref) -> float:
     ref = np.asarray(ref, dtype=np.float64)
     scale = float(np.max(np.abs(ref))) if ref.size else 0.0
     return float(np.max(np.abs(got - ref)) / max(scale, 1e-30)) if ref.size else 0.0
+
+
+def bit_exact(got, ref) -> bool:
+    return np.array_equal(np.asarray(got), np.asarray(ref))

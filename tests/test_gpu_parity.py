@@ -149,3 +149,36 @@ def test_project(case, dev):
     assert info.iterations == 25
     assert info.residual == pytest.approx(np.sqrt(r2 / b2), rel=1e-3)
     assert info.initial_residual == pytest.approx(1.0, rel=1e-9)
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("iters,zero", [(1, True), (6, False), (11, True)])
+def test_rbgs_kernels_bit_exact(case, dev, kernel, iters, zero):
+    """Both red-black kernels (plain-load halo tile, bulk async copies) equal the oracle."""
+    from conftest import bit_exact
+    from hnanosolver_b200 import lib as hl
+
+    g, t = case["grid"], case["topo"]
+    g.set_option(hl.OPT_RBGS_KERNEL, kernel)
+    div = t.divergence(case["vel"], 10.0)
+    p0 = np.zeros_like(div) if zero else (case["dens"] * 0.01).astype(np.float32)
+    p = T(p0, dev)
+    g.rbgs(T(div, dev), p, iters, 1.8, hl.SOLVE_ZERO_INIT if zero else 0)
+    g.device_status()
+    assert bit_exact(H(p), t.rbgs(div, p0, 0.1, iters, 1.8))
+    g.set_option(hl.OPT_RBGS_KERNEL, hl.RBGS_BULK)
+
+
+def test_rbgs_unaligned_pointers_fall_back(case, dev):
+    from conftest import bit_exact
+
+    g, t = case["grid"], case["topo"]
+    n = len(case["dens"])
+    div = t.divergence(case["vel"], 10.0)
+    buf = torch.zeros(2 * n + 8, device=dev)
+    dv = buf[1:n + 1]          # 4-byte offset: not 16-byte aligned
+    dv.copy_(T(div, dev))
+    p = buf[n + 3:2 * n + 3]
+    g.rbgs(dv, p, 5, 1.6, 1)
+    g.device_status()
+    assert bit_exact(H(p), t.rbgs(div, np.zeros_like(div), 0.1, 5, 1.6))

@@ -90,7 +90,7 @@ def test_convergence_stop_equals_fixed_iterations(dev, check_every):
     info_b = g.step_plain(v_in, v_b, [d_in], [d_b], _desc(max_iterations=info.iterations, omega=1.8), info=True)
     torch.cuda.synchronize()
     assert torch.equal(v_a, v_b)
-    assert info.residual == info_b.residual
+    assert info.residual == pytest.approx(info_b.residual, rel=1e-9)  # FP64 atomics: summation order varies
     assert info.residual <= 1e-4
     g.close()
 
