@@ -133,6 +133,7 @@ struct Context {
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
     int rbgs_kernel = HNS_RBGS_BULK;  // hns_set_option(HNS_OPT_RBGS_KERNEL)
+    int rbgs_threads = 128;           // hns_set_option(HNS_OPT_RBGS_THREADS): 128 or 256 per CTA
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;

@@ -103,7 +103,7 @@ int main(int argc, char** argv) {
         sop.addValueBlock<float>("divergence", sop.size());
         cudaStream_t stream = nullptr;
         Divergence(sop, 0.1f, stream);
-        dump(std::string("sop_divergence.f32"), sop.pValues<float>("divergence"), sop.size() * 4);
+        dump(std::string("sopdiv_divergence.f32"), sop.pValues<float>("divergence"), sop.size() * 4);
         AdvectIndexGrid(sop, 0.1f, 0.1f, stream);  // also advects "divergence": every float block
         AdvectIndexGridVelocity(sop, 0.1f, 0.1f, stream);
         ProjectNonDivergent(sop, 20, 0.1f, stream);
