@@ -386,9 +386,6 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
         if (option == HNS_OPT_RBGS_KERNEL) {
             if (value != HNS_RBGS_PLAIN && value != HNS_RBGS_BULK) fail(HNS_ERR_INVALID_ARG, "unknown red-black kernel");
             c->rbgs_kernel = value;
-        } else if (option == HNS_OPT_RBGS_THREADS) {
-            if (value != 128 && value != 256) fail(HNS_ERR_INVALID_ARG, "red-black CTA size must be 128 or 256");
-            c->rbgs_threads = value;
         } else {
             fail(HNS_ERR_INVALID_ARG, "unknown option");
         }

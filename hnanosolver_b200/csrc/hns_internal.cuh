@@ -133,7 +133,6 @@ struct Context {
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
     int rbgs_kernel = HNS_RBGS_BULK;  // hns_set_option(HNS_OPT_RBGS_KERNEL)
-    int rbgs_threads = 128;           // hns_set_option(HNS_OPT_RBGS_THREADS): 128 or 256 per CTA
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -184,6 +183,10 @@ void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in
 bool rbgs_bulk_eligible(const float* div, const float* p_in, const float* p_out);
 void launch_rbgs_bulk(const Context& c, const float* div, const float* p_in, float* p_out, float omega,
                       const double* check, double tol2, double* resid_out);
+// The same iteration on FP16 storage (FP32 arithmetic) with unit dx^2: the inner solve of the
+// mixed-precision refinement, L e = rhs. e_in null means e = 0.
+void launch_rbgs_bulk_half(const Context& c, const void* rhs, const void* e_in, void* e_out, float omega,
+                           const double* check, double tol2);
 void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out);
 void launch_vorticity(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale);
 // acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).

@@ -224,7 +224,6 @@ HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out);
 #define HNS_RBGS_PLAIN 0      /*   plain loads into a padded halo tile */
 #define HNS_RBGS_BULK 1       /*   bulk async copies of the contiguous leaf payload (default;
                                    used when div and p are 16-byte aligned) */
-#define HNS_OPT_RBGS_THREADS 2 /* threads per CTA of the bulk red-black kernel: 128 (default) or 256 */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */
