@@ -105,6 +105,16 @@ struct Field {
     DeviceBuffer buf;
 };
 
+// Schedule of one iterative-refinement solve (hns_mixed.cu): slots holds 2 doubles per
+// residual check (max_outer + 1 checks) followed by the per-outer FP32 scales.
+struct RefinePlan {
+    int max_outer = 0;
+    int inner = 0;
+    double tol = 0.0;
+    bool inner_fp16 = true;
+    double* slots = nullptr;
+};
+
 // Schedule of one convergence-checked pressure solve (see rbgs_solve_checked).
 struct SolvePlan {
     int max_iterations = 0;
@@ -128,6 +138,7 @@ struct Context {
     std::map<std::string, DeviceBuffer> scratch;
     DeviceBuffer d_reduce;  // FP64 reduction accumulators, allocated once (kReduceSlots doubles)
     SolvePlan last_solve;   // schedule of the most recent checked solve (hns_last_solve)
+    RefinePlan last_refine; // schedule of the most recent refined solve (hns_last_refine)
     // Profiling (hns_profile_*): device counters and per-phase events on the stream.
     DeviceBuffer d_counters;
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
@@ -192,6 +203,22 @@ void launch_vorticity(const Context& c, const float* vel, float* out, float dt, 
 // acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).
 void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags);
 void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint64_t* out);
+
+// Same iteration in FP32 with unit dx^2 (the FP32-inner refinement): L e = rhs.
+void launch_rbgs_bulk_unit(const Context& c, const float* rhs, const float* e_in, float* e_out, float omega,
+                           const double* check, double tol2);
+
+// ---- mixed precision and refinement (hns_mixed.cu) ----
+void convert_array(const Context& c, const void* src, int src_dt, void* dst, int dst_dt, int64_t n);
+template <typename TI>
+RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol);
+void refine_result(Context& c, const RefinePlan& plan, int* outer, double* residual);
+void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
+                         float dt);
+void launch_divergence_mixed(const Context& c, const void* vel, float* div);
+void launch_gradient_mixed(const Context& c, void* vel, const double* p);
+// u -= grad p for an FP32 velocity and an FP64 pressure, in place.
+void launch_gradient_f64(const Context& c, float* vel, const double* p);
 
 // HNS_Advance over the context's fields (hns_advance.cu).
 void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& params);

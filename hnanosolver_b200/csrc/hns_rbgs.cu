@@ -16,10 +16,9 @@
 //   * The z-halo (values at z = -2, -1, 8, 9 of a row) is one or two values per 32-byte
 //     row in HBM; it is fetched with plain loads into separate arrays while the bulk
 //     copies are in flight.
-//   * Each thread relaxes one z-row: it reads the row, its four x/y neighbour rows and the
-//     right-hand-side row as 16-byte vectors, updates the row's four voxels of the current
-//     colour and writes the row back. Red: 64 leaf rows, 32 x/y-ring rows and the 64
-//     z-ring voxels (two per thread); black: the 64 leaf rows.
+//   * Voxels are relaxed one per lane in warp tasks of 32 whose shared-memory reads hit 32
+//     different banks (relax_task). Red: the leaf's 256, the x/y ring's 128 and the z
+//     ring's 64; black: the leaf's 256.
 //
 // T is the storage type of p and the right-hand side (float, or __half for the inner solve
 // of the mixed-precision refinement); arithmetic is FP32.
@@ -64,60 +63,20 @@ __device__ __forceinline__ float from_f<float>(float v) { return v; }
 template <>
 __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
 
-// A row of 8 values as floats (16- or 32-byte aligned in shared memory).
-__device__ __forceinline__ void load_row(const float* p, float v[8]) {
-    const float4 a = *reinterpret_cast<const float4*>(p), b = *reinterpret_cast<const float4*>(p + 4);
-    v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
-}
-__device__ __forceinline__ void load_row(const __half* p, float v[8]) {
-    const uint4 u = *reinterpret_cast<const uint4*>(p);
-    const __half2* h = reinterpret_cast<const __half2*>(&u);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float2 f = __half22float2(h[k]);
-        v[2 * k] = f.x, v[2 * k + 1] = f.y;
-    }
-}
-__device__ __forceinline__ void store_row(float* p, const float v[8]) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-    *reinterpret_cast<float4*>(p + 4) = make_float4(v[4], v[5], v[6], v[7]);
-}
-__device__ __forceinline__ void store_row(__half* p, const float v[8]) {
-    uint4 u;
-    __half2* h = reinterpret_cast<__half2*>(&u);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) h[k] = __floats2half2_rn(v[2 * k], v[2 * k + 1]);
-    *reinterpret_cast<uint4*>(p) = u;
-}
-
-// Relaxes the four voxels of colour `par` (d = par, par+2, ...) of row r: x/y neighbour rows
-// r +- 12 and r +- 1, z-halo PZ[4r+1] (z = -1) and PZ[4r+2] (z = 8), right-hand-side row rb.
-// The six-neighbour sum is in the reference's order (x+, x-, y+, y-, z+, z-).
+// One SOR update at (a, b, d), d in [0, 8), of a row r = prow(a, b) whose x/y neighbour
+// rows are staged (the leaf's rows and the x/y ring rows): neighbour rows r +- 12 (x) and
+// r +- 1 (y), z-halo PZ[4r+1] (z = -1) and PZ[4r+2] (z = 8), right-hand-side row rb. The
+// six-neighbour sum is in the reference's order (x+, x-, y+, y-, z+, z-).
 template <typename T>
-__device__ __forceinline__ void relax_row(Smem<T>& s, int r, int rb, int par, float dx2, float omega) {
-    float c[8], xp[8], xm[8], yp[8], ym[8], bb[8];
-    load_row(&s.P[r * 8], c);
-    load_row(&s.P[(r + 12) * 8], xp);
-    load_row(&s.P[(r - 12) * 8], xm);
-    load_row(&s.P[(r + 1) * 8], yp);
-    load_row(&s.P[(r - 1) * 8], ym);
-    load_row(&s.B[rb * 8], bb);
-    const float zlo = to_f(s.PZ[r * 4 + 1]), zhi = to_f(s.PZ[r * 4 + 2]);
-    const bool odd = par != 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        // Voxel d = 2k + par; its z-neighbours are d-1 and d+1.
-        const float po = odd ? c[2 * k + 1] : c[2 * k];
-        const float zp = odd ? (k < 3 ? c[2 * k + 2] : zhi) : c[2 * k + 1];
-        const float zm = odd ? c[2 * k] : (k > 0 ? c[2 * k - 1] : zlo);
-        const float sum = (odd ? xp[2 * k + 1] : xp[2 * k]) + (odd ? xm[2 * k + 1] : xm[2 * k]) +
-                          (odd ? yp[2 * k + 1] : yp[2 * k]) + (odd ? ym[2 * k + 1] : ym[2 * k]) + zp + zm;
-        const float pgs = (sum - (odd ? bb[2 * k + 1] : bb[2 * k]) * dx2) * dev::kInv6;
-        const float pn = po + omega * (pgs - po);
-        if (odd) c[2 * k + 1] = pn;
-        else c[2 * k] = pn;
-    }
-    store_row(&s.P[r * 8], c);
+__device__ __forceinline__ void relax_cell(Smem<T>& s, int r, int rb, int d, float dx2, float omega) {
+    const T* P = s.P;
+    const int c = r * 8 + d;
+    const float zp = d < 7 ? to_f(P[c + 1]) : to_f(s.PZ[r * 4 + 2]);
+    const float zm = d > 0 ? to_f(P[c - 1]) : to_f(s.PZ[r * 4 + 1]);
+    const float sum = to_f(P[c + 96]) + to_f(P[c - 96]) + to_f(P[c + 8]) + to_f(P[c - 8]) + zp + zm;
+    const float pgs = (sum - to_f(s.B[rb * 8 + d]) * dx2) * dev::kInv6;
+    const float po = to_f(P[c]);
+    s.P[c] = from_f<T>(po + omega * (pgs - po));
 }
 
 // The same update at a z-ring voxel (a, b, -1) (hi = 0) or (a, b, 8) (hi = 1), a, b in [0, 8):
@@ -133,6 +92,29 @@ __device__ __forceinline__ void relax_zring(Smem<T>& s, int a, int b, int hi, fl
     const float pgs = (sum - to_f(s.BZ[(a * 8 + b) * 2 + hi]) * dx2) * dev::kInv6;
     const float po = to_f(Z[r * 4 + k]);
     s.PZ[r * 4 + k] = from_f<T>(po + omega * (pgs - po));
+}
+
+// The cells of one warp task, one per lane, chosen so that the 32 lanes' shared-memory
+// reads fall in 32 different banks: a task covers 4 consecutive y-rows of two x-rows 12 rows
+// apart (the same bank base) whose voxels of the current colour have opposite parity in d
+// (odd and even banks), 4 voxels per row. Tasks 0-7: the leaf's rows; red only: 8-9 the
+// x-ring rows, 10-11 the y-ring rows, 12-13 the z-ring voxels.
+template <typename T>
+__device__ __forceinline__ void relax_task(Smem<T>& s, int task, int lane, int colour, float dx2, float omega) {
+    const int k = lane & 3, q = (lane >> 2) & 3, h = (lane >> 4) & 1;
+    if (task < 8) {  // leaf rows: a = 2 (task >> 1) + h, b = 4 (task & 1) + q
+        const int a = 2 * (task >> 1) + h, b = 4 * (task & 1) + q;
+        relax_cell(s, prow(a, b), brow(a, b), 2 * k + (((a + b) & 1) ^ colour), dx2, omega);
+    } else if (task < 10) {  // x-ring rows: a = -1 or 8 (by h), b = 4 (task - 8) + q
+        const int a = h ? 8 : -1, b = 4 * (task - 8) + q;
+        if (s.nb[nbi(h ? 1 : -1, 0, 0)] >= 0) relax_cell(s, prow(a, b), brow(a, b), 2 * k + ((a + b) & 1), dx2, omega);
+    } else if (task < 12) {  // y-ring rows: b = -1 or 8 (by h), a = 4 (task - 10) + q
+        const int a = 4 * (task - 10) + q, b = h ? 8 : -1;
+        if (s.nb[nbi(0, h ? 1 : -1, 0)] >= 0) relax_cell(s, prow(a, b), brow(a, b), 2 * k + ((a + b) & 1), dx2, omega);
+    } else {  // z-ring: row (a, b) has its red voxel at z = 8 if a+b is even, else at z = -1
+        const int row = (task - 12) * 32 + lane, a = row >> 3, b = row & 7, hi = ((a + b) & 1) == 0;
+        if (s.nb[nbi(0, 0, hi ? 1 : -1)] >= 0) relax_zring(s, a, b, hi, dx2, omega);
+    }
 }
 
 // Value of p at local (a, b, d), d in [-2, 9] (residual evaluation).
@@ -302,32 +284,11 @@ __global__ void __launch_bounds__(NT) rbgs_bulk_kernel(TopoView t, const T* __re
         }
     }
 
-    // Red (colour 0). Leaf origins are multiples of 8, so a voxel's colour is the parity of
-    // its local a + b + d; the red voxels of row (a, b) have d = (a + b) mod 2 (+2k).
-    if (tid < 64) {  // leaf rows
-        const int a = tid >> 3, b = tid & 7;
-        relax_row(s, prow(a, b), brow(a, b), (a + b) & 1, dx2, omega);
-    } else if (tid < 96) {  // x/y ring rows whose leaf exists
-        const int u = tid - 64, side = u >> 3, k = u & 7;
-        int a, b, l;
-        if (side == 0) a = -1, b = k, l = s.nb[nbi(-1, 0, 0)];
-        else if (side == 1) a = 8, b = k, l = s.nb[nbi(1, 0, 0)];
-        else if (side == 2) a = k, b = -1, l = s.nb[nbi(0, -1, 0)];
-        else a = k, b = 8, l = s.nb[nbi(0, 1, 0)];
-        if (l >= 0) relax_row(s, prow(a, b), brow(a, b), (a + b) & 1, dx2, omega);
-    } else {  // z-ring voxels: row (a, b) has its red one at z = 8 if a+b is even, else z = -1
-        const int lzm = s.nb[nbi(0, 0, -1)], lzp = s.nb[nbi(0, 0, 1)];
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const int row = 2 * (tid - 96) + j, a = row >> 3, b = row & 7, hi = ((a + b) & 1) == 0;
-            if ((hi ? lzp : lzm) >= 0) relax_zring(s, a, b, hi, dx2, omega);
-        }
-    }
+    // Red (colour 0), then black (colour 1): leaf origins are multiples of 8, so a voxel's
+    // colour is the parity of its local a + b + d.
+    for (int task = warp; task < 14; task += NT / 32) relax_task(s, task, lane, 0, dx2, omega);
     __syncthreads();
-    if (tid < 64) {  // Black (colour 1): the leaf rows.
-        const int a = tid >> 3, b = tid & 7;
-        relax_row(s, prow(a, b), brow(a, b), ((a + b) & 1) ^ 1, dx2, omega);
-    }
+    for (int task = warp; task < 8; task += NT / 32) relax_task(s, task, lane, 1, dx2, omega);
     __syncthreads();
     constexpr int kVec = 16 / sizeof(T);  // values per 16-byte store
     for (int q = tid; q < 512 / kVec; q += NT) {
@@ -351,6 +312,14 @@ void launch_rbgs_bulk(const Context& c, const float* div, const float* p_in, flo
                       const double* check, double tol2, double* resid_out) {
     rbgs_bulk_kernel<float><<<(unsigned)c.topo.num_leaves, NT, 0, c.stream>>>(c.topo.view, div, p_in, p_out, c.dx * c.dx,
                                                                               omega, check, tol2, resid_out, c.counters);
+    HNS_LAUNCHED();
+}
+
+void launch_rbgs_bulk_unit(const Context& c, const float* rhs, const float* e_in, float* e_out, float omega,
+                           const double* check, double tol2) {
+    if (!aligned16(rhs) || !aligned16(e_in) || !aligned16(e_out)) fail(HNS_ERR_INVALID_ARG, "inner-solve arrays must be 16-byte aligned");
+    rbgs_bulk_kernel<float><<<(unsigned)c.topo.num_leaves, NT, 0, c.stream>>>(c.topo.view, rhs, e_in, e_out, 1.0f, omega, check,
+                                                                              tol2, nullptr, c.counters);
     HNS_LAUNCHED();
 }
 

@@ -99,6 +99,8 @@ struct SolveOutcome {
     SolvePlan plan;
     float* div;
     float* p;
+    bool refined = false;
+    RefinePlan rplan;
 };
 
 // Projection of vel (in place): divergence, checked solve from p = 0, gradient subtraction.
@@ -111,6 +113,19 @@ SolveOutcome project_in_place(Context& c, float* vel, const hns_step_desc& d) {
     launch_divergence(c, vel, o.div);
     c.phase_end();
     c.phase_begin(HNS_PHASE_SOLVE);
+    if (d.flags & HNS_SOLVE_REFINE) {
+        if (!(d.tolerance > 0.0)) fail(HNS_ERR_INVALID_ARG, "HNS_SOLVE_REFINE needs a positive tolerance");
+        double* p64 = reinterpret_cast<double*>(c.scratch_f32("refine_p", 2 * n));
+        o.refined = true;
+        o.rplan = refine_solve<float>(c, o.div, p64, d.max_outer > 0 ? d.max_outer : 8,
+                                      d.inner_iterations > 0 ? d.inner_iterations : 60, resolve_omega(c, d.omega), d.tolerance);
+        c.last_refine = o.rplan;
+        c.phase_end();
+        c.phase_begin(HNS_PHASE_GRADIENT);
+        launch_gradient_f64(c, vel, p64);
+        c.phase_end();
+        return o;
+    }
     o.plan = rbgs_solve_checked(c, o.div, o.p, d.max_iterations, resolve_omega(c, d.omega), d.flags | HNS_SOLVE_ZERO_INIT,
                                 d.tolerance, d.check_every);
     c.phase_end();
@@ -123,6 +138,18 @@ SolveOutcome project_in_place(Context& c, float* vel, const hns_step_desc& d) {
 
 hns_status finish_info(Context& c, const SolveOutcome& o, const hns_step_desc& d, hns_solve_info* info) {
     if (!info) return HNS_OK;
+    if (o.refined) {
+        int outer = 0;
+        double res = 0.0;
+        refine_result(c, o.rplan, &outer, &res);
+        info->iterations = outer * o.rplan.inner;
+        info->initial_residual = 1.0;
+        info->residual = res;
+        if (res > d.tolerance)
+            return record_error(HNS_ERR_NOT_CONVERGED, "refined solve stopped after " + std::to_string(outer) +
+                                                           " outer iterations with residual " + std::to_string(res));
+        return HNS_OK;
+    }
     int its = 0;
     double chk = 0.0;
     solve_result(c, o.plan, &its, &chk);

@@ -43,7 +43,16 @@ class SolveInfo(ctypes.Structure):
 
 class StepDesc(ctypes.Structure):
     _fields_ = [("dt", _f), ("max_iterations", _i), ("omega", _f), ("tolerance", ctypes.c_double),
-                ("check_every", _i), ("flags", _u)]
+                ("check_every", _i), ("flags", _u), ("max_outer", _i), ("inner_iterations", _i)]
+
+
+class MixedDesc(ctypes.Structure):
+    _fields_ = [("dt", _f), ("omega", _f), ("tolerance", ctypes.c_double), ("max_outer", _i),
+                ("inner_iterations", _i), ("flags", _u)]
+
+
+DTYPE_F32, DTYPE_F16, DTYPE_BF16, DTYPE_F64 = 0, 1, 2, 3
+SOLVE_REFINE = 4
 
 
 class CombustionParams(ctypes.Structure):
@@ -112,6 +121,11 @@ def _load():
     _sig(lib, "hns_field_info", _i, _p, _i, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_i))
     _sig(lib, "hns_advance", _i, _p, _i, _f, ctypes.POINTER(CombustionParams))
     _sig(lib, "hns_active_mask", _i, _p, _p)
+    _sig(lib, "hns_convert", _i, _p, _p, _i, _p, _i, _i64)
+    _sig(lib, "hns_step_mixed", _i, _p, _p, _p, _p, _p, _i, ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_step_mixed_host", _i, _p, _p, _p, _i, ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_last_refine", _i, _p, ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_refine_pressure", _i, _p, _p, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_double))
     _sig(lib, "hns_set_option", _i, _p, _i, _i)
     _sig(lib, "hns_device_status", _i, _p)
     _sig(lib, "hns_profile_enable", _i, _p, _i)
@@ -300,3 +314,37 @@ class Grid:
 
     def device_status(self):
         check(lib.hns_device_status(self._h))
+
+    # ---- mixed precision ----
+    def convert(self, src, src_dtype: int, dst, dst_dtype: int, count: int):
+        check(lib.hns_convert(self._h, _dptr(src), src_dtype, _dptr(dst), dst_dtype, count))
+
+    def step_mixed(self, vel_in, vel_out, scalars_in, scalars_out, desc: MixedDesc, info=False):
+        """vel as torch bfloat16 (N,3), scalars as torch float16 (N,)."""
+        n = len(scalars_in)
+        pin = (_p * max(1, n))(*[_dptr(t) for t in scalars_in])
+        pout = (_p * max(1, n))(*[_dptr(t) for t in scalars_out])
+        si = SolveInfo()
+        check(lib.hns_step_mixed(self._h, _dptr(vel_in), _dptr(vel_out), pin, pout, n, ctypes.byref(desc),
+                                 ctypes.byref(si) if info else None))
+        return si if info else None
+
+    def step_mixed_host(self, vel: np.ndarray, scalars, desc: MixedDesc, info=False):
+        for a in [vel, *scalars]:
+            if a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("host fields must be contiguous float32")
+        ptrs = (_p * max(1, len(scalars)))(*[a.ctypes.data for a in scalars])
+        si = SolveInfo()
+        check(lib.hns_step_mixed_host(self._h, vel.ctypes.data, ptrs, len(scalars), ctypes.byref(desc),
+                                      ctypes.byref(si) if info else None))
+        return si if info else None
+
+    def last_refine(self) -> SolveInfo:
+        si = SolveInfo()
+        check(lib.hns_last_refine(self._h, ctypes.byref(si)))
+        return si
+
+    def refine_pressure(self, out):
+        outer, res = _i(), ctypes.c_double()
+        check(lib.hns_refine_pressure(self._h, _dptr(out), ctypes.byref(outer), ctypes.byref(res)))
+        return outer.value, res.value

@@ -136,6 +136,10 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
 
 /* ---- one solver step ------------------------------------------------------------------- */
 
+#define HNS_SOLVE_REFINE 4u /* hns_step_plain: FP64 iterative refinement around FP32 red-black
+                               inner solves (max_outer x inner_iterations) instead of one plain
+                               FP32 solve; removes the FP32 rounding floor of the residual */
+
 typedef struct hns_step_desc {
     float dt;
     int max_iterations; /* red-black iteration cap (rounded up to even when tolerance > 0) */
@@ -143,6 +147,8 @@ typedef struct hns_step_desc {
     double tolerance;   /* target ||b - A p|| / ||b|| (FP64); 0 runs exactly max_iterations */
     int check_every;    /* iterations between residual checks (rounded up to even; 0 = 10) */
     unsigned flags;     /* HNS_SOLVE_* (HNS_SOLVE_ZERO_INIT is implied) */
+    int max_outer;      /* HNS_SOLVE_REFINE: outer refinement cap */
+    int inner_iterations; /* HNS_SOLVE_REFINE: red-black iterations per outer refinement */
 } hns_step_desc;
 
 /* One step of the SOP operator chain HNanoAdvect + HNanoAdvectVelocity +
@@ -165,6 +171,45 @@ HNS_API hns_status hns_step_plain_host(hns_ctx* ctx, float* vel, float* const* s
 /* Iterations and last checked residual of the most recent convergence-checked solve
  * (synchronizes). residual is -1 when that solve ran without a tolerance. */
 HNS_API hns_status hns_last_solve(hns_ctx* ctx, hns_solve_info* info);
+
+/* ---- mixed precision -------------------------------------------------------------------
+ * Fields stored as BF16 velocity (3 x bf16 interleaved per slot) and FP16 scalars, FP32
+ * arithmetic, and the pressure solve wrapped in iterative refinement: FP64 outer residual
+ * r = b - L p and FP64 accumulated pressure, each outer step solving L e = r / rms(r) with
+ * inner_iterations red-black SOR iterations on FP16 storage from e = 0. */
+#define HNS_DTYPE_F32 0
+#define HNS_DTYPE_F16 1
+#define HNS_DTYPE_BF16 2
+#define HNS_DTYPE_F64 3
+
+/* Elementwise conversion of `count` device values (round to nearest). Supported pairs:
+ * F32<->BF16, F32<->F16, F32<->F64, and same-type copies. */
+HNS_API hns_status hns_convert(hns_ctx* ctx, const void* src, int src_dtype, void* dst, int dst_dtype, int64_t count);
+
+typedef struct hns_mixed_desc {
+    float dt;
+    float omega;          /* inner SOR factor; <= 0 selects 1.9 */
+    double tolerance;     /* target ||b - L p|| / ||b|| in FP64 (> 0) */
+    int max_outer;        /* outer refinement cap */
+    int inner_iterations; /* red-black iterations per outer refinement */
+    unsigned flags;       /* reserved, 0 */
+} hns_mixed_desc;
+
+/* hns_step_plain on reduced-precision storage: vel_in/vel_out BF16 (3 per slot), scalars
+ * FP16; same operator chain, refined solve. Device pointers; scalars_in/out are host arrays
+ * of device pointers. With info the call synchronizes and reports inner iterations run
+ * (outer x inner_iterations) and the exact FP64 residual of the returned pressure. */
+HNS_API hns_status hns_step_mixed(hns_ctx* ctx, const void* vel_in, void* vel_out, const void* const* scalars_in,
+                                  void* const* scalars_out, int nscalars, const hns_mixed_desc* desc,
+                                  hns_solve_info* info);
+/* hns_step_mixed from FP32 HOST buffers updated in place: uploads, converts to BF16/FP16 on
+ * the device, steps, converts back and downloads (synchronous). */
+HNS_API hns_status hns_step_mixed_host(hns_ctx* ctx, float* vel, float* const* scalars, int nscalars,
+                                       const hns_mixed_desc* desc, hns_solve_info* info);
+/* Result of the most recent refined solve (synchronizes). */
+HNS_API hns_status hns_last_refine(hns_ctx* ctx, hns_solve_info* info);
+/* The FP64 pressure of the most recent refined solve, copied to device p_out[num_voxels]. */
+HNS_API hns_status hns_refine_pressure(hns_ctx* ctx, double* p_out, int* outer_iterations, double* residual);
 
 /* ---- named fields and the all-in-one step -----------------------------------------------
  * The context keeps named device fields, as the reference's SimContext keeps d_state and

@@ -1,0 +1,132 @@
+"""Mixed precision (BF16 velocity, FP16 scalars, FP64 iterative refinement of the pressure
+solve) against the FP64 oracle, and the FP32 refinement it is compared with.
+
+Error statements checked here (a 160^3 shell, about 1.3M voxels):
+  * the refined solve's residual ||b - L p|| / ||b||, recomputed by the oracle in FP64 from
+    the returned FP64 pressure, is <= the 1e-5 tolerance;
+  * the projected velocity differs from the FP64 oracle's (same BF16-rounded inputs, exact
+    FP64 solve to 1e-10) by <= 2e-2 of its max (BF16 storage: 8 significant bits);
+  * the advected density differs from the FP64 oracle's by <= 2e-3 of its max (FP16)."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from hnanosolver_b200 import synth
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+@pytest.fixture(scope="module")
+def shell():
+    origins = synth.shell_topology(160, 60.0, 8.0, seed=2)
+    dens, vel = synth.noise_fields(origins, seed=5)
+    return origins, dens, vel
+
+
+def test_conversions_round_to_nearest(dev, shell):
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    v = torch.from_numpy(vel).to(dev).reshape(-1)
+    b = torch.empty(v.numel(), dtype=torch.bfloat16, device=dev)
+    g.convert(v, hl.DTYPE_F32, b, hl.DTYPE_BF16, v.numel())
+    d = torch.from_numpy(dens).to(dev)
+    h = torch.empty(d.numel(), dtype=torch.float16, device=dev)
+    g.convert(d, hl.DTYPE_F32, h, hl.DTYPE_F16, d.numel())
+    back = torch.empty_like(v)
+    g.convert(b, hl.DTYPE_BF16, back, hl.DTYPE_F32, v.numel())
+    g.synchronize()
+    assert torch.equal(b, v.to(torch.bfloat16))
+    assert torch.equal(h, d.to(torch.float16))
+    assert torch.equal(back, v.to(torch.bfloat16).float())
+    g.close()
+
+
+def _mixed(g, dev, dens, vel, tol=1e-5, inner=40, outer=8):
+    from hnanosolver_b200 import lib as hl
+
+    vb = torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous()
+    dh = torch.from_numpy(dens).to(dev).to(torch.float16).contiguous()
+    vo, do = torch.empty_like(vb), torch.empty_like(dh)
+    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=tol, max_outer=outer, inner_iterations=inner, flags=0)
+    info = g.step_mixed(vb, vo, [dh], [do], desc, info=True)
+    return vb, dh, vo, do, info
+
+
+def test_mixed_step_against_fp64_oracle(dev, oracle, shell):
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    vb, dh, vo, do, info = _mixed(g, dev, dens, vel)
+    assert info.residual <= 1e-5
+    t = oracle.topo(origins)
+    v_in = vb.float().cpu().numpy()
+    # The right-hand side the kernels solved: FP32 advection of the BF16 inputs (the oracle's
+    # float path is the kernels' arithmetic), stored as BF16, then its FP32 divergence.
+    adv = torch.from_numpy(t.advect_vector(v_in, 0.1, 10.0)).to(torch.bfloat16).float().numpy()
+    div32 = t.divergence(adv, np.float32(10.0))
+    # The residual claim, recomputed by the oracle in FP64 from the returned FP64 pressure.
+    p = torch.empty(len(dens), dtype=torch.float64, device=dev)
+    outer, res = g.refine_pressure(p)
+    r2, b2 = t.residual(div32.astype(np.float64), p.cpu().numpy(), 0.1)
+    assert np.sqrt(r2 / b2) <= 1e-5
+    assert np.sqrt(r2 / b2) == pytest.approx(res, rel=1e-6)
+    # Field error against the FP64 oracle (same BF16/FP16 inputs, FP64 advection, FP64 solve
+    # to a residual far below 1e-5).
+    v64 = v_in.astype(np.float64)
+    adv64 = t.advect_vector(v64, 0.1, 10.0)
+    div64 = t.divergence(adv64, 10.0)
+    p64 = t.rbgs(div64, np.zeros_like(div64), 0.1, 1200, 1.9)
+    r2, b2 = t.residual(div64, p64, 0.1)
+    assert np.sqrt(r2 / b2) < 1e-9
+    ref_v = t.subtract_gradient(adv64, p64, 10.0)
+    assert rel_err(vo.float().cpu().numpy(), ref_v) <= 2e-2
+    ref_d = t.advect_scalar(v64, dh.float().cpu().numpy().astype(np.float64), 0.1, 10.0)
+    assert rel_err(do.float().cpu().numpy(), ref_d) <= 2e-3
+    g.close()
+
+
+def test_mixed_host_equals_device(dev, shell):
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    vb, dh, vo, do, info = _mixed(g, dev, dens, vel)
+    hv = vb.float().cpu().numpy().copy()
+    hd = dh.float().cpu().numpy().copy()
+    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=8, inner_iterations=40, flags=0)
+    info_h = g.step_mixed_host(hv, [hd], desc, info=True)
+    assert np.array_equal(hv, vo.float().cpu().numpy())
+    assert np.array_equal(hd, do.float().cpu().numpy())
+    assert info_h.iterations == info.iterations
+    g.close()
+
+
+def test_fp32_refined_reaches_tolerance_plain_fp32_cannot(dev, shell):
+    """Plain FP32 SOR at omega 1.9 stalls above 1e-5 on this grid (its rounding floor);
+    the same solve inside FP64 refinement reaches it."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    v_in, d_in = torch.from_numpy(vel).to(dev), torch.from_numpy(dens).to(dev)
+    v_out, d_out = torch.empty_like(v_in), torch.empty_like(d_in)
+    desc = hl.StepDesc(dt=0.1, max_iterations=0, omega=1.9, tolerance=1e-6, check_every=10,
+                       flags=hl.SOLVE_REFINE, max_outer=10, inner_iterations=40)
+    info = g.step_plain(v_in, v_out, [d_in], [d_out], desc, info=True)
+    assert info.residual <= 1e-6
+    plain = hl.StepDesc(dt=0.1, max_iterations=3000, omega=1.9, tolerance=1e-6, check_every=10, flags=0)
+    with pytest.raises(hl.HnsError) as e:
+        g.step_plain(v_in, v_out, [d_in], [d_out], plain, info=True)
+    assert e.value.status == 6
+    g.close()
