@@ -6,9 +6,11 @@
 
 A step is one pass of the hot path over the grid: the SOP operator chain
 HNanoAdvect + HNanoAdvectVelocity + HNanoProjectNonDivergent (scalars and velocity advected
-along one MacCormack trace, divergence, red-black SOR to a relative FP64 Poisson residual of
+along one MacCormack trace, divergence, pressure solve to a relative FP64 Poisson residual of
 1e-5, gradient subtraction), through the C ABI of libhns.so. The metric is active
-voxel-steps/s. Under torchrun every rank runs an independent replica of the workload
+voxel-steps/s. --precision mixed (default): BF16 velocity, FP16 density, FP64 iterative
+refinement around FP16 red-black inner solves; the FP32 forms (plain red-black SOR, and the
+same refinement with FP32 inner solves) are measured in the same run at the same residual. Under torchrun every rank runs an independent replica of the workload
 (the solver does not shard a grid across GPUs), so scaling is weak.
 
 --impl reference times the reference's own CPU implementation of the same step (its
@@ -38,11 +40,11 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "shell512": dict(desc="512^3 box, 16-voxel band (+ leaf half-diagonal) around a seeded radius-200 sphere, "
                           "fields: value-noise density, value-noise velocity in (-1,1)",
-                     dx=0.1, dt=0.1, omega=1.8, tolerance=1e-5, cap=3000, check_every=10, fp32_iterations=800),
+                     dx=0.1, dt=0.1, omega=1.8, omega_refined=1.9, inner=30, tolerance=1e-5, cap=3000, check_every=10,
+                     fp32_iterations=620),
     "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60",
-                     dx=0.1, dt=1.0 / 24.0, omega=1.9, tolerance=1e-5, cap=2000, check_every=10, fp32_iterations=None),
-    "box64": dict(desc="64^3 box fully active (512 leaves)", dx=0.1, dt=0.1, omega=1.0, tolerance=0.0, cap=40,
-                  check_every=0, fp32_iterations=40),
+                     dx=0.1, dt=1.0 / 24.0, omega=1.8, omega_refined=1.9, inner=30, tolerance=1e-5, cap=3000,
+                     check_every=10, fp32_iterations=None),
 }
 RBGS_BYTES_PER_VOXEL = 12  # one fused red+black iteration: read p, read div, write p (FP32)
 
@@ -56,10 +58,10 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload: str):
-    """DRAM bytes per launch of the red-black kernel from the committed ncu summary
-    (profiles/rbgs_iteration_<workload>.md, line `dram_bytes_per_launch: <int>`), or None."""
-    path = os.path.join(ROOT, "profiles", f"rbgs_iteration_{workload}.md")
+def profiled_traffic(workload: str, kind: str):
+    """DRAM bytes per launch of the red-black kernel (kind f32 or f16) from the committed ncu
+    summary profiles/rbgs_<kind>_<workload>.md (line `dram_bytes_per_launch: <int>`), or None."""
+    path = os.path.join(ROOT, "profiles", f"rbgs_{kind}_{workload}.md")
     try:
         with open(path) as fh:
             for line in fh:
@@ -200,6 +202,17 @@ def cpu_baseline(args, wl, iters):
                       f"{iters} red-black iterations", "cpu": binding.cpu_model()}
 
 
+def _timed_steps(torch, stream, fn, steps):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
 def ours(args, wl):
     import torch
 
@@ -223,55 +236,107 @@ def ours(args, wl):
     g = hl.Grid(origins, voxel_size=wl["dx"], device=local)
     stream = torch.cuda.Stream(device=dev)
     g.set_stream(stream.cuda_stream)
+    mixed = args.precision == "mixed"
+    tol = wl["tolerance"]
+
+    # ---- FP32 forms (always measured: the comparison at equal residual) ----
     v = [torch.from_numpy(vel).to(dev), torch.empty((n, 3), device=dev)]
     d = [torch.from_numpy(dens).to(dev), torch.empty(n, device=dev)]
-    torch.cuda.synchronize()
 
-    def desc(cap):
-        return hl.StepDesc(dt=wl["dt"], max_iterations=cap, omega=wl["omega"], tolerance=wl["tolerance"],
+    def plain_desc(cap, refine=False):
+        if refine:
+            return hl.StepDesc(dt=wl["dt"], max_iterations=0, omega=wl["omega_refined"], tolerance=tol, check_every=10,
+                               flags=hl.SOLVE_REFINE, max_outer=cap, inner_iterations=wl["inner"])
+        return hl.StepDesc(dt=wl["dt"], max_iterations=cap, omega=wl["omega"], tolerance=tol,
                            check_every=wl["check_every"], flags=0)
 
-    # Iterations the solve needs on this grid: one checked solve, then a cap with a margin
-    # of two check periods so that few launches are skipped at the end of each solve.
-    try:
-        info = g.step_plain(v[0], v[1], [d[0]], [d[1]], desc(wl["cap"]), info=True)
-    except hl.HnsError as e:
-        if e.status != 6:  # HNS_ERR_NOT_CONVERGED: the FP32 floor; keep the cap
-            raise
-        info = g.last_solve()
-    need = info.iterations
-    cap = need if wl["tolerance"] == 0 else need + 2 * max(2, wl["check_every"])
-    st = desc(cap)
-    state = 1
+    def solve_once(fn, last):
+        try:
+            return fn()
+        except hl.HnsError as e:
+            if e.status != 6:  # HNS_ERR_NOT_CONVERGED: keep the cap
+                raise
+            return last()
 
-    def step():
-        nonlocal state
-        g.step_plain(v[state], v[1 - state], [d[state]], [d[1 - state]], st)
-        state = 1 - state
+    info32 = solve_once(lambda: g.step_plain(v[0], v[1], [d[0]], [d[1]], plain_desc(wl["cap"]), info=True), g.last_solve)
+    if args.no_fp32_comparison and mixed:
+        info32 = hl.SolveInfo(iterations=wl["fp32_iterations"] or info32.iterations, residual=info32.residual)
+    cap32 = info32.iterations if tol == 0 else info32.iterations + 2 * max(2, wl["check_every"])
+    if args.no_fp32_comparison and mixed:
+        infor = hl.SolveInfo(iterations=wl["inner"], residual=0.0)
+    else:
+        infor = solve_once(lambda: g.step_plain(v[0], v[1], [d[0]], [d[1]], plain_desc(16, True), info=True), g.last_refine)
+    outer_r = max(1, infor.iterations // wl["inner"]) + 1
+    state = [0]
+
+    def step32(desc):
+        def f():
+            s0 = state[0]
+            g.step_plain(v[s0], v[1 - s0], [d[s0]], [d[1 - s0]], desc)
+            state[0] = 1 - s0
+        return f
+
+    cmp_steps = max(1, min(args.steps, 3))
+    if args.no_fp32_comparison and mixed:
+        cmp_steps = 0
+    for _ in range(2 if cmp_steps else 0):
+        step32(plain_desc(cap32))()
+    ms_plain = _timed_steps(torch, stream, step32(plain_desc(cap32)), cmp_steps) / max(1, cmp_steps)
+    last32 = g.last_solve()
+    for _ in range(2 if cmp_steps else 0):
+        step32(plain_desc(outer_r, True))()
+    ms_ref = _timed_steps(torch, stream, step32(plain_desc(outer_r, True)), cmp_steps) / max(1, cmp_steps)
+    lastr = g.last_refine()
+    fp32 = None if not cmp_steps else {"plain": {"value": n / (ms_plain / 1e3), "ms_per_step": ms_plain, "omega": wl["omega"],
+                      "red_black_iterations": last32.iterations, "residual_checked": last32.residual},
+            "refined": {"value": n / (ms_ref / 1e3), "ms_per_step": ms_ref, "omega": wl["omega_refined"],
+                        "inner_iterations": wl["inner"], "red_black_iterations": lastr.iterations,
+                        "residual": lastr.residual}}
+
+    # ---- the timed form ----
+    if mixed:
+        vb = [torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous(), torch.empty((n, 3), dtype=torch.bfloat16, device=dev)]
+        dh = [torch.from_numpy(dens).to(dev).to(torch.float16).contiguous(), torch.empty(n, dtype=torch.float16, device=dev)]
+
+        def mdesc(outer):
+            return hl.MixedDesc(dt=wl["dt"], omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
+                                inner_iterations=wl["inner"], flags=0)
+
+        info = solve_once(lambda: g.step_mixed(vb[0], vb[1], [dh[0]], [dh[1]], mdesc(16), info=True), g.last_refine)
+        outer = max(1, info.iterations // wl["inner"]) + 1
+        st = mdesc(outer)
+        ms_state = [0]
+
+        def step():
+            s0 = ms_state[0]
+            g.step_mixed(vb[s0], vb[1 - s0], [dh[s0]], [dh[1 - s0]], st)
+            ms_state[0] = 1 - s0
+
+        launches_per_step = 4 + outer * (3 + wl["inner"])
+        kernel_bytes, kernel_name, phase = 6, "rbgs_bulk_kernel<__half> (inner solve)", "inner"
+    else:
+        info, outer = info32, None
+        st = plain_desc(cap32)
+        step = step32(st)
+        launches_per_step = 3 + cap32
+        kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_bulk_kernel<float>", "solve"
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     if dist:
         td.barrier()
-    clocks = ClockSampler(torch.cuda.current_device() if not os.environ.get("CUDA_VISIBLE_DEVICES") else local)
+    clocks = ClockSampler(local)
     clocks.start()
     g.profile_read()
     g.profile_enable(True)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
+    ms = _timed_steps(torch, stream, step, args.steps)
     if dist:
         td.barrier()
-    ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     g.profile_enable(False)
     prof = g.profile_read()
-    last = g.last_solve()
+    last = g.last_refine() if mixed else g.last_solve()
     if dist:
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         td.all_reduce(t, op=td.ReduceOp.MAX)
@@ -279,25 +344,28 @@ def ours(args, wl):
     ms_step = ms / args.steps
     value = world * n * args.steps / (ms / 1e3)
 
-    # Dominant kernel: the fused red-black iteration. Average duration of the launches that ran
-    # inside the timed region (solve-phase events / device launch counter).
-    solve_ms = prof.phase_ms[hl.PHASES["solve"]]
+    # Dominant kernel: average duration of its launches inside the timed region (phase
+    # events around them / device counter of launches that ran).
+    kms = prof.phase_ms[hl.PHASES[phase]]
     launches = max(1, prof.solver_launches)
-    rbgs_ms = solve_ms / launches
+    k_ms = kms / launches
     peak, peak_kind = measured_peak_gbs()
-    achieved = RBGS_BYTES_PER_VOXEL * n / (rbgs_ms / 1e3) / 1e9
-    traffic = profiled_traffic(args.workload)
+    achieved = kernel_bytes * n / (k_ms / 1e3) / 1e9
+    traffic = profiled_traffic(args.workload, "f16" if mixed else "f32")
 
-    # End to end through the C ABI with host buffers: each step uploads the velocity and
+    # End to end through the C ABI with FP32 host buffers: each step uploads velocity and
     # density from pinned host memory, steps, and downloads both.
     hv = torch.from_numpy(vel).pin_memory().numpy()
     hd = torch.from_numpy(dens).pin_memory().numpy()
     e2e_steps = max(1, min(args.steps, 5))
-    g.step_plain_host(hv, [hd], st)
-    torch.cuda.synchronize()
+    if mixed:
+        run_host = lambda: g.step_mixed_host(hv, [hd], st)  # noqa: E731
+    else:
+        run_host = lambda: g.step_plain_host(hv, [hd], st)  # noqa: E731
+    run_host()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        g.step_plain_host(hv, [hd], st)
+        run_host()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     if dist:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
@@ -306,31 +374,38 @@ def ours(args, wl):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, wl, need)
+        cpu = cpu_baseline(args, wl, info32.iterations)
 
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
+        cfg = {"workload": args.workload, "description": wl["desc"], "voxels": n, "leaves": len(origins),
+               "precision": args.precision, "dt": wl["dt"], "dx": wl["dx"], "tolerance": tol,
+               "residual": "relative FP64 Poisson residual ||b - L p|| / ||b||, b = div dx^2",
+               "l2": "inputs larger than L2 (%.0f MB of fields and solver state per GPU)" % (((12 + 4) * 2 + 8 + 16) * n / 1e6),
+               "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+               "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
+               "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
+               "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None}
+        if mixed:
+            cfg.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+                        "omega_inner": wl["omega_refined"], "inner_iterations": wl["inner"], "outer_cap": outer,
+                        "red_black_iterations": last.iterations, "residual_reached": last.residual})
+        else:
+            cfg.update({"omega": wl["omega"], "red_black_iterations": last.iterations, "iteration_cap": cap32,
+                        "residual_checked": last.residual})
         line = {
             "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "description": wl["desc"], "voxels": n, "leaves": len(origins),
-                       "precision": args.precision, "dt": wl["dt"], "dx": wl["dx"], "omega": wl["omega"],
-                       "tolerance": wl["tolerance"], "red_black_iterations": last.iterations,
-                       "iterations_needed_at_start": need, "iteration_cap": cap,
-                       "last_checked_residual": last.residual, "residual_at_start": info.residual,
-                       "l2": "inputs larger than L2 (state %.0f MB per GPU)" % ((16 * 2 + 8) * n / 1e6),
-                       "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
-                       "phase_ms_per_step": phase_ms},
-            "roofline": {"kernel": "rbgs_bulk_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes_per_launch": RBGS_BYTES_PER_VOXEL * n, "launch_ms": rbgs_ms,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "roofline": {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": kernel_bytes * n, "launch_ms": k_ms,
                          "launches_timed": int(prof.solver_launches)},
             "cpu_baseline": cpu,
             "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 16 * n, "steps": e2e_steps,
-                    "path": "hns_step_plain_host (C ABI, pinned host buffers)"},
-            "gpu_launches": args.steps * (3 + cap),
+                    "path": ("hns_step_mixed_host" if mixed else "hns_step_plain_host") + " (C ABI, pinned FP32 host buffers)"},
+            "gpu_launches": args.steps * launches_per_step,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)
@@ -346,8 +421,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="shell512")
-    ap.add_argument("--precision", choices=["fp32"], default="fp32")
+    ap.add_argument("--precision", choices=["mixed", "fp32"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32-comparison", action="store_true",
+                    help="skip the FP32 forms measured beside the mixed one (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")

@@ -202,11 +202,13 @@ void Context::phase_begin(int phase) {
     HNS_CUDA(cudaEventCreate(&e.stop));
     HNS_CUDA(cudaEventRecord(e.start, stream));
     phase_events.push_back(e);
+    open_phases.push_back(phase_events.size() - 1);
 }
 
 void Context::phase_end() {
-    if (!profiling || phase_events.empty()) return;
-    HNS_CUDA(cudaEventRecord(phase_events.back().stop, stream));
+    if (!profiling || open_phases.empty()) return;
+    HNS_CUDA(cudaEventRecord(phase_events[open_phases.back()].stop, stream));
+    open_phases.pop_back();
 }
 
 Context* check_ctx(hns_ctx* ctx) {

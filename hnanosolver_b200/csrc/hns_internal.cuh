@@ -149,6 +149,7 @@ struct Context {
         cudaEvent_t start, stop;
     };
     std::vector<PhaseEvent> phase_events;
+    std::vector<size_t> open_phases;  // indices into phase_events (phases nest)
     void phase_begin(int phase);
     void phase_end();
     // Named fields in insertion order.

@@ -368,6 +368,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         refine_scale_kernel<TI><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         HNS_LAUNCHED();
         const TI* src = nullptr;
+        c.phase_begin(HNS_PHASE_INNER);
         for (int it = 0; it < plan.inner; ++it) {
             TI* dst = e[it & 1];
             if constexpr (sizeof(TI) == 2)
@@ -377,6 +378,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                                       reinterpret_cast<float*>(dst), omega, chk, tol2);
             src = dst;
         }
+        c.phase_end();
         refine_update_kernel<TI><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
         HNS_LAUNCHED();
         refine_residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, nullptr, r, h2, chk, tol2,

@@ -68,7 +68,7 @@ class CombustionParams(ctypes.Structure):
 
 
 NUM_PHASES = 8
-PHASES = {"advect": 0, "divergence": 1, "solve": 2, "gradient": 3, "forces": 4}
+PHASES = {"advect": 0, "divergence": 1, "solve": 2, "gradient": 3, "forces": 4, "inner": 5}
 
 
 class ProfileData(ctypes.Structure):

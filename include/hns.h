@@ -282,6 +282,7 @@ HNS_API hns_status hns_device_status(hns_ctx* ctx);
 #define HNS_PHASE_SOLVE 2
 #define HNS_PHASE_GRADIENT 3
 #define HNS_PHASE_FORCES 4
+#define HNS_PHASE_INNER 5 /* refinement: the inner red-black iterations (also counted in SOLVE) */
 #define HNS_NUM_PHASES 8
 
 typedef struct hns_profile_data {

@@ -78,7 +78,8 @@ def test_mixed_step_against_fp64_oracle(dev, oracle, shell):
     # The residual claim, recomputed by the oracle in FP64 from the returned FP64 pressure.
     p = torch.empty(len(dens), dtype=torch.float64, device=dev)
     outer, res = g.refine_pressure(p)
-    r2, b2 = t.residual(div32.astype(np.float64), p.cpu().numpy(), 0.1)
+    dx32 = float(np.float32(0.1))  # the library's voxel size is a float
+    r2, b2 = t.residual(div32.astype(np.float64), p.cpu().numpy(), dx32)
     assert np.sqrt(r2 / b2) <= 1e-5
     assert np.sqrt(r2 / b2) == pytest.approx(res, rel=1e-6)
     # Field error against the FP64 oracle (same BF16/FP16 inputs, FP64 advection, FP64 solve
