@@ -43,11 +43,33 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return done != 0;
 }
 
+// try_wait that may suspend the thread for up to `suspend_ns` nanoseconds before returning
+// (the hint bounds how long one poll can sleep; the phase completing wakes it earlier).
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t phase, uint32_t suspend_ns) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(phase), "r"(suspend_ns)
+        : "memory");
+    return done != 0;
+}
+
 // Waits for `phase` of `bar` at most `max_polls` polls (each try_wait itself blocks for a
 // hardware-defined interval). Returns false if the wait gave up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t max_polls) {
     for (uint32_t i = 0; i < max_polls; ++i)
         if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+// The same with a suspend hint per poll: total wait at most about max_polls * suspend_ns.
+__device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t* bar, uint32_t phase, uint32_t max_polls,
+                                                        uint32_t suspend_ns) {
+    for (uint32_t i = 0; i < max_polls; ++i)
+        if (mbar_try_wait_hint(bar, phase, suspend_ns)) return true;
     return false;
 }
 

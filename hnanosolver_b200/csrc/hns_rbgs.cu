@@ -35,7 +35,10 @@ namespace hns {
 namespace {
 
 constexpr int NT = 128;
-constexpr uint32_t kMaxPolls = 1u << 22;  // bounded mbarrier wait (far above any real copy latency)
+// Bounded mbarrier wait: at most kMaxPolls polls of at most kSuspendNs each -- far above
+// any real copy latency (microseconds), and about 1 s when every poll sleeps its full hint.
+constexpr uint32_t kSuspendNs = 20000;
+constexpr uint32_t kMaxPolls = 50000;
 
 // Neighbour-table index of the leaf at offset (dx, dy, dz) in {-1,0,1}^3.
 __host__ __device__ constexpr int nbi(int dx, int dy, int dz) { return (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1); }
@@ -49,6 +52,7 @@ struct Smem {
     double red[2][NT / 32];
     uint64_t bar;
     int nb[27];
+    int wait_ok;
 };
 
 __device__ __forceinline__ int prow(int a, int b) { return (a + 2) * 12 + (b + 2); }
@@ -208,47 +212,50 @@ __global__ void __launch_bounds__(NT) rbgs_bulk_kernel(TopoView t, const T* __re
         if (lane == 0) ptx::mbar_arrive_expect_tx(&s.bar, bytes);
         __syncwarp();
         for (int i = 0; i < np; ++i) piece_issue(pcs[i], &s.bar);
-    } else {
-        // The z-halo with plain loads, spread over warps 1-3 (u = tid - 32 in [0, 96)):
-        //   tasks [0, 128):   p at z = -2,-1 / 8,9 and rhs at z = -1 / 8 of leaf row (a, b)
-        //   tasks [128, 192): p at z = -1 / 8 of an x/y ring row, from the edge leaves.
-        for (int u = tid - 32; u < 192; u += NT - 32) {
-            if (u < 128) {
-                const int hi = u >> 6, row = u & 63, a = row >> 3, b = row & 7;
-                const int l = s.nb[hi ? nbi(0, 0, 1) : nbi(0, 0, -1)];
-                T pz0 = from_f<T>(0.f), pz1 = from_f<T>(0.f), dz = from_f<T>(0.f);
-                if (l >= 0) {
-                    const int64_t rs = ((int64_t)l << 9) + a * 64 + b * 8 + (hi ? 0 : 6);
-                    if (p_in != nullptr) pz0 = p_in[rs], pz1 = p_in[rs + 1];
-                    dz = rhs[rs + (hi ? 0 : 1)];
-                }
-                T* z = &s.PZ[prow(a, b) * 4 + (hi ? 2 : 0)];
-                z[0] = pz0;
-                z[1] = pz1;
-                s.BZ[(a * 8 + b) * 2 + hi] = dz;
-            } else {
-                const int v = u - 128, side = v >> 4, hi = (v >> 3) & 1, k = v & 7;
-                int a, b, la, lb;
-                if (side == 0) a = -1, b = k, la = -1, lb = 0;
-                else if (side == 1) a = 8, b = k, la = 1, lb = 0;
-                else if (side == 2) a = k, b = -1, la = 0, lb = -1;
-                else a = k, b = 8, la = 0, lb = 1;
-                const int l = s.nb[nbi(la, lb, hi ? 1 : -1)];
-                T val = from_f<T>(0.f);
-                if (l >= 0 && p_in != nullptr) val = p_in[((int64_t)l << 9) + (a & 7) * 64 + (b & 7) * 8 + (hi ? 0 : 7)];
-                s.PZ[prow(a, b) * 4 + (hi ? 2 : 1)] = val;
-            }
+    }
+    // The z-halo with plain loads, one task per thread (warp 0 after issuing its copies):
+    //   tid in [0, 128):  p at z = -2,-1 (tid < 64, from the -z leaf) or z = 8,9 (from the +z
+    //                     leaf) and rhs at z = -1 / 8 of leaf row (a, b) = (row >> 3, row & 7)
+    //   tid in [64, 128): also p at z = -1 / 8 of an x/y ring row, from the edge leaves.
+    {
+        const int hi = tid >> 6, row = tid & 63, a = row >> 3, b = row & 7;
+        const int l = s.nb[hi ? nbi(0, 0, 1) : nbi(0, 0, -1)];
+        T pz0 = from_f<T>(0.f), pz1 = from_f<T>(0.f), dz = from_f<T>(0.f);
+        if (l >= 0) {
+            const int64_t rs = ((int64_t)l << 9) + a * 64 + b * 8 + (hi ? 0 : 6);
+            if (p_in != nullptr) pz0 = p_in[rs], pz1 = p_in[rs + 1];
+            dz = rhs[rs + (hi ? 0 : 1)];
+        }
+        T* z = &s.PZ[prow(a, b) * 4 + (hi ? 2 : 0)];
+        z[0] = pz0;
+        z[1] = pz1;
+        s.BZ[(a * 8 + b) * 2 + hi] = dz;
+    }
+    if (tid >= 64) {
+        const int v = tid - 64, side = v >> 4, zhi = (v >> 3) & 1, k = v & 7;
+        int a, b, la, lb;
+        if (side == 0) a = -1, b = k, la = -1, lb = 0;
+        else if (side == 1) a = 8, b = k, la = 1, lb = 0;
+        else if (side == 2) a = k, b = -1, la = 0, lb = -1;
+        else a = k, b = 8, la = 0, lb = 1;
+        const int l = s.nb[nbi(la, lb, zhi ? 1 : -1)];
+        T val = from_f<T>(0.f);
+        if (l >= 0 && p_in != nullptr) val = p_in[((int64_t)l << 9) + (a & 7) * 64 + (b & 7) * 8 + (zhi ? 0 : 7)];
+        s.PZ[prow(a, b) * 4 + (zhi ? 2 : 1)] = val;
+    }
+    // One thread waits for the copies (sleeping between polls); the others wait at the CTA
+    // barrier, which costs no issue slots.
+    if (tid == 0) {
+        s.wait_ok = ptx::mbar_wait_bounded_sleep(&s.bar, 0, kMaxPolls, kSuspendNs) ? 1 : 0;
+        if (!s.wait_ok) {
+            // The copies did not land in time: flag it and give them a second bounded wait so
+            // that no copy is still writing when the CTA's shared memory is released.
+            if (counters != nullptr) atomicExch(counters + 1, 1ull);
+            (void)ptx::mbar_wait_bounded_sleep(&s.bar, 0, kMaxPolls, kSuspendNs);
         }
     }
     __syncthreads();
-    if (!ptx::mbar_wait_bounded(&s.bar, 0, kMaxPolls)) {
-        // The copies did not land in time: flag it, give them a second bounded wait so that
-        // no copy is still writing when the CTA's shared memory is released, and leave p_out
-        // untouched for this leaf.
-        if (tid == 0 && counters != nullptr) atomicExch(counters + 1, 1ull);
-        (void)ptx::mbar_wait_bounded(&s.bar, 0, kMaxPolls);
-        return;
-    }
+    if (!s.wait_ok) return;  // leave p_out untouched for this leaf
 
     if (resid_out != nullptr) {
         const double h2 = (double)dx2;
