@@ -110,6 +110,7 @@ def _load():
     _sig(lib, "hns_subtract_gradient", _i, _p, _p, _p, _p)
     _sig(lib, "hns_vorticity_confinement", _i, _p, _p, _p, _f, _f, _f)
     _sig(lib, "hns_project", _i, _p, _p, _i, _f, _u, ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_project_static", _i, _p, _p, _i, _f, _u, ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_step_plain", _i, _p, _p, _p, _p, _p, _i, ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_step_plain_host", _i, _p, _p, _p, _i, ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_last_solve", _i, _p, ctypes.POINTER(SolveInfo))

@@ -134,6 +134,21 @@ typedef struct hns_solve_info {
 HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float omega, unsigned flags,
                                hns_solve_info* info);
 
+/* hns_project without any device allocation: same arguments and results, but the divergence,
+ * pressure and ping-pong scratch live in one fixed 12 MiB device array inside the library
+ * rather than in buffers the context allocates on first use. No counterpart in the reference.
+ * For callers that must not allocate while they run a solve: cudaMalloc synchronizes the
+ * device and fails once another allocator (a host application's memory pool, a caching
+ * allocator) holds the free memory.
+ * - At most 1,048,576 active voxels (2048 leaves); larger grids return HNS_ERR_UNSUPPORTED.
+ * - The first call on each device looks the array's address up (cudaGetSymbolAddress, which
+ *   also loads its module); make that first call before any stream capture begins.
+ * - The array is shared by every context on a device: calls that overlap in time on one
+ *   device (different streams or threads) race on it. Serialise them.
+ * - The pressure scratch is cleared to zero on every call. */
+HNS_API hns_status hns_project_static(hns_ctx* ctx, float* vel, int iterations, float omega, unsigned flags,
+                                      hns_solve_info* info);
+
 /* ---- one solver step ------------------------------------------------------------------- */
 
 #define HNS_SOLVE_REFINE 4u /* hns_step_plain: FP64 iterative refinement around FP32 red-black
