@@ -31,6 +31,36 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, u
         : "memory");
 }
 
+// Asynchronous copy of kBytes (4, 8 or 16; both addresses kBytes-aligned) from global to
+// this CTA's shared memory, cached in L1 and L2.
+template <int kBytes>
+__device__ __forceinline__ void cp_async_ca(void* dst_smem, const void* src_gmem) {
+    static_assert(kBytes == 4 || kBytes == 8 || kBytes == 16, "cp.async.ca copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst_smem)), "l"(src_gmem), "n"(kBytes)
+                 : "memory");
+}
+
+template <int kBytes>
+__device__ __forceinline__ void cp_async_ca(uint32_t dst_smem, const void* src_gmem) {
+    static_assert(kBytes == 4 || kBytes == 8 || kBytes == 16, "cp.async.ca copies 4, 8 or 16 bytes");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(dst_smem), "l"(src_gmem), "n"(kBytes) : "memory");
+}
+
+// 16-byte asynchronous copy global -> shared cached in L2 only; both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async_cg16(uint32_t dst_smem, const void* src_gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst_smem), "l"(src_gmem) : "memory");
+}
+
+// Arrive on `bar` once this thread's earlier cp.async copies have landed. With .noinc the
+// arrival counts toward the barrier's expected arrival count (set it at mbarrier.init).
+__device__ __forceinline__ void cp_async_mbar_arrive_noinc(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Orders this thread's earlier generic-proxy shared-memory accesses before later async-proxy
+// (bulk copy) accesses of the same memory.
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     uint32_t done;
     asm volatile(
