@@ -315,13 +315,13 @@ def ours(args, wl):
             ms_state[0] = 1 - s0
 
         launches_per_step = 4 + outer * (3 + wl["inner"])
-        kernel_bytes, kernel_name, phase = 6, "rbgs_bulk_kernel<__half> (inner solve)", "inner"
+        kernel_bytes, kernel_name, phase = 6, "rbgs_stream_kernel<__half> (inner solve)", "inner"
     else:
         info, outer = info32, None
         st = plain_desc(cap32)
         step = step32(st)
         launches_per_step = 3 + cap32
-        kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_bulk_kernel<float>", "solve"
+        kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_stream_kernel<float>", "solve"
 
     for _ in range(args.warmup):
         step()
