@@ -143,7 +143,8 @@ struct Context {
     DeviceBuffer d_counters;
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
-    int rbgs_kernel = HNS_RBGS_BULK;  // hns_set_option(HNS_OPT_RBGS_KERNEL)
+    int rbgs_kernel = HNS_RBGS_BULK;      // hns_set_option(HNS_OPT_RBGS_KERNEL)
+    int inner_layout = HNS_INNER_ROWS;    // hns_set_option(HNS_OPT_INNER_LAYOUT)
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -204,6 +205,11 @@ void launch_vorticity(const Context& c, const float* vel, float* out, float dt, 
 // acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).
 void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags);
 void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint64_t* out);
+
+// The FP16 iteration on colour-packed rows (hns_rbgs_packed.cu): slot 8 r + z of a row r
+// holds z at position (z & 1) * 4 + (z >> 1). rhs, e_in, e_out in that layout.
+void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* e_in, void* e_out, float omega,
+                             const double* check, double tol2);
 
 // Same iteration in FP32 with unit dx^2 (the FP32-inner refinement): L e = rhs.
 void launch_rbgs_bulk_unit(const Context& c, const float* rhs, const float* e_in, float* e_out, float omega,

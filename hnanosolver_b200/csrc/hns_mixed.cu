@@ -235,8 +235,13 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
     block_sum2(res * res, b * b, acc);
 }
 
-// r^ = r / s with s = rms(r) from the latest check (stored into *scale); FP16 or FP32.
-template <typename TI>
+// Slot of the colour-packed layout of the FP16 inner solve (launch_rbgs_packed_half): z of a
+// row is stored at position (z & 1) * 4 + (z >> 1).
+__device__ __forceinline__ int64_t packed_slot(int64_t q) { return (q & ~int64_t(7)) | ((q & 1) << 2) | ((q >> 1) & 3); }
+
+// r^ = r / s with s = rms(r) from the latest check (stored into *scale); FP16 or FP32;
+// kPacked: r^ in the colour-packed layout.
+template <typename TI, bool kPacked>
 __global__ void __launch_bounds__(kThreads) refine_scale_kernel(const float* __restrict__ r, TI* __restrict__ rhat,
                                                                  int64_t n, const double* __restrict__ check,
                                                                  double tol2, float* __restrict__ scale) {
@@ -246,18 +251,18 @@ __global__ void __launch_bounds__(kThreads) refine_scale_kernel(const float* __r
     const float inv = 1.0f / sc;
     if (blockIdx.x == 0 && threadIdx.x == 0) *scale = sc;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        sstore(rhat, q, __ldg(r + q) * inv);
+        sstore(rhat, kPacked ? packed_slot(q) : q, __ldg(r + q) * inv);
 }
 
-// p += s e (FP64), pointwise.
-template <typename TI>
+// p += s e (FP64), pointwise; kPacked: e in the colour-packed layout.
+template <typename TI, bool kPacked>
 __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restrict__ p, const TI* __restrict__ e,
                                                                   int64_t n, const float* __restrict__ scale,
                                                                   const double* __restrict__ check, double tol2) {
     if (converged(check, tol2)) return;
     const double sc = (double)*scale;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        p[q] += sc * (double)sload(e, q);
+        p[q] += sc * (double)sload(e, kPacked ? packed_slot(q) : q);
 }
 
 unsigned stream_blocks(const Context& c, int64_t n) {
@@ -360,26 +365,37 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     const double h2 = (double)c.dx * (double)c.dx;
     const double tol2 = tol * tol;
     const unsigned g = stream_blocks(c, n);
+    // The FP16 inner solve runs on colour-packed rows unless the option selects the plain order.
+    const bool packed = sizeof(TI) == 2 && c.inner_layout == HNS_INNER_PACKED;
     refine_residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2, nullptr, tol2,
                                                                      plan.slots);
     HNS_LAUNCHED();
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
-        refine_scale_kernel<TI><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+        if (packed)
+            refine_scale_kernel<TI, true><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+        else
+            refine_scale_kernel<TI, false><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         HNS_LAUNCHED();
         const TI* src = nullptr;
         c.phase_begin(HNS_PHASE_INNER);
         for (int it = 0; it < plan.inner; ++it) {
             TI* dst = e[it & 1];
-            if constexpr (sizeof(TI) == 2)
-                launch_rbgs_bulk_half(c, rhat, src, dst, omega, chk, tol2);
-            else
+            if constexpr (sizeof(TI) == 2) {
+                if (packed)
+                    launch_rbgs_packed_half(c, rhat, src, dst, omega, chk, tol2);
+                else
+                    launch_rbgs_bulk_half(c, rhat, src, dst, omega, chk, tol2);
+            } else
                 launch_rbgs_bulk_unit(c, reinterpret_cast<const float*>(rhat), reinterpret_cast<const float*>(src),
                                       reinterpret_cast<float*>(dst), omega, chk, tol2);
             src = dst;
         }
         c.phase_end();
-        refine_update_kernel<TI><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+        if (packed)
+            refine_update_kernel<TI, true><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+        else
+            refine_update_kernel<TI, false><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
         HNS_LAUNCHED();
         refine_residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, nullptr, r, h2, chk, tol2,
                                                                          plan.slots + 2 * (k + 1));

@@ -18,6 +18,10 @@ __device__ __forceinline__ void fence_barrier_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
@@ -28,6 +32,19 @@ __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, u
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst_smem)),
         "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Tiled 4-D tensor load (TMA, no multicast): the box at coordinates (c0, c1, c2, c3), innermost
+// first, of the tensor map at `map` (a kernel parameter or global memory) into this CTA's shared
+// memory at dst_smem (128-byte aligned); completion is counted on `bar` in bytes. Elements
+// outside the tensor arrive as zeros.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst_smem, const void* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];" ::"r"(dst_smem),
+        "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
         : "memory");
 }
 
@@ -101,6 +118,15 @@ __device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t* bar, uint32_t 
     for (uint32_t i = 0; i < max_polls; ++i)
         if (mbar_try_wait_hint(bar, phase, suspend_ns)) return true;
     return false;
+}
+
+// Waits for `phase` of `bar` with try_wait polls (no suspend hint) for at most `max_cycles`
+// SM clock cycles. Returns false if the wait gave up.
+__device__ __forceinline__ bool mbar_wait_bounded_clock(uint64_t* bar, uint32_t phase, long long max_cycles) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, phase))
+        if (clock64() - t0 > max_cycles) return false;
+    return true;
 }
 
 }  // namespace ptx
