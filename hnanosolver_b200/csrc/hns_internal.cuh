@@ -144,7 +144,7 @@ struct Context {
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
     int rbgs_kernel = HNS_RBGS_BULK;      // hns_set_option(HNS_OPT_RBGS_KERNEL)
-    int inner_layout = HNS_INNER_ROWS;    // hns_set_option(HNS_OPT_INNER_LAYOUT)
+    int inner_layout = HNS_INNER_PACKED;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -207,9 +207,14 @@ void launch_residual(const Context& c, const float* div, const float* p, double*
 void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint64_t* out);
 
 // The FP16 iteration on colour-packed rows (hns_rbgs_packed.cu): slot 8 r + z of a row r
-// holds z at position (z & 1) * 4 + (z >> 1). rhs, e_in, e_out in that layout.
-void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* e_in, void* e_out, float omega,
-                             const double* check, double tol2);
+// holds z at position (z & 1) * 4 + (z >> 1). rhs, e_in, e_out in that layout; faces_in/out the
+// face buffers of e_in/e_out (kPackedFaceBytes per leaf; the kernel writes faces_out); halo the
+// rhs halo records (kPackedHaloBytes per leaf, from launch_rhs_halo_pack). e_in null: e = 0.
+constexpr int kPackedFaceBytes = 1024;
+constexpr int kPackedHaloBytes = 640;
+void launch_rhs_halo_pack(const Context& c, const void* rhs, void* halo, const double* check, double tol2);
+void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
+                             void* e_out, void* faces_out, float omega, const double* check, double tol2);
 
 // Same iteration in FP32 with unit dx^2 (the FP32-inner refinement): L e = rhs.
 void launch_rbgs_bulk_unit(const Context& c, const float* rhs, const float* e_in, float* e_out, float omega,

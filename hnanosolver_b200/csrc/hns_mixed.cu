@@ -367,6 +367,15 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     const unsigned g = stream_blocks(c, n);
     // The FP16 inner solve runs on colour-packed rows unless the option selects the plain order.
     const bool packed = sizeof(TI) == 2 && c.inner_layout == HNS_INNER_PACKED;
+    // Packed: the face buffers of e[0] and e[1] and the rhs halo records.
+    void* faces[2] = {nullptr, nullptr};
+    void* halo = nullptr;
+    if (packed) {
+        const size_t leaves = (size_t)c.topo.num_leaves;
+        faces[0] = c.scratch_f32("refine_faces0", leaves * kPackedFaceBytes / 4);
+        faces[1] = c.scratch_f32("refine_faces1", leaves * kPackedFaceBytes / 4);
+        halo = c.scratch_f32("refine_rhs_halo", leaves * kPackedHaloBytes / 4);
+    }
     refine_residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2, nullptr, tol2,
                                                                      plan.slots);
     HNS_LAUNCHED();
@@ -377,14 +386,17 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         else
             refine_scale_kernel<TI, false><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         HNS_LAUNCHED();
+        if (packed) launch_rhs_halo_pack(c, rhat, halo, chk, tol2);
         const TI* src = nullptr;
+        const void* src_faces = nullptr;
         c.phase_begin(HNS_PHASE_INNER);
         for (int it = 0; it < plan.inner; ++it) {
             TI* dst = e[it & 1];
             if constexpr (sizeof(TI) == 2) {
-                if (packed)
-                    launch_rbgs_packed_half(c, rhat, src, dst, omega, chk, tol2);
-                else
+                if (packed) {
+                    launch_rbgs_packed_half(c, rhat, halo, src, src_faces, dst, faces[it & 1], omega, chk, tol2);
+                    src_faces = faces[it & 1];
+                } else
                     launch_rbgs_bulk_half(c, rhat, src, dst, omega, chk, tol2);
             } else
                 launch_rbgs_bulk_unit(c, reinterpret_cast<const float*>(rhat), reinterpret_cast<const float*>(src),

@@ -129,5 +129,15 @@ __device__ __forceinline__ bool mbar_wait_bounded_clock(uint64_t* bar, uint32_t 
     return true;
 }
 
+// The same, but each poll may suspend the thread for up to `suspend_ns` (it resumes as soon as
+// the phase completes), so a waiting thread takes no issue slots.
+__device__ __forceinline__ bool mbar_wait_bounded_clock_sleep(uint64_t* bar, uint32_t phase, long long max_cycles,
+                                                              uint32_t suspend_ns) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait_hint(bar, phase, suspend_ns))
+        if (clock64() - t0 > max_cycles) return false;
+    return true;
+}
+
 }  // namespace ptx
 }  // namespace hns

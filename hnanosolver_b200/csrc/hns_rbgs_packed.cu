@@ -8,28 +8,37 @@
 // one 4-byte load per neighbour row: a warp's load moves 64 useful values per shared-memory
 // wavefront where a scalar FP16 load moves 32.
 //
-// Staging. The arrays are viewed as 4-D tensors [leaf][x][y][z] of FP16 with 16-byte rows, and
-// one thread stages a leaf's stencil with 26 TMA box loads (cp.async.bulk.tensor, no multicast):
-// the leaf, x-face pairs, y-face pairs, the xy-edge rows, the two z-neighbour leaves with the
-// ring rows their x/y neighbours hold, and the right-hand side with its one-voxel halo. A
-// missing neighbour is the leaf coordinate -1, which TMA fills with zeros (the reference's
-// p = 0 outside the domain). Every box lands densely at a 128-byte-aligned offset.
+// Faces. A leaf's y- and z-faces are scattered over its 128-byte lines (a y-face row pair per
+// x-plane, two values per z-row), and a TMA box moves whole lines, so fetching them from the
+// leaf itself would move the whole leaf. Each iteration therefore also writes the faces it
+// computes into a face buffer beside e (1 KiB per leaf, four 256-byte slots):
+//   slot 0: rows b = 0, 1 of every x-plane    slot 1: rows b = 6, 7     (y faces, [a][2 rows])
+//   slot 2: (z = 0, z = 1) of every row       slot 3: (z = 6, z = 7)    (z faces, [a][b][2])
+// and the right-hand side, constant over an inner solve, is gathered once per outer step into a
+// 640-byte halo record per leaf (rhs_halo_pack_kernel): its x- and y-face rows and the values
+// at the leaf rows' red z-ring voxels.
+//
+// Staging. One producer warp stages a leaf's stencil with 21 TMA box loads (cp.async.bulk.tensor,
+// no multicast): the leaf and its x-face pairs from e, the neighbours' y- and z-face slots and
+// single face entries (xy edges, the ring rows' z-halo), and the leaf's right-hand side with its
+// halo record. A missing neighbour is the leaf coordinate -1, which TMA fills with zeros (the
+// reference's p = 0 outside the domain). Every box lands densely at a 128-byte-aligned offset.
 //
 // Per leaf, the update is one full iteration of redBlackGaussSeidelUpdate
 // (src/Cuda/Kernel.cu:459-489) -- red on the leaf and its one-voxel face ring, then black on
 // the leaf -- with the arithmetic, operation order and FP16 rounding points of
 // rbgs_stream_kernel<__half> in hns_rbgs.cu, so both produce the same values to the bit (the
 // tests compare them). The kernel is persistent: CTA g relaxes leaves g, g + G, ..., with
-// kStages shared-memory stages so that the boxes of the next leaves are in flight while one
-// is relaxed.
+// kStages shared-memory stages; a producer warp fills them while four consumer warps relax.
 //
-// Work of a lane: warp w owns leaf rows (a, b) with a in {2w, 2w+1}, lane = 16 (a - 2w) +
-// 2 b + m, and updates the pair m (voxels 2m, 2m+1 of the colour's half-row):
+// Work of a consumer lane: warp w owns leaf rows (a, b) with a in {2w, 2w+1}, lane =
+// 16 (a - 2w) + 2 b + m, and updates the pair m (voxels 2m, 2m+1 of the colour's half-row):
 //   * red: the pair from the four x/y neighbour rows and the row's own black half (one 8-byte
 //     load gives all its z-neighbours), and the row's red z-ring voxel (z = 8 if a + b is even,
 //     else z = -1), which only this row's black voxels need, so it stays in a register;
 //   * black: the pair from the neighbour rows' updated red halves, the lane's own red pair and
-//     its partner lane's (a shuffle), and the z-ring voxel; both pairs go straight to HBM.
+//     its partner lane's (a shuffle), and the z-ring voxel; both pairs go straight to HBM, with
+//     the row's z-face values and, for rows b = 0, 1, 6, 7, the row into the face buffer.
 // Warps 2 and 3 also relax the red voxels of the x-ring rows (a = -1, 8) and the y-ring rows
 // (b = -1, 8), when the leaf on that side exists.
 #include <cuda.h>
@@ -50,40 +59,50 @@ namespace pk {
 
 constexpr int NC = 128;      // consumer threads (4 warps): the relaxation
 constexpr int NT = NC + 32;  // + one producer warp: the neighbour tables and the TMA boxes
-constexpr int kMinBlocksPerSM = 7;
-// Shared-memory stages: a CTA's boxes run kStages - 1 leaves ahead of its relaxation.
-constexpr int kStages = 3;
-// Bounded mbarrier wait: give up after kWaitCycles SM cycles (about 1 s at 2 GHz).
+constexpr int kMinBlocksPerSM = 8;
+// Shared-memory stages: the producer runs up to kStages leaves ahead of the consumers.
+constexpr int kStages = 4;
+// Bounded mbarrier wait: give up after kWaitCycles SM cycles (about 1 s at 2 GHz); each poll
+// sleeps up to kSuspendNs unless the phase completes first.
 constexpr long long kWaitCycles = 2000000000LL;
+constexpr uint32_t kSuspendNs = 20000;
+
+__device__ __forceinline__ bool wait_stage(uint64_t* bar, uint32_t parity, long long max_cycles) {
+    return ptx::mbar_wait_bounded_clock_sleep(bar, parity, max_cycles, kSuspendNs);
+}
+
+constexpr int kFaceBytes = kPackedFaceBytes;  // face buffer per leaf
+constexpr int kHaloRows = 40;                 // rhs halo record per leaf, in 16-byte rows
+constexpr int kHaloBytes = kHaloRows * 16;
+static_assert(kHaloBytes == kPackedHaloBytes, "halo record size");
 
 __host__ __device__ constexpr int nbi(int dx, int dy, int dz) { return (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1); }
 __host__ __device__ constexpr int parity(int a, int b) { return (a + b) & 1; }  // two's complement: ok for -1
 
 // ---- stage layout (bytes; a row is 16 bytes = 8 packed FP16 values) -------------------------
 //   E    e rows (a, b), a in [-2, 9] (12 planes of 8 rows), b in [0, 8)
-//   YM   e rows (a, b), a in [0, 8), b in {-2, -1}: [a][2]
-//   YP   e rows (a, b), a in [0, 8), b in {8, 9}: [a][2]
+//   YM   e rows (a, b), a in [0, 8), b in {-2, -1}: [a][2]     (the -y leaf's face slot 1)
+//   YP   e rows (a, b), a in [0, 8), b in {8, 9}: [a][2]       (the +y leaf's face slot 0)
 //   YE   e rows of the four xy-edge columns, one 128-byte slot each: (-1, {-2,-1}),
-//        (8, {-2,-1}), (-1, {8,9}), (8, {8,9})
-//   ZM   rows of the -z leaf: (a, b) for a in [-1, 8], b in [0, 8) (10 planes), then the rows
-//        (a, -1) and (a, 8), a in [0, 8) -- z = -1 is at row position 7, z = -2 at 3
-//   ZP   the same for the +z leaf -- z = 8 at position 0, z = 9 at 4
-//   B    right-hand-side rows (a, b), a in [-1, 8], b in [0, 8); then (a, -1), (a, 8)
-//   BZM  the -z leaf's right-hand side (a, b), a, b in [0, 8); BZP the +z leaf's
+//        (8, {-2,-1}), (-1, {8,9}), (8, {8,9})                (one face entry each)
+//   ZFM  (z = -2, z = -1) of rows (a, b), a, b in [0, 8)        (the -z leaf's face slot 3)
+//   ZFP  (z = 8, z = 9) of rows (a, b)                          (the +z leaf's face slot 2)
+//   ZX   the same pairs of the x-ring rows (a = -1, 8) at -z and +z, one 128-byte slot each
+//   ZY   the z-face slots of the leaves (0, -1, -1), (0, 1, -1), (0, -1, 1), (0, 1, 1): the
+//        y-ring rows' pairs are their entries (a, 7) or (a, 0)
+//   B    right-hand-side rows (a, b), a, b in [0, 8)
+//   RH   the leaf's rhs halo record: rows (-1, b), (8, b), (a, -1), (a, 8), then the z-ring values
 constexpr int kOffE = 0;
 constexpr int kOffYM = kOffE + 12 * 128;
 constexpr int kOffYP = kOffYM + 256;
 constexpr int kOffYE = kOffYP + 256;
-constexpr int kOffZM = kOffYE + 4 * 128;
-constexpr int kZPlanes = 10 * 128;       // planes a = -1..8
-constexpr int kZBytes = kZPlanes + 256;  // + rows (a, -1) and (a, 8)
-constexpr int kOffZP = kOffZM + kZBytes;
-constexpr int kOffB = kOffZP + kZBytes;
-constexpr int kOffBYM = kOffB + 10 * 128;
-constexpr int kOffBYP = kOffBYM + 128;
-constexpr int kOffBZM = kOffBYP + 128;
-constexpr int kOffBZP = kOffBZM + 1024;
-constexpr int kStageBytes = kOffBZP + 1024;
+constexpr int kOffZFM = kOffYE + 4 * 128;
+constexpr int kOffZFP = kOffZFM + 256;
+constexpr int kOffZX = kOffZFP + 256;
+constexpr int kOffZY = kOffZX + 4 * 128;
+constexpr int kOffB = kOffZY + 4 * 256;
+constexpr int kOffRH = kOffB + 1024;
+constexpr int kStageBytes = kOffRH + kHaloBytes;
 
 // Byte offset of e row (a, b) in a stage: a in [-2, 9] for b in [0, 8); otherwise the y-face
 // and edge rows listed above.
@@ -92,105 +111,110 @@ __host__ __device__ constexpr int e_row(int a, int b) {
            : (a >= 0 && a < 8) ? (b < 0 ? kOffYM + a * 32 + (b + 2) * 16 : kOffYP + a * 32 + (b - 8) * 16)
            : kOffYE + ((a < 0 ? 0 : 1) + (b < 0 ? 0 : 2)) * 128 + (b < 0 ? b + 2 : b - 8) * 16;
 }
-// Row (a, b) of the -z (zoff = kOffZM) or +z (kOffZP) leaf: a in [-1, 8] for b in [0, 8);
-// b = -1 or 8 for a in [0, 8).
-__host__ __device__ constexpr int z_row(int zoff, int a, int b) {
-    return (b >= 0 && b < 8) ? zoff + (a + 1) * 128 + b * 16 : zoff + kZPlanes + (b < 0 ? 0 : 128) + a * 16;
+// Byte offset of the z-face pair of row (a, b) beyond the leaf: side 0 = (z = -2, -1) from the
+// -z side, side 1 = (z = 8, 9) from the +z side. a, b in [0, 8), or one of them -1 or 8.
+__host__ __device__ constexpr int z_pair(int side, int a, int b) {
+    return (a >= 0 && a < 8 && b >= 0 && b < 8) ? (side ? kOffZFP : kOffZFM) + a * 32 + b * 4
+           : (a < 0)  ? kOffZX + (side ? 256 : 0) + b * 4
+           : (a >= 8) ? kOffZX + (side ? 384 : 128) + b * 4
+           : (b < 0)  ? kOffZY + (side ? 512 : 0) + a * 32 + 7 * 4
+                      : kOffZY + (side ? 768 : 256) + a * 32;
 }
-// Right-hand-side row (a, b) of the leaf: a in [-1, 8] for b in [0, 8); b = -1 or 8 for a in [0, 8).
+// Right-hand-side row (a, b): the leaf's rows, or its halo record's.
 __host__ __device__ constexpr int b_row(int a, int b) {
-    return (b >= 0 && b < 8) ? kOffB + (a + 1) * 128 + b * 16 : (b < 0 ? kOffBYM : kOffBYP) + a * 16;
+    return (a >= 0 && a < 8 && b >= 0 && b < 8) ? kOffB + a * 128 + b * 16
+           : (a < 0)  ? kOffRH + b * 16
+           : (a >= 8) ? kOffRH + 128 + b * 16
+           : (b < 0)  ? kOffRH + 256 + a * 16
+                      : kOffRH + 384 + a * 16;
 }
+// Halo record, row r: r < 8: rhs row (7, r) of the -x leaf; < 16: (0, r - 8) of the +x leaf;
+// < 24: (r - 16, 7) of the -y leaf; < 32: (r - 24, 0) of the +y leaf; then 64 FP16 values,
+// entry a * 8 + b: the rhs at row (a, b)'s red z-ring voxel (z = 8 of the +z leaf if a + b is
+// even, else z = -1 of the -z leaf).
+constexpr int kHaloZ = 32 * 16;
 
 struct __align__(128) Stage {
     uint4 data[kStageBytes / 16];
-    uint64_t bar;  // completes when the stage's 26 boxes have landed
+    uint64_t bar;  // completes when the stage's boxes have landed
     int nb[27];    // the staged leaf's neighbour table
 };
 
 // ---- the boxes of one leaf -------------------------------------------------------------------
-// Tensor maps (passed as one kernel parameter): e maps first, then right-hand-side maps. Box
-// extents are (z, y, x, leaf); coordinates (0, y0, x0, neighbour leaf).
+// Tensor maps (one kernel parameter), all 4-D with coordinates (0, c1, c2, leaf):
 enum MapId : int {
-    kMapFull = 0,   // e (8, 8, 8, 1)
-    kMapXPair,      // e (8, 8, 2, 1)
-    kMapXPlane,     // e (8, 8, 1, 1)
-    kMapYPair,      // e (8, 2, 8, 1)
-    kMapYRow,       // e (8, 1, 8, 1)
-    kMapEdge,       // e (8, 2, 1, 1)
-    kMapRFull,      // rhs (8, 8, 8, 1)
-    kMapRXPlane,    // rhs (8, 8, 1, 1)
-    kMapRYRow,      // rhs (8, 1, 8, 1)
+    kMapE = 0,      // e [leaf][x][y][z]: box (z 8, y 8, x 8); c1 = y, c2 = x
+    kMapEXPair,     // e: box (8, 8, 2)
+    kMapFace,       // face buffer [leaf][slot 4][a 8][32 bytes]: box (16, 8, 1) = a slot; c1 = a, c2 = slot
+    kMapFaceEntry,  // face buffer: box (16, 1, 1) = one entry (a)
+    kMapR,          // rhs [leaf][x][y][z]: box (8, 8, 8)
+    kMapRH,         // rhs halo records [leaf][1][40 rows][16 bytes]: box (8, 40, 1)
     kNumMaps
 };
-constexpr int kBoxX[kNumMaps] = {8, 2, 1, 8, 8, 1, 8, 1, 8};
-constexpr int kBoxY[kNumMaps] = {8, 8, 8, 2, 1, 2, 8, 8, 1};
+constexpr int kMapBytes[kNumMaps] = {1024, 256, 256, 32, 1024, kHaloBytes};
 
 struct TensorMaps {
     CUtensorMap m[kNumMaps];
 };
 
 struct Box {
-    int map, y0, x0, q, dst;
+    int map, c1, c2, q, dst;
 };
-constexpr int kBoxes = 26;
+constexpr int kBoxes = 21;
 
 __host__ __device__ constexpr Box box(int i) {
     // clang-format off
     constexpr Box list[kBoxes] = {
-        {kMapXPair, 0, 6, nbi(-1, 0, 0), e_row(-2, 0)},   // x-face planes a = -2, -1
-        {kMapFull, 0, 0, nbi(0, 0, 0), e_row(0, 0)},      // the leaf
-        {kMapXPair, 0, 0, nbi(1, 0, 0), e_row(8, 0)},     // x-face planes a = 8, 9
-        {kMapYPair, 6, 0, nbi(0, -1, 0), e_row(0, -2)},   // y-face rows b = -2, -1
-        {kMapYPair, 0, 0, nbi(0, 1, 0), e_row(0, 8)},     // y-face rows b = 8, 9
-        {kMapEdge, 6, 7, nbi(-1, -1, 0), e_row(-1, -2)},  // xy-edge columns
-        {kMapEdge, 6, 0, nbi(1, -1, 0), e_row(8, -2)},
-        {kMapEdge, 0, 7, nbi(-1, 1, 0), e_row(-1, 8)},
-        {kMapEdge, 0, 0, nbi(1, 1, 0), e_row(8, 8)},
-        {kMapXPlane, 0, 7, nbi(-1, 0, -1), z_row(kOffZM, -1, 0)},  // -z leaf and its ring rows
-        {kMapFull, 0, 0, nbi(0, 0, -1), z_row(kOffZM, 0, 0)},
-        {kMapXPlane, 0, 0, nbi(1, 0, -1), z_row(kOffZM, 8, 0)},
-        {kMapYRow, 7, 0, nbi(0, -1, -1), z_row(kOffZM, 0, -1)},
-        {kMapYRow, 0, 0, nbi(0, 1, -1), z_row(kOffZM, 0, 8)},
-        {kMapXPlane, 0, 7, nbi(-1, 0, 1), z_row(kOffZP, -1, 0)},   // +z leaf and its ring rows
-        {kMapFull, 0, 0, nbi(0, 0, 1), z_row(kOffZP, 0, 0)},
-        {kMapXPlane, 0, 0, nbi(1, 0, 1), z_row(kOffZP, 8, 0)},
-        {kMapYRow, 7, 0, nbi(0, -1, 1), z_row(kOffZP, 0, -1)},
-        {kMapYRow, 0, 0, nbi(0, 1, 1), z_row(kOffZP, 0, 8)},
-        {kMapRXPlane, 0, 7, nbi(-1, 0, 0), b_row(-1, 0)},  // right-hand side, one-voxel halo
-        {kMapRFull, 0, 0, nbi(0, 0, 0), b_row(0, 0)},
-        {kMapRXPlane, 0, 0, nbi(1, 0, 0), b_row(8, 0)},
-        {kMapRYRow, 7, 0, nbi(0, -1, 0), b_row(0, -1)},
-        {kMapRYRow, 0, 0, nbi(0, 1, 0), b_row(0, 8)},
-        {kMapRFull, 0, 0, nbi(0, 0, -1), kOffBZM},          // z-neighbour right-hand sides
-        {kMapRFull, 0, 0, nbi(0, 0, 1), kOffBZP},
+        {kMapEXPair, 0, 6, nbi(-1, 0, 0), e_row(-2, 0)},     // x-face planes a = -2, -1
+        {kMapE, 0, 0, nbi(0, 0, 0), e_row(0, 0)},            // the leaf
+        {kMapEXPair, 0, 0, nbi(1, 0, 0), e_row(8, 0)},       // x-face planes a = 8, 9
+        {kMapFace, 0, 1, nbi(0, -1, 0), kOffYM},             // y-face rows b = -2, -1
+        {kMapFace, 0, 0, nbi(0, 1, 0), kOffYP},              // y-face rows b = 8, 9
+        {kMapFaceEntry, 7, 1, nbi(-1, -1, 0), kOffYE},       // xy-edge columns
+        {kMapFaceEntry, 0, 1, nbi(1, -1, 0), kOffYE + 128},
+        {kMapFaceEntry, 7, 0, nbi(-1, 1, 0), kOffYE + 256},
+        {kMapFaceEntry, 0, 0, nbi(1, 1, 0), kOffYE + 384},
+        {kMapFace, 0, 3, nbi(0, 0, -1), kOffZFM},            // z faces
+        {kMapFace, 0, 2, nbi(0, 0, 1), kOffZFP},
+        {kMapFaceEntry, 7, 3, nbi(-1, 0, -1), kOffZX},       // x-ring rows' z-halo
+        {kMapFaceEntry, 0, 3, nbi(1, 0, -1), kOffZX + 128},
+        {kMapFaceEntry, 7, 2, nbi(-1, 0, 1), kOffZX + 256},
+        {kMapFaceEntry, 0, 2, nbi(1, 0, 1), kOffZX + 384},
+        {kMapFace, 0, 3, nbi(0, -1, -1), kOffZY},            // y-ring rows' z-halo
+        {kMapFace, 0, 3, nbi(0, 1, -1), kOffZY + 256},
+        {kMapFace, 0, 2, nbi(0, -1, 1), kOffZY + 512},
+        {kMapFace, 0, 2, nbi(0, 1, 1), kOffZY + 768},
+        {kMapR, 0, 0, nbi(0, 0, 0), kOffB},                  // right-hand side
+        {kMapRH, 0, 0, nbi(0, 0, 0), kOffRH},                // its halo record
     };
     // clang-format on
     return list[i];
 }
 
-constexpr int box_bytes(int i) { return 8 * 2 * kBoxY[box(i).map] * kBoxX[box(i).map]; }
 constexpr int stage_tx_bytes() {
     int s = 0;
-    for (int i = 0; i < kBoxes; ++i) s += box_bytes(i);
+    for (int i = 0; i < kBoxes; ++i) s += kMapBytes[box(i).map];
     return s;
 }
 constexpr uint32_t kStageTx = stage_tx_bytes();
 
-// Fixed shared-memory byte offsets (relative to a stage) of one thread's loads and stores.
+// Fixed shared-memory byte offsets (relative to a stage) of one consumer thread's loads, and
+// its offsets in a leaf's output blocks.
 struct LaneGeom {
     int a, b, m, pi;  // leaf row (a, b), pair m, parity of a + b
     int red;          // the row's red pair (E); x neighbours at +- 128
     int yp, ym;       // the y-neighbour rows' pairs at the red positions
     int dk;           // black positions - red positions (8 - 16 pi)
     int b_red;        // right-hand side of the red pair; the black pair's at + dk
-    int zm7;          // z = -1 of the row (ZM row, position 7); z = 8 (ZP position 0) at + kZP0
-    int zc;           // the row's red z-ring voxel (zp0 if pi = 0, else zm7); x neighbours at +- 128
-    int zyp, zym;     // its y neighbours
+    int zlo;          // z = -1 of the row; z = 8 at + kZHi
+    int zc;           // the row's red z-ring voxel (z = 8 if pi = 0, else z = -1)
+    int zxp, zxm, zyp, zym;  // its x and y neighbours
     int zfar;         // its z-neighbour beyond: z = 9 if pi = 0, else z = -2
     int bz;           // right-hand side of the z-ring voxel
     int zq;           // neighbour-table index of the leaf holding the z-ring voxel
-    int gout;         // byte offset of the row in a leaf's block
+    int gout;         // byte offset of the row in a leaf's 1 KiB block of e
+    int zface;        // byte offset of the lane's z-face pair in a leaf's face block
+    int yface;        // byte offset of the row in the face block (rows b = 0, 1, 6, 7), else -1
     // ring row (warps 2, 3): x-ring (a = -1, 8) for warp 2, y-ring (b = -1, 8) for warp 3
     int ra, rb, rpi;
     int rred, rxp, rxm, ryp, rym;  // its red pair and the neighbours' pairs at the same positions
@@ -199,7 +223,7 @@ struct LaneGeom {
     int rhalo;                     // the z-halo its red voxels need: z = -1 if rpi = 0, else z = 8
     int rq;                        // neighbour-table index of the ring row's leaf
 };
-constexpr int kZP0 = kOffZP - kOffZM - 14;  // z_row(kOffZP, a, b) - (z_row(kOffZM, a, b) + 14)
+constexpr int kZHi = z_pair(1, 0, 0) - (z_pair(0, 0, 0) + 2);
 
 __host__ __device__ inline LaneGeom lane_geom(int tid) {
     LaneGeom g{};
@@ -214,20 +238,24 @@ __host__ __device__ inline LaneGeom lane_geom(int tid) {
     g.ym = e_row(g.a, g.b - 1) + pos;
     g.dk = 8 - 16 * g.pi;
     g.b_red = b_row(g.a, g.b) + pos;
-    g.zm7 = z_row(kOffZM, g.a, g.b) + 14;
-    const int zoff = g.pi ? kOffZM : kOffZP, zpos = g.pi ? 14 : 0;
-    g.zc = z_row(zoff, g.a, g.b) + zpos;
-    g.zyp = z_row(zoff, g.a, g.b + 1) + zpos;
-    g.zym = z_row(zoff, g.a, g.b - 1) + zpos;
-    g.zfar = g.pi ? g.zc - 8 : g.zc + 8;
-    g.bz = (g.pi ? kOffBZM + 14 : kOffBZP) + g.a * 128 + g.b * 16;
+    g.zlo = z_pair(0, g.a, g.b) + 2;
+    const int side = g.pi ? 0 : 1, zpos = g.pi ? 2 : 0;
+    g.zc = z_pair(side, g.a, g.b) + zpos;
+    g.zxp = z_pair(side, g.a + 1, g.b) + zpos;
+    g.zxm = z_pair(side, g.a - 1, g.b) + zpos;
+    g.zyp = z_pair(side, g.a, g.b + 1) + zpos;
+    g.zym = z_pair(side, g.a, g.b - 1) + zpos;
+    g.zfar = g.pi ? g.zc - 2 : g.zc + 2;
+    g.bz = kOffRH + kHaloZ + (g.a * 8 + g.b) * 2;
     g.zq = nbi(0, 0, g.pi ? -1 : 1);
     g.gout = (g.a * 64 + g.b * 8) * 2;
-    const int side = lane >> 4, k = (lane >> 1) & 7;
+    g.zface = (2 + g.m) * 256 + g.a * 32 + g.b * 4;
+    g.yface = g.b < 2 ? g.a * 32 + g.b * 16 : g.b >= 6 ? 256 + g.a * 32 + (g.b - 6) * 16 : -1;
+    const int rside = lane >> 4, k = (lane >> 1) & 7;
     if (warp == 2) {
-        g.ra = side ? 8 : -1, g.rb = k, g.rq = nbi(side ? 1 : -1, 0, 0);
+        g.ra = rside ? 8 : -1, g.rb = k, g.rq = nbi(rside ? 1 : -1, 0, 0);
     } else if (warp == 3) {
-        g.ra = k, g.rb = side ? 8 : -1, g.rq = nbi(0, side ? 1 : -1, 0);
+        g.ra = k, g.rb = rside ? 8 : -1, g.rq = nbi(0, rside ? 1 : -1, 0);
     } else {
         g.ra = 0, g.rb = 0, g.rq = nbi(0, 0, 0);  // unused
     }
@@ -240,7 +268,7 @@ __host__ __device__ inline LaneGeom lane_geom(int tid) {
     g.rym = e_row(g.ra, g.rb - 1) + rpos;
     g.rblack = e_row(g.ra, g.rb) + 8 * (1 - g.rpi);
     g.rb_red = b_row(g.ra, g.rb) + rpos;
-    g.rhalo = g.rpi ? z_row(kOffZP, g.ra, g.rb) : z_row(kOffZM, g.ra, g.rb) + 14;
+    g.rhalo = g.rpi ? z_pair(1, g.ra, g.rb) : z_pair(0, g.ra, g.rb) + 2;
     return g;
 }
 
@@ -316,16 +344,17 @@ __device__ __forceinline__ void red_z_pairs(uint32_t k01, uint32_t k23, uint32_t
     zm = pi ? same : shifted;
 }
 
-// Issues the 26 boxes of leaf `leaf` into stage S (one thread). e_zero: e = 0 (the first
-// iteration of a solve), so every e box is read at leaf -1 and arrives as zeros.
+// Issues the boxes of the leaf whose neighbour table is in S.nb into stage S (one thread).
+// e_zero: e = 0 (the first iteration of a solve), so every box of e or its faces is read at
+// leaf -1 and arrives as zeros.
 __device__ __forceinline__ void stage_issue(Stage& S, const TensorMaps& maps, int e_zero) {
     const uint32_t base = ptx::smem_addr(&S);
     ptx::mbar_arrive_expect_tx(&S.bar, kStageTx);
 #pragma unroll
     for (int i = 0; i < kBoxes; ++i) {
         const Box bx = box(i);
-        const int leaf = (e_zero && bx.map < kMapRFull) ? -1 : S.nb[bx.q];
-        ptx::tma_load_4d(base + bx.dst, &maps.m[bx.map], 0, bx.y0, bx.x0, leaf, &S.bar);
+        const int leaf = (e_zero && bx.map < kMapR) ? -1 : S.nb[bx.q];
+        ptx::tma_load_4d(base + bx.dst, &maps.m[bx.map], 0, bx.c1, bx.c2, leaf, &S.bar);
     }
 }
 
@@ -333,7 +362,8 @@ __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;"
 
 // Consumers (warps 0-3): relax the CTA's leaves in order from the staged boxes.
 __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, const LaneGeom& g, int tid, int64_t L,
-                                        int64_t G, char* out, float omega, unsigned long long* counters) {
+                                        int64_t G, char* out, char* faces, float omega,
+                                        unsigned long long* counters) {
     const int warp = tid >> 5, lane = tid & 31;
     int64_t leaf = blockIdx.x;
     for (uint32_t j = 0; leaf < L; ++j, leaf += G) {
@@ -342,7 +372,7 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
         // One thread waits for the stage's boxes; the others wait at the consumer barrier, and
         // all of them read the outcome after it.
         if (tid == 0) {
-            const bool landed = ptx::mbar_wait_bounded_clock(&cur.bar, (j / kStages) & 1, kWaitCycles);
+            const bool landed = wait_stage(&cur.bar, (j / kStages) & 1, kWaitCycles);
             if (!landed && counters != nullptr) atomicExch(counters + 1, 1ull);
             *cok = landed ? 1 : 0;
         }
@@ -353,9 +383,9 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
         // ---- red ----
         uint32_t k01, k23;
         lds64(S + g.red - 4 * g.m + g.dk, k01, k23);  // the row's black half
-        const uint32_t zm7 = lds16(S + g.zm7), zp0 = lds16(S + g.zm7 + kZP0);
+        const uint32_t zlo = lds16(S + g.zlo), zhi = lds16(S + g.zlo + kZHi);
         uint32_t zp, zm;
-        red_z_pairs(k01, k23, zm7, zp0, g.m, g.pi, zp, zm);
+        red_z_pairs(k01, k23, zlo, zhi, g.m, g.pi, zp, zm);
         const uint32_t red = relax2(lds32(S + g.red + 128), lds32(S + g.red - 128), lds32(S + g.yp), lds32(S + g.ym), zp, zm,
                                     lds32(S + g.b_red), lds32(S + g.red), omega);
         sts32(S + g.red, red);
@@ -366,8 +396,8 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
         {
             const uint32_t near = g.pi ? (k01 & 0xffffu) : (k23 >> 16);
             const uint32_t far = lds16(S + g.zfar);
-            const uint32_t ctr = g.pi ? zm7 : zp0;
-            const float v = relax1(lds16(S + g.zc + 128), lds16(S + g.zc - 128), lds16(S + g.zyp), lds16(S + g.zym),
+            const uint32_t ctr = g.pi ? zlo : zhi;
+            const float v = relax1(lds16(S + g.zxp), lds16(S + g.zxm), lds16(S + g.zyp), lds16(S + g.zym),
                                    g.pi ? near : far, g.pi ? far : near, lds16(S + g.bz), ctr, omega);
             zring = cur.nb[g.zq] >= 0 ? round_half(v) : ctr;
         }
@@ -399,9 +429,19 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
         const uint32_t cb = g.m ? k23 : k01;  // the lane's black pair, unchanged by the red sweep
         const uint32_t blk = relax2(lds32(S + g.red + g.dk + 128), lds32(S + g.red + g.dk - 128), lds32(S + g.yp + g.dk),
                                     lds32(S + g.ym + g.dk), bzp, bzm, lds32(S + g.b_red + g.dk), cb, omega);
+        // The row into e_out; its z-face pair ((z0, z1) for m = 0, (z6, z7) for m = 1) and, on the
+        // y faces, the row into the face buffer.
         char* row = out + (leaf << 10) + g.gout;
-        *reinterpret_cast<uint32_t*>(row + 8 * g.pi + 4 * g.m) = red;
-        *reinterpret_cast<uint32_t*>(row + 8 * (1 - g.pi) + 4 * g.m) = blk;
+        const int pr = 8 * g.pi + 4 * g.m, pb = 8 * (1 - g.pi) + 4 * g.m;
+        *reinterpret_cast<uint32_t*>(row + pr) = red;
+        *reinterpret_cast<uint32_t*>(row + pb) = blk;
+        char* face = faces + (leaf << 10);
+        *reinterpret_cast<uint32_t*>(face + g.zface) =
+            __byte_perm(g.pi ? blk : red, g.pi ? red : blk, g.m ? 0x7632 : 0x5410);
+        if (g.yface >= 0) {
+            *reinterpret_cast<uint32_t*>(face + g.yface + pr) = red;
+            *reinterpret_cast<uint32_t*>(face + g.yface + pb) = blk;
+        }
         // This warp is done with the stage: order its reads and writes of it before the next
         // boxes (async proxy) and release it to the producer.
         ptx::fence_proxy_async_smem();
@@ -411,9 +451,9 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
 }
 
 // Producer (warp 4): for each of the CTA's leaves, waits until the consumers have released the
-// stage's previous leaf, writes the leaf's neighbour table into it and issues its 26 boxes.
-// If a release never comes (the consumers stopped), it waits for its boxes still in flight so
-// that none lands after the CTA has exited.
+// stage's previous leaf, writes the leaf's neighbour table into it and issues its boxes. If a
+// release never comes (the consumers stopped), it waits for its boxes still in flight so that
+// none lands after the CTA has exited.
 __device__ __forceinline__ void produce(Stage* st, uint64_t* empty, const TensorMaps& maps, const TopoView& t,
                                         int lane, int64_t L, int64_t G, int e_zero, unsigned long long* counters) {
     int64_t leaf = blockIdx.x;
@@ -423,13 +463,13 @@ __device__ __forceinline__ void produce(Stage* st, uint64_t* empty, const Tensor
         const int nb = nb_next;
         nb_next = (lane < 27 && leaf + G < L) ? __ldg(t.nbr27 + (leaf + G) * 27 + lane) : -1;
         bool released = true;
-        if (j >= kStages && lane == 0) released = ptx::mbar_wait_bounded_clock(&empty[s], (j / kStages - 1) & 1, kWaitCycles);
+        if (j >= kStages && lane == 0) released = wait_stage(&empty[s], (j / kStages - 1) & 1, kWaitCycles);
         released = __shfl_sync(0xffffffffu, released ? 1 : 0, 0) != 0;
         if (!released) {
             if (lane == 0) {
                 if (counters != nullptr) atomicExch(counters + 1, 1ull);
                 for (uint32_t k = j > kStages ? j - kStages : 0; k < j; ++k)
-                    (void)ptx::mbar_wait_bounded_clock(&st[k % kStages].bar, (k / kStages) & 1, kWaitCycles);
+                    (void)wait_stage(&st[k % kStages].bar, (k / kStages) & 1, kWaitCycles);
             }
             return;
         }
@@ -441,9 +481,9 @@ __device__ __forceinline__ void produce(Stage* st, uint64_t* empty, const Tensor
 }
 
 __global__ void __launch_bounds__(NT, kMinBlocksPerSM)
-    rbgs_packed_kernel(const __grid_constant__ TensorMaps maps, TopoView t, __half* __restrict__ e_out, int e_zero,
-                       float omega, const double* __restrict__ check, double tol2,
-                       unsigned long long* __restrict__ counters) {
+    rbgs_packed_kernel(const __grid_constant__ TensorMaps maps, TopoView t, __half* __restrict__ e_out,
+                       char* __restrict__ faces_out, int e_zero, float omega, const double* __restrict__ check,
+                       double tol2, unsigned long long* __restrict__ counters) {
     __shared__ Stage st[kStages];
     __shared__ uint64_t empty[kStages];
     __shared__ int cok;
@@ -463,9 +503,35 @@ __global__ void __launch_bounds__(NT, kMinBlocksPerSM)
         produce(st, empty, maps, t, tid & 31, L, G, e_zero, counters);
     } else {
         const LaneGeom g = lane_geom(tid);
-        consume(st, empty, &cok, g, tid, L, G, reinterpret_cast<char*>(e_out), omega, counters);
+        consume(st, empty, &cok, g, tid, L, G, reinterpret_cast<char*>(e_out), faces_out, omega, counters);
     }
     __syncthreads();  // no thread leaves while boxes of this CTA may still be landing
+}
+
+// The rhs halo records of every leaf (layout at kHaloRows): block = leaf, threads 0-31 copy the
+// 32 face rows, threads 32-95 the 64 z-ring values. Rows and values of missing leaves are 0.
+__global__ void __launch_bounds__(96) rhs_halo_pack_kernel(TopoView t, const __half* __restrict__ rhs,
+                                                             uint4* __restrict__ halo, const double* __restrict__ check,
+                                                             double tol2) {
+    if (check != nullptr && check[0] <= tol2 * check[1]) return;
+    const int64_t leaf = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int* nb = t.nbr27 + leaf * 27;
+    uint4* out = halo + leaf * kHaloRows;
+    const uint4* r4 = reinterpret_cast<const uint4*>(rhs);  // row (l, a, b) at r4[l * 64 + a * 8 + b]
+    if (tid < 32) {
+        const int k = tid & 7, part = tid >> 3;
+        const int q = part == 0 ? nbi(-1, 0, 0) : part == 1 ? nbi(1, 0, 0) : part == 2 ? nbi(0, -1, 0) : nbi(0, 1, 0);
+        const int a = part == 0 ? 7 : part == 1 ? 0 : k, b = part < 2 ? k : part == 2 ? 7 : 0;
+        const int l = __ldg(nb + q);
+        out[tid] = l >= 0 ? __ldg(r4 + (int64_t)l * 64 + a * 8 + b) : make_uint4(0, 0, 0, 0);
+    } else {
+        const int e = tid - 32, a = e >> 3, b = e & 7, even = parity(a, b) == 0;
+        const int l = __ldg(nb + nbi(0, 0, even ? 1 : -1));
+        // z = 0 of the +z leaf's row is at packed position 0, z = 7 of the -z leaf's at 7.
+        const __half v = l >= 0 ? rhs[((int64_t)l * 64 + a * 8 + b) * 8 + (even ? 0 : 7)] : __ushort_as_half(0);
+        reinterpret_cast<__half*>(out + 32)[e] = v;
+    }
 }
 
 bool aligned16(const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -487,11 +553,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// One FP16 map over `base` viewed as [num_leaves][8 x][8 y][8 z], with box (8, by, bx, 1).
-void encode_map(CUtensorMap* m, const void* base, int64_t num_leaves, int bx, int by) {
-    const cuuint64_t dims[4] = {8, 8, 8, (cuuint64_t)num_leaves};
-    const cuuint64_t strides[3] = {16, 128, 1024};
-    const cuuint32_t boxdim[4] = {8, (cuuint32_t)by, (cuuint32_t)bx, 1};
+// A 4-D FP16 map over `base` (dims innermost first, strides in bytes of dims 1-3) with a box.
+void encode4(CUtensorMap* m, const void* base, const cuuint64_t (&dims)[4], const cuuint64_t (&strides)[3],
+             const cuuint32_t (&boxdim)[4]) {
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, const_cast<void*>(base), dims, strides, boxdim,
                                    estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -499,23 +563,34 @@ void encode_map(CUtensorMap* m, const void* base, int64_t num_leaves, int bx, in
     if (r != CUDA_SUCCESS) fail(HNS_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
 }
 
-// Maps for (e, rhs), cached per thread for the most recent few pointer pairs: a solve alternates
-// between two e buffers over one rhs, so re-encoding happens only when the arrays change.
-const TensorMaps& maps_for(const void* e, const void* rhs, int64_t num_leaves) {
+void encode_maps(TensorMaps& t, const void* e, const void* faces, const void* rhs, const void* halo, int64_t L) {
+    const cuuint64_t leaf_dims[4] = {8, 8, 8, (cuuint64_t)L}, leaf_str[3] = {16, 128, 1024};
+    const cuuint64_t face_dims[4] = {16, 8, 4, (cuuint64_t)L}, face_str[3] = {32, 256, (cuuint64_t)kFaceBytes};
+    const cuuint64_t halo_dims[4] = {8, kHaloRows, 1, (cuuint64_t)L}, halo_str[3] = {16, kHaloBytes, kHaloBytes};
+    encode4(&t.m[kMapE], e, leaf_dims, leaf_str, {8, 8, 8, 1});
+    encode4(&t.m[kMapEXPair], e, leaf_dims, leaf_str, {8, 8, 2, 1});
+    encode4(&t.m[kMapFace], faces, face_dims, face_str, {16, 8, 1, 1});
+    encode4(&t.m[kMapFaceEntry], faces, face_dims, face_str, {16, 1, 1, 1});
+    encode4(&t.m[kMapR], rhs, leaf_dims, leaf_str, {8, 8, 8, 1});
+    encode4(&t.m[kMapRH], halo, halo_dims, halo_str, {8, kHaloRows, 1, 1});
+}
+
+// Maps for (e, faces, rhs, halo), cached per thread for the most recent few combinations: a solve
+// alternates between two e buffers over one rhs, so re-encoding happens only when arrays change.
+const TensorMaps& maps_for(const void* e, const void* faces, const void* rhs, const void* halo, int64_t L) {
     struct Entry {
-        const void* e = nullptr;
-        const void* rhs = nullptr;
+        const void* key[4] = {nullptr, nullptr, nullptr, nullptr};
         int64_t leaves = 0;
         TensorMaps maps;
     };
     thread_local Entry cache[4];
     thread_local int next = 0;
     for (Entry& c : cache)
-        if (c.e == e && c.rhs == rhs && c.leaves == num_leaves && c.leaves > 0) return c.maps;
+        if (c.leaves == L && c.key[0] == e && c.key[1] == faces && c.key[2] == rhs && c.key[3] == halo) return c.maps;
     Entry& c = cache[next];
     next = (next + 1) % 4;
-    for (int k = 0; k < kNumMaps; ++k) encode_map(&c.maps.m[k], k < kMapRFull ? e : rhs, num_leaves, kBoxX[k], kBoxY[k]);
-    c.e = e, c.rhs = rhs, c.leaves = num_leaves;
+    encode_maps(c.maps, e, faces, rhs, halo, L);
+    c.key[0] = e, c.key[1] = faces, c.key[2] = rhs, c.key[3] = halo, c.leaves = L;
     return c.maps;
 }
 
@@ -541,16 +616,29 @@ unsigned packed_grid(const Context& c) {
 
 }  // namespace pk
 
-void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* e_in, void* e_out, float omega,
-                             const double* check, double tol2) {
-    if (!pk::aligned16(rhs) || !pk::aligned16(e_in) || !pk::aligned16(e_out) || rhs == nullptr || e_out == nullptr)
+void launch_rhs_halo_pack(const Context& c, const void* rhs, void* halo, const double* check, double tol2) {
+    if (!pk::aligned16(rhs) || !pk::aligned16(halo) || rhs == nullptr || halo == nullptr)
         fail(HNS_ERR_INVALID_ARG, "inner-solve arrays must be non-null and 16-byte aligned");
     if (c.topo.num_leaves <= 0) return;
-    // With e_in null (e = 0) the e maps are made over rhs and every e box is read at leaf -1.
-    const pk::TensorMaps& maps = pk::maps_for(e_in != nullptr ? e_in : rhs, rhs, c.topo.num_leaves);
+    pk::rhs_halo_pack_kernel<<<(unsigned)c.topo.num_leaves, 96, 0, c.stream>>>(
+        c.topo.view, static_cast<const __half*>(rhs), static_cast<uint4*>(halo), check, tol2);
+    HNS_LAUNCHED();
+}
+
+void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
+                             void* e_out, void* faces_out, float omega, const double* check, double tol2) {
+    const void* ptrs[6] = {rhs, halo, e_in, faces_in, e_out, faces_out};
+    for (int k = 0; k < 6; ++k)
+        if (!pk::aligned16(ptrs[k]) || (ptrs[k] == nullptr && k != 2 && k != 3))
+            fail(HNS_ERR_INVALID_ARG, "inner-solve arrays must be 16-byte aligned (only e_in and its faces may be null)");
+    if (c.topo.num_leaves <= 0) return;
+    // With e_in null (e = 0) the maps of e and its faces are made over arrays of the same shapes
+    // (rhs, faces_out) and every box of them is read at leaf -1, so no memory is read.
+    const bool zero = e_in == nullptr || faces_in == nullptr;
+    const pk::TensorMaps& maps = pk::maps_for(zero ? rhs : e_in, zero ? faces_out : faces_in, rhs, halo, c.topo.num_leaves);
     pk::rbgs_packed_kernel<<<pk::packed_grid(c), pk::NT, 0, c.stream>>>(maps, c.topo.view, static_cast<__half*>(e_out),
-                                                                       e_in == nullptr ? 1 : 0, omega, check, tol2,
-                                                                       c.counters);
+                                                                       static_cast<char*>(faces_out), zero ? 1 : 0,
+                                                                       omega, check, tol2, c.counters);
     HNS_LAUNCHED();
 }
 
