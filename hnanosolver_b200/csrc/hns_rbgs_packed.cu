@@ -57,7 +57,7 @@
 namespace hns {
 namespace pk {
 
-constexpr int NC = 128;      // consumer threads (4 warps): the relaxation
+constexpr int NC = 96;       // consumer threads (3 warps): the relaxation
 constexpr int NT = NC + 32;  // + one producer warp: the neighbour tables and the TMA boxes
 constexpr int kMinBlocksPerSM = 8;
 // Shared-memory stages: the producer runs up to kStages leaves ahead of the consumers.
@@ -199,76 +199,69 @@ constexpr int stage_tx_bytes() {
 constexpr uint32_t kStageTx = stage_tx_bytes();
 
 // Fixed shared-memory byte offsets (relative to a stage) of one consumer thread's loads, and
-// its offsets in a leaf's output blocks.
+// its offsets in a leaf's output blocks. Warps 0 and 1: leaf row (a, b) = (4 w + lane / 8,
+// lane % 8), all four red then all four black voxels; warp 2: ring row lane (lanes 0-15 the
+// x-ring rows (-1, b), (8, b); 16-31 the y-ring rows (a, -1), (a, 8)), its four red voxels.
 struct LaneGeom {
-    int a, b, m, pi;  // leaf row (a, b), pair m, parity of a + b
-    int red;          // the row's red pair (E); x neighbours at +- 128
-    int yp, ym;       // the y-neighbour rows' pairs at the red positions
-    int dk;           // black positions - red positions (8 - 16 pi)
-    int b_red;        // right-hand side of the red pair; the black pair's at + dk
-    int zlo;          // z = -1 of the row; z = 8 at + kZHi
-    int zc;           // the row's red z-ring voxel (z = 8 if pi = 0, else z = -1)
+    int a, b, pi;  // the row and the parity of a + b
+    int red;       // the row's red half (8 bytes)
+    int xp, xm;    // the x-neighbour rows' halves at the red positions (leaf rows: red +- 128)
+    int yp, ym;    // the y-neighbour rows' halves at the red positions
+    int dk;        // black half - red half (8 - 16 pi)
+    int b_red;     // right-hand side of the red half; the black half's at + dk
+    int zlo;       // z = -1 of the row; z = 8 at + kZHi (leaf rows); for ring rows the z-halo
+                   // their red voxels need: z = -1 if pi = 0, else z = 8
+    int zc;        // the row's red z-ring voxel (z = 8 if pi = 0, else z = -1)
     int zxp, zxm, zyp, zym;  // its x and y neighbours
-    int zfar;         // its z-neighbour beyond: z = 9 if pi = 0, else z = -2
-    int bz;           // right-hand side of the z-ring voxel
-    int zq;           // neighbour-table index of the leaf holding the z-ring voxel
-    int gout;         // byte offset of the row in a leaf's 1 KiB block of e
-    int zface;        // byte offset of the lane's z-face pair in a leaf's face block
-    int yface;        // byte offset of the row in the face block (rows b = 0, 1, 6, 7), else -1
-    // ring row (warps 2, 3): x-ring (a = -1, 8) for warp 2, y-ring (b = -1, 8) for warp 3
-    int ra, rb, rpi;
-    int rred, rxp, rxm, ryp, rym;  // its red pair and the neighbours' pairs at the same positions
-    int rblack;                    // its black half (8 bytes)
-    int rb_red;                    // right-hand side of the red pair
-    int rhalo;                     // the z-halo its red voxels need: z = -1 if rpi = 0, else z = 8
-    int rq;                        // neighbour-table index of the ring row's leaf
+    int zfar;      // its z-neighbour beyond: z = 9 if pi = 0, else z = -2
+    int bz;        // right-hand side of the z-ring voxel
+    int zq;        // neighbour-table index of the leaf holding the z-ring voxel
+    int q;         // ring rows: neighbour-table index of the row's leaf
+    int gout;      // byte offset of the row in a leaf's 1 KiB block of e
+    int zface;     // byte offset of the row's (z0, z1) pair in a leaf's face block; (z6, z7) at + 256
+    int yface;     // byte offset of the row in the face block (rows b = 0, 1, 6, 7), else -1
 };
 constexpr int kZHi = z_pair(1, 0, 0) - (z_pair(0, 0, 0) + 2);
 
 __host__ __device__ inline LaneGeom lane_geom(int tid) {
     LaneGeom g{};
     const int lane = tid & 31, warp = tid >> 5;
-    g.m = lane & 1;
-    g.b = (lane >> 1) & 7;
-    g.a = 2 * warp + (lane >> 4);
+    if (warp < 2) {
+        g.a = 4 * warp + (lane >> 3);
+        g.b = lane & 7;
+    } else if (lane < 16) {
+        g.a = (lane >> 3) ? 8 : -1, g.b = lane & 7;
+        g.q = nbi((lane >> 3) ? 1 : -1, 0, 0);
+    } else {
+        g.a = lane & 7, g.b = ((lane >> 3) & 1) ? 8 : -1;
+        g.q = nbi(0, ((lane >> 3) & 1) ? 1 : -1, 0);
+    }
     g.pi = parity(g.a, g.b);
-    const int pos = 8 * g.pi + 4 * g.m;
+    const int pos = 8 * g.pi;
     g.red = e_row(g.a, g.b) + pos;
+    g.xp = e_row(g.a + 1, g.b) + pos;
+    g.xm = e_row(g.a - 1, g.b) + pos;
     g.yp = e_row(g.a, g.b + 1) + pos;
     g.ym = e_row(g.a, g.b - 1) + pos;
     g.dk = 8 - 16 * g.pi;
     g.b_red = b_row(g.a, g.b) + pos;
-    g.zlo = z_pair(0, g.a, g.b) + 2;
-    const int side = g.pi ? 0 : 1, zpos = g.pi ? 2 : 0;
-    g.zc = z_pair(side, g.a, g.b) + zpos;
-    g.zxp = z_pair(side, g.a + 1, g.b) + zpos;
-    g.zxm = z_pair(side, g.a - 1, g.b) + zpos;
-    g.zyp = z_pair(side, g.a, g.b + 1) + zpos;
-    g.zym = z_pair(side, g.a, g.b - 1) + zpos;
-    g.zfar = g.pi ? g.zc - 2 : g.zc + 2;
-    g.bz = kOffRH + kHaloZ + (g.a * 8 + g.b) * 2;
-    g.zq = nbi(0, 0, g.pi ? -1 : 1);
-    g.gout = (g.a * 64 + g.b * 8) * 2;
-    g.zface = (2 + g.m) * 256 + g.a * 32 + g.b * 4;
-    g.yface = g.b < 2 ? g.a * 32 + g.b * 16 : g.b >= 6 ? 256 + g.a * 32 + (g.b - 6) * 16 : -1;
-    const int rside = lane >> 4, k = (lane >> 1) & 7;
-    if (warp == 2) {
-        g.ra = rside ? 8 : -1, g.rb = k, g.rq = nbi(rside ? 1 : -1, 0, 0);
-    } else if (warp == 3) {
-        g.ra = k, g.rb = rside ? 8 : -1, g.rq = nbi(0, rside ? 1 : -1, 0);
+    if (warp < 2) {
+        g.zlo = z_pair(0, g.a, g.b) + 2;
+        const int side = g.pi ? 0 : 1, zpos = g.pi ? 2 : 0;
+        g.zc = z_pair(side, g.a, g.b) + zpos;
+        g.zxp = z_pair(side, g.a + 1, g.b) + zpos;
+        g.zxm = z_pair(side, g.a - 1, g.b) + zpos;
+        g.zyp = z_pair(side, g.a, g.b + 1) + zpos;
+        g.zym = z_pair(side, g.a, g.b - 1) + zpos;
+        g.zfar = g.pi ? g.zc - 2 : g.zc + 2;
+        g.bz = kOffRH + kHaloZ + (g.a * 8 + g.b) * 2;
+        g.zq = nbi(0, 0, g.pi ? -1 : 1);
+        g.gout = (g.a * 64 + g.b * 8) * 2;
+        g.zface = 2 * 256 + g.a * 32 + g.b * 4;
+        g.yface = g.b < 2 ? g.a * 32 + g.b * 16 : g.b >= 6 ? 256 + g.a * 32 + (g.b - 6) * 16 : -1;
     } else {
-        g.ra = 0, g.rb = 0, g.rq = nbi(0, 0, 0);  // unused
+        g.zlo = g.pi ? z_pair(1, g.a, g.b) : z_pair(0, g.a, g.b) + 2;
     }
-    g.rpi = parity(g.ra, g.rb);
-    const int rpos = 8 * g.rpi + 4 * g.m;
-    g.rred = e_row(g.ra, g.rb) + rpos;
-    g.rxp = e_row(g.ra + 1, g.rb) + rpos;
-    g.rxm = e_row(g.ra - 1, g.rb) + rpos;
-    g.ryp = e_row(g.ra, g.rb + 1) + rpos;
-    g.rym = e_row(g.ra, g.rb - 1) + rpos;
-    g.rblack = e_row(g.ra, g.rb) + 8 * (1 - g.rpi);
-    g.rb_red = b_row(g.ra, g.rb) + rpos;
-    g.rhalo = g.rpi ? z_pair(1, g.ra, g.rb) : z_pair(0, g.ra, g.rb) + 2;
     return g;
 }
 
@@ -330,20 +323,6 @@ __device__ __forceinline__ uint32_t relax2(uint32_t xp, uint32_t xm, uint32_t yp
 
 __device__ __forceinline__ uint32_t round_half(float v) { return __half_as_ushort(__float2half_rn(v)); }
 
-// The z-neighbour pairs of the lane's red pair from the row's black half (k01, k23) and the
-// row's z = -1 / z = 8 values: with pi = 0 the red voxels are at even z and their z+ are the
-// black values at the same index, their z- one index lower; with pi = 1 the other way round.
-__device__ __forceinline__ void red_z_pairs(uint32_t k01, uint32_t k23, uint32_t zlo, uint32_t zhi, int m, int pi,
-                                            uint32_t& zp, uint32_t& zm) {
-    const uint32_t same = m ? k23 : k01;                     // black values 2m, 2m+1
-    const uint32_t mid = __byte_perm(k01, k23, 0x5432);      // black values 1, 2
-    const uint32_t lo_edge = __byte_perm(zlo, k01, 0x5410);  // z = -1, black value 0
-    const uint32_t hi_edge = __byte_perm(k23, zhi, 0x5432);  // black value 3, z = 8
-    const uint32_t shifted = (pi != m) ? mid : (pi ? hi_edge : lo_edge);
-    zp = pi ? shifted : same;
-    zm = pi ? same : shifted;
-}
-
 // Issues the boxes of the leaf whose neighbour table is in S.nb into stage S (one thread).
 // e_zero: e = 0 (the first iteration of a solve), so every box of e or its faces is read at
 // leaf -1 and arrives as zeros.
@@ -360,7 +339,27 @@ __device__ __forceinline__ void stage_issue(Stage& S, const TensorMaps& maps, in
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, %0;" ::"r"(NC) : "memory"); }
 
-// Consumers (warps 0-3): relax the CTA's leaves in order from the staged boxes.
+// The z-neighbour pairs of a row's four red voxels (pairs 0-1 and 2-3) from its black half
+// (k01, k23) and its values beyond the leaf at z = -1 (zlo) and z = 8 (zhi): with pi = 0 the
+// red voxels are at even z, their z+ the black values at the same index and their z- one
+// index lower; with pi = 1 the other way round.
+__device__ __forceinline__ void red_z(uint32_t k01, uint32_t k23, uint32_t zlo, uint32_t zhi, int pi, uint32_t& zp0,
+                                      uint32_t& zp1, uint32_t& zm0, uint32_t& zm1) {
+    const uint32_t mid = __byte_perm(k01, k23, 0x5432);  // black values 1, 2
+    if (pi == 0) {
+        zp0 = k01, zp1 = k23;
+        zm0 = __byte_perm(zlo, k01, 0x5410), zm1 = mid;  // (z = -1, 0), (1, 2)
+    } else {
+        zm0 = k01, zm1 = k23;
+        zp0 = mid, zp1 = __byte_perm(k23, zhi, 0x5432);  // (1, 2), (3, z = 8)
+    }
+}
+
+__device__ __forceinline__ void sts64(uint32_t a, uint32_t lo, uint32_t hi) {
+    asm volatile("st.shared.v2.b32 [%0], {%1, %2};" ::"r"(a), "r"(lo), "r"(hi));
+}
+
+// Consumers (warps 0-2): relax the CTA's leaves in order from the staged boxes.
 __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, const LaneGeom& g, int tid, int64_t L,
                                         int64_t G, char* out, char* faces, float omega,
                                         unsigned long long* counters) {
@@ -380,67 +379,70 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
         if (!*cok) return;  // e_out keeps its old values for the leaves left
         const uint32_t S = ptx::smem_addr(&cur);
 
-        // ---- red ----
-        uint32_t k01, k23;
-        lds64(S + g.red - 4 * g.m + g.dk, k01, k23);  // the row's black half
-        const uint32_t zlo = lds16(S + g.zlo), zhi = lds16(S + g.zlo + kZHi);
-        uint32_t zp, zm;
-        red_z_pairs(k01, k23, zlo, zhi, g.m, g.pi, zp, zm);
-        const uint32_t red = relax2(lds32(S + g.red + 128), lds32(S + g.red - 128), lds32(S + g.yp), lds32(S + g.ym), zp, zm,
-                                    lds32(S + g.b_red), lds32(S + g.red), omega);
-        sts32(S + g.red, red);
-        // The row's red z-ring voxel: its x/y neighbours are the neighbour rows' values at the
-        // same z; its z-neighbours are the row's black value at z = 7 (pi = 0) or z = 0 (pi = 1)
-        // and the value beyond it.
-        uint32_t zring;
-        {
+        // ---- red: the row's four red voxels, as two pairs ----
+        uint32_t k01, k23, c01, c23, xp0, xp1, xm0, xm1, yp0, yp1, ym0, ym1, b01, b23;
+        lds64(S + g.red + g.dk, k01, k23);  // the row's black half
+        lds64(S + g.red, c01, c23);
+        lds64(S + g.xp, xp0, xp1);
+        lds64(S + g.xm, xm0, xm1);
+        lds64(S + g.yp, yp0, yp1);
+        lds64(S + g.ym, ym0, ym1);
+        lds64(S + g.b_red, b01, b23);
+        const bool leaf_row = warp < 2;
+        const uint32_t zlo = lds16(S + g.zlo), zhi = leaf_row ? lds16(S + g.zlo + kZHi) : zlo;
+        uint32_t zp0, zp1, zm0, zm1;
+        red_z(k01, k23, zlo, zhi, g.pi, zp0, zp1, zm0, zm1);
+        const uint32_t r01 = relax2(xp0, xm0, yp0, ym0, zp0, zm0, b01, c01, omega);
+        const uint32_t r23 = relax2(xp1, xm1, yp1, ym1, zp1, zm1, b23, c23, omega);
+        uint32_t zring = 0;
+        if (leaf_row) {
+            sts64(S + g.red, r01, r23);
+            // The row's red z-ring voxel: its x/y neighbours are the neighbour rows' values at
+            // the same z; its z-neighbours are the row's black value at z = 7 (pi = 0) or z = 0
+            // (pi = 1) and the value beyond it.
             const uint32_t near = g.pi ? (k01 & 0xffffu) : (k23 >> 16);
             const uint32_t far = lds16(S + g.zfar);
             const uint32_t ctr = g.pi ? zlo : zhi;
             const float v = relax1(lds16(S + g.zxp), lds16(S + g.zxm), lds16(S + g.zyp), lds16(S + g.zym),
                                    g.pi ? near : far, g.pi ? far : near, lds16(S + g.bz), ctr, omega);
             zring = cur.nb[g.zq] >= 0 ? round_half(v) : ctr;
-        }
-        if (warp >= 2 && cur.nb[g.rq] >= 0) {  // ring rows
-            uint32_t r01, r23;
-            lds64(S + g.rblack, r01, r23);
-            const uint32_t h = lds16(S + g.rhalo);
-            uint32_t rzp, rzm;
-            red_z_pairs(r01, r23, h, h, g.m, g.rpi, rzp, rzm);
-            sts32(S + g.rred, relax2(lds32(S + g.rxp), lds32(S + g.rxm), lds32(S + g.ryp), lds32(S + g.rym), rzp, rzm,
-                                     lds32(S + g.rb_red), lds32(S + g.rred), omega));
+        } else if (cur.nb[g.q] >= 0) {  // ring row of an existing neighbour leaf
+            sts64(S + g.red, r01, r23);
         }
         consumer_sync();
 
-        // ---- black ----
-        // z-neighbours: pi = 0 (black at odd z): z- = the red value at the same index, z+ = the
-        // next one (the partner lane's first, or the z-ring voxel at z = 8); pi = 1 (black at
-        // even z): z+ = the red value at the same index, z- = the previous one (the partner's
-        // last, or the z-ring voxel at z = -1).
-        const uint32_t other = __shfl_xor_sync(0xffffffffu, red, 1);
-        uint32_t bzp, bzm;
-        if (g.pi == 0) {
-            bzm = red;
-            bzp = __byte_perm(red, g.m ? zring : other, 0x5432);
-        } else {
-            bzp = red;
-            bzm = __byte_perm(g.m ? other : (zring << 16), red, 0x5432);
-        }
-        const uint32_t cb = g.m ? k23 : k01;  // the lane's black pair, unchanged by the red sweep
-        const uint32_t blk = relax2(lds32(S + g.red + g.dk + 128), lds32(S + g.red + g.dk - 128), lds32(S + g.yp + g.dk),
-                                    lds32(S + g.ym + g.dk), bzp, bzm, lds32(S + g.b_red + g.dk), cb, omega);
-        // The row into e_out; its z-face pair ((z0, z1) for m = 0, (z6, z7) for m = 1) and, on the
-        // y faces, the row into the face buffer.
-        char* row = out + (leaf << 10) + g.gout;
-        const int pr = 8 * g.pi + 4 * g.m, pb = 8 * (1 - g.pi) + 4 * g.m;
-        *reinterpret_cast<uint32_t*>(row + pr) = red;
-        *reinterpret_cast<uint32_t*>(row + pb) = blk;
-        char* face = faces + (leaf << 10);
-        *reinterpret_cast<uint32_t*>(face + g.zface) =
-            __byte_perm(g.pi ? blk : red, g.pi ? red : blk, g.m ? 0x7632 : 0x5410);
-        if (g.yface >= 0) {
-            *reinterpret_cast<uint32_t*>(face + g.yface + pr) = red;
-            *reinterpret_cast<uint32_t*>(face + g.yface + pb) = blk;
+        if (leaf_row) {
+            // ---- black: the row's four black voxels ----
+            // z-neighbours from the row's updated red values r0..r3 and the z-ring voxel:
+            // pi = 0 (black at odd z): z- = r[i], z+ = r[i+1] (r[4] = z-ring at z = 8);
+            // pi = 1 (black at even z): z+ = r[i], z- = r[i-1] (r[-1] = z-ring at z = -1).
+            const uint32_t mid = __byte_perm(r01, r23, 0x5432);  // r1, r2
+            uint32_t bzp0, bzp1, bzm0, bzm1;
+            if (g.pi == 0) {
+                bzm0 = r01, bzm1 = r23;
+                bzp0 = mid, bzp1 = __byte_perm(r23, zring, 0x5432);
+            } else {
+                bzp0 = r01, bzp1 = r23;
+                bzm0 = __byte_perm(zring, r01, 0x5410), bzm1 = mid;
+            }
+            const uint32_t ob = S + g.red + g.dk;
+            lds64(ob + 128, xp0, xp1);
+            lds64(ob - 128, xm0, xm1);
+            lds64(S + g.yp + g.dk, yp0, yp1);
+            lds64(S + g.ym + g.dk, ym0, ym1);
+            lds64(S + g.b_red + g.dk, b01, b23);
+            const uint32_t k01n = relax2(xp0, xm0, yp0, ym0, bzp0, bzm0, b01, k01, omega);
+            const uint32_t k23n = relax2(xp1, xm1, yp1, ym1, bzp1, bzm1, b23, k23, omega);
+            // The row (even-z half first) into e_out, its z-face pairs (z0, z1) and (z6, z7),
+            // and on the y faces the row into the face buffer.
+            const uint32_t e01 = g.pi ? k01n : r01, e23 = g.pi ? k23n : r23;
+            const uint32_t o01 = g.pi ? r01 : k01n, o23 = g.pi ? r23 : k23n;
+            const uint4 rowv = make_uint4(e01, e23, o01, o23);
+            *reinterpret_cast<uint4*>(out + (leaf << 10) + g.gout) = rowv;
+            char* face = faces + (leaf << 10);
+            *reinterpret_cast<uint32_t*>(face + g.zface) = __byte_perm(e01, o01, 0x5410);        // (z0, z1)
+            *reinterpret_cast<uint32_t*>(face + g.zface + 256) = __byte_perm(e23, o23, 0x7632);  // (z6, z7)
+            if (g.yface >= 0) *reinterpret_cast<uint4*>(face + g.yface) = rowv;
         }
         // This warp is done with the stage: order its reads and writes of it before the next
         // boxes (async proxy) and release it to the producer.
@@ -450,7 +452,7 @@ __device__ __forceinline__ void consume(Stage* st, uint64_t* empty, int* cok, co
     }
 }
 
-// Producer (warp 4): for each of the CTA's leaves, waits until the consumers have released the
+// Producer (warp 3): for each of the CTA's leaves, waits until the consumers have released the
 // stage's previous leaf, writes the leaf's neighbour table into it and issues its boxes. If a
 // release never comes (the consumers stopped), it waits for its boxes still in flight so that
 // none lands after the CTA has exited.
