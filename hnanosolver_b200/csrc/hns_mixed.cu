@@ -204,7 +204,9 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
 // ---- refinement --------------------------------------------------------------------------
 
 // r = b - L p (FP64; p null means p = 0, and p_zero_out then receives zeros), stored FP32;
-// acc += {sum r^2, sum b^2}.
+// acc += {sum r^2, sum b^2}. One block per leaf: the leaf's p and its six one-voxel face halos
+// (0 where the neighbour leaf does not exist) are read with coalesced loads into a 10^3 tile,
+// and each thread forms the Laplacian of two voxels from it, in the order of residual_kernel.
 __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, const float* __restrict__ div,
                                                                     const double* __restrict__ p,
                                                                     double* __restrict__ p_zero_out,
@@ -212,27 +214,53 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
                                                                     const double* __restrict__ check, double tol2,
                                                                     double* __restrict__ acc) {
     if (converged(check, tol2)) return;
-    __shared__ LeafNbhd L;
-    const VoxelIdx v = voxel_of_block();
-    load_nbhd(L, t, v.leaf);
-    __syncthreads();
-    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
-    const int64_t s = (v.leaf << 9) + v.n;
-    const double b = (double)__ldg(div + s) * h2;
-    double res = b;
+    __shared__ double P[10][10][10];  // (a + 1, b + 1, z + 1)
+    const int64_t leaf = blockIdx.x;
+    const int tid = threadIdx.x;
     if (p != nullptr) {
-        auto P = [&](int a, int bb, int c) {
-            const int64_t q = slot_of(t, L, a, bb, c);
-            return q < 0 ? 0.0 : __ldg(p + q);
-        };
-        const double lap = P(i + 1, j, k) + P(i - 1, j, k) + P(i, j + 1, k) + P(i, j - 1, k) + P(i, j, k + 1) +
-                           P(i, j, k - 1) - 6.0 * __ldg(p + s);
-        res = b - lap;
-    } else if (p_zero_out != nullptr) {
-        p_zero_out[s] = 0.0;
+        const double* pl = p + (leaf << 9);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int n = tid + h * kThreads;
+            P[(n >> 6) + 1][((n >> 3) & 7) + 1][(n & 7) + 1] = __ldg(pl + n);
+        }
+        for (int f = tid; f < 6 * 64; f += kThreads) {
+            const int face = f >> 6, u = (f >> 3) & 7, v = f & 7;
+            int q, slot;
+            double* dst;
+            switch (face) {
+                case 0: q = 4, slot = 7 * 64 + u * 8 + v, dst = &P[0][u + 1][v + 1]; break;    // -x: x = 7
+                case 1: q = 22, slot = u * 8 + v, dst = &P[9][u + 1][v + 1]; break;            // +x: x = 0
+                case 2: q = 10, slot = u * 64 + 7 * 8 + v, dst = &P[u + 1][0][v + 1]; break;   // -y: y = 7
+                case 3: q = 16, slot = u * 64 + v, dst = &P[u + 1][9][v + 1]; break;           // +y: y = 0
+                case 4: q = 12, slot = u * 64 + v * 8 + 7, dst = &P[u + 1][v + 1][0]; break;   // -z: z = 7
+                default: q = 14, slot = u * 64 + v * 8, dst = &P[u + 1][v + 1][9]; break;      // +z: z = 0
+            }
+            const int l = __ldg(t.nbr27 + leaf * 27 + q);
+            *dst = l >= 0 ? __ldg(p + ((int64_t)l << 9) + slot) : 0.0;
+        }
+        __syncthreads();
     }
-    r[s] = (float)res;
-    block_sum2(res * res, b * b, acc);
+    double r2 = 0.0, b2 = 0.0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int n = tid + h * kThreads;
+        const int a = (n >> 6) + 1, b = ((n >> 3) & 7) + 1, z = (n & 7) + 1;
+        const int64_t s = (leaf << 9) + n;
+        const double bb = (double)__ldg(div + s) * h2;
+        double res = bb;
+        if (p != nullptr) {
+            const double lap = P[a + 1][b][z] + P[a - 1][b][z] + P[a][b + 1][z] + P[a][b - 1][z] + P[a][b][z + 1] +
+                               P[a][b][z - 1] - 6.0 * P[a][b][z];
+            res = bb - lap;
+        } else if (p_zero_out != nullptr) {
+            p_zero_out[s] = 0.0;
+        }
+        r[s] = (float)res;
+        r2 += res * res;
+        b2 += bb * bb;
+    }
+    block_sum2(r2, b2, acc);
 }
 
 // Slot of the colour-packed layout of the FP16 inner solve (launch_rbgs_packed_half): z of a
@@ -376,8 +404,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         faces[1] = c.scratch_f32("refine_faces1", leaves * kPackedFaceBytes / 4);
         halo = c.scratch_f32("refine_rhs_halo", leaves * kPackedHaloBytes / 4);
     }
-    refine_residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2, nullptr, tol2,
-                                                                     plan.slots);
+    refine_residual_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2,
+                                                                                   nullptr, tol2, plan.slots);
     HNS_LAUNCHED();
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
@@ -409,8 +437,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         else
             refine_update_kernel<TI, false><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
         HNS_LAUNCHED();
-        refine_residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, nullptr, r, h2, chk, tol2,
-                                                                         plan.slots + 2 * (k + 1));
+        refine_residual_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+            c.topo.view, div, p, nullptr, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
         HNS_LAUNCHED();
     }
     return plan;
