@@ -220,6 +220,17 @@ void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo
 void launch_rbgs_bulk_unit(const Context& c, const float* rhs, const float* e_in, float* e_out, float omega,
                            const double* check, double tol2);
 
+// ---- adjoints (hns_adjoint.cu): each adds its transpose into the adjoint arrays ----
+void launch_adj_advect_scalar(const Context& c, const float* vel, const float* in, const float* out_bar, float* in_bar,
+                              float* vel_bar, float dt);
+void launch_adj_advect_vec3(const Context& c, const float* vel, const float* out_bar, float* vel_bar, float dt);
+void launch_adj_divergence(const Context& c, const float* div_bar, float* vel_bar);
+void launch_adj_gradient(const Context& c, const float* out_bar, float* p_bar);
+void launch_adj_rbgs_half(const Context& c, const float* lam_in, float* lam_out, float* div_bar, int colour, float omega);
+void launch_adj_confinement(const Context& c, const float* vel, const float* out_bar, float* vel_bar, float dt,
+                            float scale, float factor_scale);
+void launch_adj_accumulate(const Context& c, const float* src, float* dst, int64_t n);
+
 // ---- mixed precision and refinement (hns_mixed.cu) ----
 void convert_array(const Context& c, const void* src, int src_dt, void* dst, int dst_dt, int64_t n);
 template <typename TI>

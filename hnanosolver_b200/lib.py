@@ -129,6 +129,14 @@ def _load():
     _sig(lib, "hns_step_mixed_host", _i, _p, _p, _p, _i, ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_last_refine", _i, _p, ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_refine_pressure", _i, _p, _p, ctypes.POINTER(_i), ctypes.POINTER(ctypes.c_double))
+    _sig(lib, "hns_adjoint_advect_scalar", _i, _p, _p, _p, _p, _p, _p, _f)
+    _sig(lib, "hns_adjoint_advect_vec3", _i, _p, _p, _p, _p, _f)
+    _sig(lib, "hns_adjoint_divergence", _i, _p, _p, _p)
+    _sig(lib, "hns_adjoint_subtract_gradient", _i, _p, _p, _p, _p)
+    _sig(lib, "hns_adjoint_rbgs", _i, _p, _p, _p, _i, _f)
+    _sig(lib, "hns_adjoint_project", _i, _p, _p, _i, _f)
+    _sig(lib, "hns_adjoint_vorticity_confinement", _i, _p, _p, _p, _p, _f, _f, _f)
+    _sig(lib, "hns_adjoint_step_plain", _i, _p, _p, _p, _i, _p, _p, _p, _p, _f, _i, _f)
     _sig(lib, "hns_set_option", _i, _p, _i, _i)
     _sig(lib, "hns_device_status", _i, _p)
     _sig(lib, "hns_profile_enable", _i, _p, _i)
@@ -317,6 +325,37 @@ class Grid:
 
     def device_status(self):
         check(lib.hns_device_status(self._h))
+
+    # ---- adjoints (each adds into the *_bar arrays) ----
+    def adjoint_advect_scalar(self, vel, inp, out_bar, in_bar, vel_bar, dt):
+        check(lib.hns_adjoint_advect_scalar(self._h, _dptr(vel), _dptr(inp), _dptr(out_bar), _dptr(in_bar), _dptr(vel_bar), dt))
+
+    def adjoint_advect_vec3(self, vel, out_bar, vel_bar, dt):
+        check(lib.hns_adjoint_advect_vec3(self._h, _dptr(vel), _dptr(out_bar), _dptr(vel_bar), dt))
+
+    def adjoint_divergence(self, div_bar, vel_bar):
+        check(lib.hns_adjoint_divergence(self._h, _dptr(div_bar), _dptr(vel_bar)))
+
+    def adjoint_subtract_gradient(self, out_bar, vel_bar, p_bar):
+        check(lib.hns_adjoint_subtract_gradient(self._h, _dptr(out_bar), _dptr(vel_bar), _dptr(p_bar)))
+
+    def adjoint_rbgs(self, p_bar, div_bar, iterations, omega):
+        check(lib.hns_adjoint_rbgs(self._h, _dptr(p_bar), _dptr(div_bar), iterations, omega))
+
+    def adjoint_project(self, vel_bar, iterations, omega=-1.0):
+        check(lib.hns_adjoint_project(self._h, _dptr(vel_bar), iterations, omega))
+
+    def adjoint_vorticity_confinement(self, vel, out_bar, vel_bar, dt, scale, factor_scale):
+        check(lib.hns_adjoint_vorticity_confinement(self._h, _dptr(vel), _dptr(out_bar), _dptr(vel_bar), dt, scale,
+                                                    factor_scale))
+
+    def adjoint_step_plain(self, vel_in, scalars_in, vel_out_bar, scalars_out_bar, vel_in_bar, scalars_in_bar, dt,
+                           iterations, omega):
+        n = len(scalars_in)
+        arr = lambda ts: (_p * max(1, n))(*[_dptr(t) for t in ts])  # noqa: E731
+        check(lib.hns_adjoint_step_plain(self._h, _dptr(vel_in), arr(scalars_in), n, _dptr(vel_out_bar),
+                                         arr(scalars_out_bar), _dptr(vel_in_bar), arr(scalars_in_bar), dt, iterations,
+                                         omega))
 
     # ---- mixed precision ----
     def convert(self, src, src_dtype: int, dst, dst_dtype: int, count: int):

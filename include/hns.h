@@ -279,6 +279,41 @@ HNS_API hns_status hns_advance(hns_ctx* ctx, int iterations, float dt, const hns
  * build_activity_mask marks every slot active, src/Cuda/Kernel.cu:75). */
 HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out);
 
+/* ---- adjoints ----------------------------------------------------------------------------
+ * Reverse-mode derivatives of the step's operators, for gradient-based use of the solver
+ * (inverse design, control, learned closures). The reference has no adjoint path; these
+ * differentiate the forward operators declared above. Each takes the forward operator's
+ * inputs and the adjoint of its output (device arrays, same layouts) and ADDS the transpose of
+ * the forward derivative, taken at those inputs, into the adjoint arrays of the inputs, which
+ * the caller zeroes before their first use. Scatters use FP32 atomics, so the last bits vary
+ * from run to run. */
+
+/* hns_advect_scalar: in_bar += (d out / d in)^T out_bar, vel_bar += (d out / d vel)^T out_bar. */
+HNS_API hns_status hns_adjoint_advect_scalar(hns_ctx* ctx, const float* vel, const float* in, const float* out_bar,
+                                             float* in_bar, float* vel_bar, float dt);
+/* hns_advect_vec3 (self-advection): vel_bar += (d out / d vel)^T out_bar. */
+HNS_API hns_status hns_adjoint_advect_vec3(hns_ctx* ctx, const float* vel, const float* out_bar, float* vel_bar, float dt);
+/* hns_divergence: vel_bar += D^T div_bar. */
+HNS_API hns_status hns_adjoint_divergence(hns_ctx* ctx, const float* div_bar, float* vel_bar);
+/* hns_subtract_gradient: vel_bar += out_bar (may be NULL to skip), p_bar += (d out / d p)^T out_bar. */
+HNS_API hns_status hns_adjoint_subtract_gradient(hns_ctx* ctx, const float* out_bar, float* vel_bar, float* p_bar);
+/* hns_rbgs from p = 0 (HNS_SOLVE_ZERO_INIT), `iterations` iterations: div_bar += M^T p_bar,
+ * where p = M div is the linear map of the iterations. omega is used as given, as hns_rbgs
+ * uses it. */
+HNS_API hns_status hns_adjoint_rbgs(hns_ctx* ctx, const float* p_bar, float* div_bar, int iterations, float omega);
+/* hns_project (`iterations` iterations from p = 0): vel_bar, the adjoint of the projected
+ * velocity, becomes the adjoint of the velocity before the projection (in place). */
+HNS_API hns_status hns_adjoint_project(hns_ctx* ctx, float* vel_bar, int iterations, float omega);
+/* hns_vorticity_confinement: vel_bar += (d out / d vel)^T out_bar. */
+HNS_API hns_status hns_adjoint_vorticity_confinement(hns_ctx* ctx, const float* vel, const float* out_bar, float* vel_bar,
+                                                     float dt, float scale, float factor_scale);
+/* hns_step_plain with a fixed iteration count (tolerance 0): from the step's inputs and the
+ * adjoints of its outputs, adds the adjoints of its inputs (velocity and each scalar).
+ * scalars_in, scalars_out_bar, scalars_in_bar: host arrays of nscalars device pointers. */
+HNS_API hns_status hns_adjoint_step_plain(hns_ctx* ctx, const float* vel_in, const float* const* scalars_in, int nscalars,
+                                          const float* vel_out_bar, const float* const* scalars_out_bar, float* vel_in_bar,
+                                          float* const* scalars_in_bar, float dt, int iterations, float omega);
+
 /* ---- options ----------------------------------------------------------------------------- */
 #define HNS_OPT_RBGS_KERNEL 1 /* which red-black kernel: */
 #define HNS_RBGS_PLAIN 0      /*   plain loads into a padded halo tile */
