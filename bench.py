@@ -59,7 +59,7 @@ def measured_peak_gbs():
 
 
 def profiled_traffic(workload: str, kind: str):
-    """DRAM bytes per launch of the red-black kernel (kind f32 or packed) from the committed ncu
+    """DRAM bytes per launch of the red-black kernel (kind f32 or split) from the committed ncu
     summary profiles/rbgs_<kind>_<workload>.md (line `dram_bytes_per_launch: <int>`), or None."""
     path = os.path.join(ROOT, "profiles", f"rbgs_{kind}_{workload}.md")
     try:
@@ -314,8 +314,10 @@ def ours(args, wl):
             g.step_mixed(vb[s0], vb[1 - s0], [dh[s0]], [dh[1 - s0]], st)
             ms_state[0] = 1 - s0
 
-        launches_per_step = 4 + outer * (3 + wl["inner"])
-        kernel_bytes, kernel_name, phase = 6, "rbgs_packed_kernel (FP16 inner solve, colour-packed rows)", "inner"
+        launches_per_step = 5 + outer * (3 + 2 * wl["inner"])
+        # One launch is a half-sweep: half of an iteration's pass-model bytes (read e, read r,
+        # write e at 2 bytes each).
+        kernel_bytes, kernel_name, phase = 3, "rbgs_split_half_kernel (FP16 inner solve, colour-split, one colour per launch)", "inner"
     else:
         info, outer = info32, None
         st = plain_desc(cap32)
@@ -353,7 +355,7 @@ def ours(args, wl):
     k_ms = kms / launches
     peak, peak_kind = measured_peak_gbs()
     achieved = kernel_bytes * n / (k_ms / 1e3) / 1e9
-    traffic = profiled_traffic(args.workload, "packed" if mixed else "f32")
+    traffic = profiled_traffic(args.workload, "split" if mixed else "f32")
 
     # End to end through the C ABI with FP32 host buffers: each step uploads velocity and
     # density from pinned host memory, steps, and downloads both.

@@ -389,7 +389,8 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
             if (value != HNS_RBGS_PLAIN && value != HNS_RBGS_BULK) fail(HNS_ERR_INVALID_ARG, "unknown red-black kernel");
             c->rbgs_kernel = value;
         } else if (option == HNS_OPT_INNER_LAYOUT) {
-            if (value != HNS_INNER_ROWS && value != HNS_INNER_PACKED) fail(HNS_ERR_INVALID_ARG, "unknown inner layout");
+            if (value != HNS_INNER_ROWS && value != HNS_INNER_PACKED && value != HNS_INNER_SPLIT)
+                fail(HNS_ERR_INVALID_ARG, "unknown inner layout");
             c->inner_layout = value;
         } else {
             fail(HNS_ERR_INVALID_ARG, "unknown option");

@@ -144,7 +144,7 @@ struct Context {
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
     int rbgs_kernel = HNS_RBGS_BULK;      // hns_set_option(HNS_OPT_RBGS_KERNEL)
-    int inner_layout = HNS_INNER_PACKED;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
+    int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -213,6 +213,13 @@ void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint6
 constexpr int kPackedFaceBytes = 1024;
 constexpr int kPackedHaloBytes = 640;
 void launch_rhs_halo_pack(const Context& c, const void* rhs, void* halo, const double* check, double tol2);
+// The FP16 inner solve on colour-split leaves (hns_rbgs_split.cu): the face-neighbour table
+// (8 ints per leaf, missing neighbours = the zero leaf L) and one in-place half-sweep (colour 0
+// red, 1 black). e holds L + 1 leaves, the last all zeros. e_zero: e = 0 before this red
+// half-sweep (the first of a solve).
+void launch_split_face_table(const Context& c, int* nb8);
+void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
+                            float omega, const double* check, double tol2);
 void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
                              void* e_out, void* faces_out, float omega, const double* check, double tol2);
 

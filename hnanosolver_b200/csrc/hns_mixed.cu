@@ -267,9 +267,26 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
 // row is stored at position (z & 1) * 4 + (z >> 1).
 __device__ __forceinline__ int64_t packed_slot(int64_t q) { return (q & ~int64_t(7)) | ((q & 1) << 2) | ((q >> 1) & 3); }
 
+// Slot of the colour-split layout (launch_rbgs_split_half): a leaf's red values, then its black
+// ones; within a colour, the row (x, y) = (a, b) at position R = 32 ((a + b) & 1) + 4 a + (b >> 1),
+// entry 4 R + (z >> 1).
+__device__ __forceinline__ int64_t split_slot(int64_t q) {
+    const int n = (int)(q & 511), a = n >> 6, b = (n >> 3) & 7, z = n & 7;
+    const int colour = (a + b + z) & 1;
+    const int row = 32 * ((a + b) & 1) + 4 * a + (b >> 1);
+    return (q & ~int64_t(511)) | (colour << 8) | (row << 2) | (z >> 1);
+}
+
+template <int kLayout>
+__device__ __forceinline__ int64_t inner_slot(int64_t q) {
+    if constexpr (kLayout == HNS_INNER_PACKED) return packed_slot(q);
+    else if constexpr (kLayout == HNS_INNER_SPLIT) return split_slot(q);
+    else return q;
+}
+
 // r^ = r / s with s = rms(r) from the latest check (stored into *scale); FP16 or FP32;
-// kPacked: r^ in the colour-packed layout.
-template <typename TI, bool kPacked>
+// r^ in the inner solve's layout kLayout.
+template <typename TI, int kLayout>
 __global__ void __launch_bounds__(kThreads) refine_scale_kernel(const float* __restrict__ r, TI* __restrict__ rhat,
                                                                  int64_t n, const double* __restrict__ check,
                                                                  double tol2, float* __restrict__ scale) {
@@ -279,18 +296,18 @@ __global__ void __launch_bounds__(kThreads) refine_scale_kernel(const float* __r
     const float inv = 1.0f / sc;
     if (blockIdx.x == 0 && threadIdx.x == 0) *scale = sc;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        sstore(rhat, kPacked ? packed_slot(q) : q, __ldg(r + q) * inv);
+        sstore(rhat, inner_slot<kLayout>(q), __ldg(r + q) * inv);
 }
 
-// p += s e (FP64), pointwise; kPacked: e in the colour-packed layout.
-template <typename TI, bool kPacked>
+// p += s e (FP64), pointwise; e in the inner solve's layout kLayout.
+template <typename TI, int kLayout>
 __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restrict__ p, const TI* __restrict__ e,
                                                                   int64_t n, const float* __restrict__ scale,
                                                                   const double* __restrict__ check, double tol2) {
     if (converged(check, tol2)) return;
     const double sc = (double)*scale;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        p[q] += sc * (double)sload(e, kPacked ? packed_slot(q) : q);
+        p[q] += sc * (double)sload(e, inner_slot<kLayout>(q));
 }
 
 unsigned stream_blocks(const Context& c, int64_t n) {
@@ -393,8 +410,18 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     const double h2 = (double)c.dx * (double)c.dx;
     const double tol2 = tol * tol;
     const unsigned g = stream_blocks(c, n);
-    // The FP16 inner solve runs on colour-packed rows unless the option selects the plain order.
-    const bool packed = sizeof(TI) == 2 && c.inner_layout == HNS_INNER_PACKED;
+    // The FP16 inner solve's layout is an option (colour-split, colour-packed or plain order).
+    const int layout = sizeof(TI) == 2 ? c.inner_layout : HNS_INNER_ROWS;
+    const bool packed = layout == HNS_INNER_PACKED;
+    // Colour-split: e in place with one extra all-zero leaf, and the face-neighbour table.
+    TI* e_split = nullptr;
+    int* nb8 = nullptr;
+    if (layout == HNS_INNER_SPLIT) {
+        e_split = reinterpret_cast<TI*>(c.scratch_f32("refine_e_split", ((size_t)(n + 512) * sizeof(TI) + 3) / 4));
+        nb8 = reinterpret_cast<int*>(c.scratch_f32("refine_split_nb8", (size_t)c.topo.num_leaves * 8));
+        HNS_CUDA(cudaMemsetAsync(e_split + n, 0, 512 * sizeof(TI), c.stream));
+        launch_split_face_table(c, nb8);
+    }
     // Packed: the face buffers of e[0] and e[1] and the rhs halo records.
     void* faces[2] = {nullptr, nullptr};
     void* halo = nullptr;
@@ -409,10 +436,12 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     HNS_LAUNCHED();
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
-        if (packed)
-            refine_scale_kernel<TI, true><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+        if (layout == HNS_INNER_PACKED)
+            refine_scale_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+        else if (layout == HNS_INNER_SPLIT)
+            refine_scale_kernel<TI, HNS_INNER_SPLIT><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         else
-            refine_scale_kernel<TI, false><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+            refine_scale_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         HNS_LAUNCHED();
         if (packed) launch_rhs_halo_pack(c, rhat, halo, chk, tol2);
         const TI* src = nullptr;
@@ -421,7 +450,12 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         for (int it = 0; it < plan.inner; ++it) {
             TI* dst = e[it & 1];
             if constexpr (sizeof(TI) == 2) {
-                if (packed) {
+                if (layout == HNS_INNER_SPLIT) {
+                    // In place: red, then black.
+                    dst = e_split;
+                    launch_rbgs_split_half(c, nb8, rhat, dst, 0, it == 0, omega, chk, tol2);
+                    launch_rbgs_split_half(c, nb8, rhat, dst, 1, false, omega, chk, tol2);
+                } else if (packed) {
                     launch_rbgs_packed_half(c, rhat, halo, src, src_faces, dst, faces[it & 1], omega, chk, tol2);
                     src_faces = faces[it & 1];
                 } else
@@ -432,10 +466,12 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
             src = dst;
         }
         c.phase_end();
-        if (packed)
-            refine_update_kernel<TI, true><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+        if (layout == HNS_INNER_PACKED)
+            refine_update_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+        else if (layout == HNS_INNER_SPLIT)
+            refine_update_kernel<TI, HNS_INNER_SPLIT><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
         else
-            refine_update_kernel<TI, false><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+            refine_update_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
         HNS_LAUNCHED();
         refine_residual_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
             c.topo.view, div, p, nullptr, r, h2, chk, tol2, plan.slots + 2 * (k + 1));

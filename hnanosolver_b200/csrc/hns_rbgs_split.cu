@@ -1,0 +1,204 @@
+// The red-black SOR half-sweep on colour-split FP16 leaves: the inner solve of the
+// mixed-precision refinement (L e = r with unit spacing, e and r in FP16, FP32 arithmetic), one
+// launch per colour, in place.
+//
+// Layout. The inner solve's arrays belong to the solver, so their layout is free. Each leaf
+// stores its 256 red values (colour (x + y + z) & 1 = 0) and then its 256 black values. Within
+// a colour, entry 4 R + j is the row (local x = a, y = b) at position
+// R = 32 ((a + b) & 1) + 4 a + (b >> 1), at the j-th z of that colour in the row:
+// z = 2 j + ((a + b + colour) & 1). A colour of a row is 8 contiguous bytes, and the 32 rows of
+// one parity of a + b are 256 contiguous bytes: one warp's load.
+//
+// Neighbours of voxel (a, b, z = 2 j + p) of colour c: its x and y neighbours are entry j of
+// the other colour in rows (a -+ 1, b) and (a, b -+ 1) (in the neighbour leaf across a face,
+// rows wrapped mod 8), all of the other parity of a + b; its z neighbours are entries of the
+// other colour of its own row: j - 1 and j for p = 0, j and j + 1 for p = 1, where entry -1 is
+// the -z leaf's entry 3 of that row and entry 4 the +z leaf's entry 0. A missing leaf reads 0
+// (the reference's p = 0 outside the domain).
+//
+// Work: a thread relaxes the four voxels of one colour of a row, in two leaves, from eight
+// 8-byte loads per leaf (the row's two colours, its right-hand side, the four neighbour rows)
+// and one of 2 bytes, and one 8-byte store. A half-sweep reads both colours of e and the
+// colour's right-hand side and writes the colour in place: about 3 bytes per voxel from DRAM,
+// with no staging, no halo copies and no second buffer of e. The update of each voxel is
+// relax16::relax1, the arithmetic of every other FP16 inner kernel, so all layouts give the
+// same values to the bit (the tests compare them). Sweeps follow redBlackGaussSeidelUpdate
+// (src/Cuda/Kernel.cu:459-489): red, then black, per iteration.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hns_internal.cuh"
+#include "hns_relax16.cuh"
+
+namespace hns {
+namespace {
+
+using namespace relax16;
+
+constexpr int kLeavesPerBlock = 4;   // leaves whose rows one block's threads cover
+constexpr int kLeavesPerThread = 2;  // leaves a thread relaxes its row in
+constexpr int kThreads = 64 * kLeavesPerBlock;
+
+// nbr27 indices of the six face neighbours: (dx+1)*9 + (dy+1)*3 + (dz+1).
+constexpr int kNbXp = 22, kNbXm = 4, kNbYp = 16, kNbYm = 10, kNbZp = 14, kNbZm = 12;
+
+__device__ __forceinline__ uint2 ld8(const __half* p) { return __ldg(reinterpret_cast<const uint2*>(p)); }
+// Loads that other threads of this launch may write: the colour being updated is only read by
+// the thread that writes it, so plain (non-.nc) loads of it are enough; the other colour is
+// read-only during the launch.
+__device__ __forceinline__ uint2 ld8_rw(const __half* p) { return *reinterpret_cast<const uint2*>(p); }
+
+__device__ __forceinline__ uint32_t half_at(uint2 v, int j) {
+    const uint32_t w = (j & 2) ? v.y : v.x;
+    return (j & 1) ? (w >> 16) : (w & 0xFFFFu);
+}
+
+__device__ __forceinline__ uint32_t pack2(float lo, float hi) {
+    const __half2 r = __floats2half2_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&r);
+}
+
+// Face-neighbour table of the half-sweep: per leaf {+x, -x, +y, -y, +z, -z, the leaf, 0}, a
+// missing neighbour replaced by the zero leaf (index L, just past the last leaf of e, which the
+// sweeps read and never write), so that no load needs a test.
+__global__ void split_face_table_kernel(TopoView t, int4* __restrict__ nb8) {
+    const int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= t.num_leaves) return;
+    const int* nb = t.nbr27 + l * 27;
+    const int L = (int)t.num_leaves;
+    auto f = [&](int k) { const int v = __ldg(nb + k); return v < 0 ? L : v; };
+    nb8[2 * l] = make_int4(f(kNbXp), f(kNbXm), f(kNbYp), f(kNbYm));
+    nb8[2 * l + 1] = make_int4(f(kNbZp), f(kNbZm), (int)l, 0);
+}
+
+// One row's update for z parity P of its colour (P = 0: z = 0, 2, 4, 6): z neighbours are
+// entries j - 1 and j (P = 0) or j and j + 1 (P = 1) of the row's other colour K, with ZC the
+// entry across the z face.
+template <int P>
+__device__ __forceinline__ uint2 relax_row(uint2 XP, uint2 XM, uint2 YP, uint2 YM, uint2 K, uint32_t ZC, uint2 B,
+                                           uint2 C, float omega) {
+    float v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t zm = P ? half_at(K, j) : (j > 0 ? half_at(K, j - 1) : ZC);
+        const uint32_t zp = P ? (j < 3 ? half_at(K, j + 1) : ZC) : half_at(K, j);
+        v[j] = relax1(half_at(XP, j), half_at(XM, j), half_at(YP, j), half_at(YM, j), zp, zm, half_at(B, j), half_at(C, j),
+                      omega);
+    }
+    return make_uint2(pack2(v[0], v[1]), pack2(v[2], v[3]));
+}
+
+// kZero: e = 0 before this (red) half-sweep, the first of a solve: every neighbour and old
+// value is 0, nothing of e is read, and the row's black entries are written as 0.
+//
+// Warp w of a leaf takes the 32 rows of parity w of a + b, lane l the row at R = 32 w + l
+// (a = l / 4, b = 2 (l % 4) + ((a + w) & 1)), so the z parity of the colour is uniform in a warp
+// and the z neighbours need no selects. A thread relaxes its row in kLeavesPerThread leaves
+// (kLeavesPerBlock apart), issuing every load before any arithmetic: the kernel is bound by
+// memory latency, and this doubles the bytes each thread has in flight. Loads are
+// unconditional: a row on a leaf face reads the neighbour leaf's row, a missing neighbour the
+// zero leaf. Offsets are 32-bit element counts (fewer than 2^22 leaves).
+template <bool kZero>
+__global__ void __launch_bounds__(kThreads) rbgs_split_half_kernel(const int* __restrict__ nb8,
+                                                                    const __half* __restrict__ rhs, __half* e,
+                                                                    int num_leaves, int colour, float omega,
+                                                                    const double* __restrict__ check, double tol2,
+                                                                    unsigned long long* __restrict__ counters) {
+    if (check != nullptr && check[0] <= tol2 * check[1]) return;  // the refinement has converged
+    if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, 1ull);  // launches that ran
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
+    const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
+    const int p = (w + colour) & 1;  // z parity of this colour in the warp's rows
+    const int leaf0 = (int)blockIdx.x * (kLeavesPerBlock * kLeavesPerThread) + (int)(threadIdx.x >> 6);
+    const uint32_t rowc = ((uint32_t)colour << 8) | (uint32_t)(4 * (32 * w + lane));  // own entries within a leaf
+    uint32_t own[kLeavesPerThread];
+    bool live[kLeavesPerThread];
+#pragma unroll
+    for (int k = 0; k < kLeavesPerThread; ++k) {
+        const int leaf = leaf0 + k * kLeavesPerBlock;
+        live[k] = leaf < num_leaves;
+        own[k] = ((uint32_t)(live[k] ? leaf : 0) << 9) | rowc;  // a dead slot reads leaf 0 and stores nothing
+    }
+    uint2 B[kLeavesPerThread], out[kLeavesPerThread];
+#pragma unroll
+    for (int k = 0; k < kLeavesPerThread; ++k) B[k] = ld8(rhs + own[k]);
+    if constexpr (kZero) {
+#pragma unroll
+        for (int k = 0; k < kLeavesPerThread; ++k) {
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = relax1(0u, 0u, 0u, 0u, 0u, 0u, half_at(B[k], j), 0u, omega);
+            out[k] = make_uint2(pack2(v[0], v[1]), pack2(v[2], v[3]));
+            if (live[k]) *reinterpret_cast<uint2*>(e + (own[k] ^ 256u)) = make_uint2(0u, 0u);
+        }
+    } else {
+        // Row (a', b') of the other parity in the other colour of leaf n.
+        const uint32_t co = ((uint32_t)(colour ^ 1) << 8) | (uint32_t)(128 * (w ^ 1));
+        auto row = [&](uint32_t n, int a2, int b2) { return (n << 9) | co | (uint32_t)(16 * a2 + 4 * (b2 >> 1)); };
+        const int sx = a == 7 ? 0 : a == 0 ? 1 : 6, sy = b == 7 ? 2 : b == 0 ? 3 : 6, sz = 5 - p;
+        uint32_t nx[kLeavesPerThread], ny[kLeavesPerThread], nz[kLeavesPerThread];
+#pragma unroll
+        for (int k = 0; k < kLeavesPerThread; ++k) {
+            const int* nb = nb8 + 8 * (own[k] >> 9);
+            nx[k] = (uint32_t)__ldg(nb + sx);
+            ny[k] = (uint32_t)__ldg(nb + sy);
+            nz[k] = (uint32_t)__ldg(nb + sz);  // -z leaf for p = 0, +z for p = 1
+        }
+        uint2 C[kLeavesPerThread], K[kLeavesPerThread], XP[kLeavesPerThread], XM[kLeavesPerThread],
+            YP[kLeavesPerThread], YM[kLeavesPerThread];
+        uint32_t ZC[kLeavesPerThread];
+#pragma unroll
+        for (int k = 0; k < kLeavesPerThread; ++k) {
+            C[k] = ld8_rw(e + own[k]);
+            K[k] = ld8(e + (own[k] ^ 256u));
+        }
+#pragma unroll
+        for (int k = 0; k < kLeavesPerThread; ++k) {
+            const uint32_t lf = own[k] >> 9;
+            XP[k] = ld8(e + row(a == 7 ? nx[k] : lf, (a + 1) & 7, b));
+            XM[k] = ld8(e + row(a == 0 ? nx[k] : lf, (a - 1) & 7, b));
+            YP[k] = ld8(e + row(b == 7 ? ny[k] : lf, a, (b + 1) & 7));
+            YM[k] = ld8(e + row(b == 0 ? ny[k] : lf, a, (b - 1) & 7));
+            ZC[k] = (uint32_t)__half_as_ushort(
+                __ldg(e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1)));
+        }
+#pragma unroll
+        for (int k = 0; k < kLeavesPerThread; ++k)
+            out[k] = p ? relax_row<1>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega)
+                       : relax_row<0>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega);
+    }
+#pragma unroll
+    for (int k = 0; k < kLeavesPerThread; ++k)
+        if (live[k]) *reinterpret_cast<uint2*>(e + own[k]) = out[k];
+}
+
+}  // namespace
+
+void launch_split_face_table(const Context& c, int* nb8) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0) return;
+    split_face_table_kernel<<<(unsigned)((L + 255) / 256), 256, 0, c.stream>>>(c.topo.view, reinterpret_cast<int4*>(nb8));
+    HNS_LAUNCHED();
+}
+
+void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
+                            float omega, const double* check, double tol2) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0) return;
+    if (L >= (int64_t(1) << 22)) fail(HNS_ERR_INVALID_ARG, "too many leaves for the colour-split inner solve");
+    const int per_block = kLeavesPerBlock * kLeavesPerThread;
+    const unsigned blocks = (unsigned)((L + per_block - 1) / per_block);
+    const auto* r = static_cast<const __half*>(rhs);
+    auto* x = static_cast<__half*>(e);
+    if (e_zero)
+        rbgs_split_half_kernel<true><<<blocks, kThreads, 0, c.stream>>>(nb8, r, x, (int)L, colour, omega, check, tol2,
+                                                                         c.counters);
+    else
+        rbgs_split_half_kernel<false><<<blocks, kThreads, 0, c.stream>>>(nb8, r, x, (int)L, colour, omega, check, tol2,
+                                                                          c.counters);
+    HNS_LAUNCHED();
+}
+
+}  // namespace hns

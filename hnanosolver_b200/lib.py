@@ -22,7 +22,7 @@ STATUS_NAMES = {
 OPT_RBGS_KERNEL = 1
 RBGS_PLAIN, RBGS_BULK = 0, 1
 OPT_INNER_LAYOUT = 2
-INNER_ROWS, INNER_PACKED = 0, 1
+INNER_ROWS, INNER_PACKED, INNER_SPLIT = 0, 1, 2
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 

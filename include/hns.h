@@ -322,8 +322,11 @@ HNS_API hns_status hns_adjoint_step_plain(hns_ctx* ctx, const float* vel_in, con
 #define HNS_OPT_INNER_LAYOUT 2 /* layout of the FP16 inner solve of the mixed-precision refinement: */
 #define HNS_INNER_ROWS 0       /*   the leaf-dense slot order, relaxed by the HNS_RBGS_BULK kernel */
 #define HNS_INNER_PACKED 1     /*   colour-packed rows (z = 0,2,4,6 then 1,3,5,7) with face buffers,
-                                    staged by TMA (default). Same results to the bit; the solver's
-                                    own arrays, never the caller's */
+                                    staged by TMA, both colours per launch */
+#define HNS_INNER_SPLIT 2      /*   colour-split leaves (a leaf's red values, then its black ones),
+                                    one in-place launch per colour (default). All three give the
+                                    same results to the bit; the solver's own arrays, never the
+                                    caller's */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */

@@ -134,10 +134,11 @@ def test_fp32_refined_reaches_tolerance_plain_fp32_cannot(dev, shell):
 
 
 @pytest.mark.parametrize("grid", ["shell", "spheres"])
-def test_packed_inner_solve_bit_exact_with_row_order(dev, shell, grid):
-    """The FP16 inner solve on colour-packed rows (the default) and on the plain slot order
-    relax every voxel with the same arithmetic, so the whole mixed step -- refined pressure,
-    outer iteration count, projected velocity, advected density -- is identical to the bit.
+def test_inner_solve_layouts_bit_exact(dev, shell, grid):
+    """The FP16 inner solve on colour-split leaves (the default), on colour-packed rows and on
+    the plain slot order relax every voxel with the same arithmetic, so the whole mixed step --
+    refined pressure, outer iteration count, projected velocity, advected density -- is
+    identical to the bit.
     The sparse spheres exercise missing neighbour leaves (face rings and z rings left at 0)."""
     from hnanosolver_b200 import lib as hl
 
@@ -147,7 +148,7 @@ def test_packed_inner_solve_bit_exact_with_row_order(dev, shell, grid):
         origins = synth.spheres_topology(96, 3, 8.0, 20.0, seed=11)
         dens, vel = synth.noise_fields(origins, seed=7)
     out = {}
-    for layout in (hl.INNER_ROWS, hl.INNER_PACKED):
+    for layout in (hl.INNER_ROWS, hl.INNER_PACKED, hl.INNER_SPLIT):
         g = hl.Grid(origins, voxel_size=0.1)
         g.set_option(hl.OPT_INNER_LAYOUT, layout)
         vb, dh, vo, do, info = _mixed(g, dev, dens, vel, inner=30, outer=12)
@@ -157,9 +158,11 @@ def test_packed_inner_solve_bit_exact_with_row_order(dev, shell, grid):
         torch.cuda.synchronize()
         out[layout] = (vo.cpu(), do.cpu(), p.cpu(), outer, res, info.iterations)
         g.close()
-    a, b = out[hl.INNER_ROWS], out[hl.INNER_PACKED]
-    assert a[3] == b[3] and a[5] == b[5]
-    assert a[4] == pytest.approx(b[4], rel=1e-12)  # FP64 atomics: summation order varies
-    assert torch.equal(a[2], b[2])
-    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
-    assert b[4] <= 1e-5
+    a = out[hl.INNER_ROWS]
+    for layout in (hl.INNER_PACKED, hl.INNER_SPLIT):
+        b = out[layout]
+        assert a[3] == b[3] and a[5] == b[5]
+        assert a[4] == pytest.approx(b[4], rel=1e-12)  # FP64 atomics: summation order varies
+        assert torch.equal(a[2], b[2])
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+        assert b[4] <= 1e-5
