@@ -30,7 +30,7 @@ constexpr int kThreads = 256;
 // the lerp-chain trilinear velocity there -- so the trace and the 8+8 tap addresses are
 // computed once and every field is sampled from them. vel_out may be null (scalars only) and
 // f.count may be 0 (velocity only); each output equals the reference kernel's.
-__global__ void __launch_bounds__(kThreads) advect_fused_kernel(TopoView t, const float* __restrict__ vel,
+__global__ void __launch_bounds__(kThreads, 3) advect_fused_kernel(TopoView t, const float* __restrict__ vel,
                                                                  float* __restrict__ vel_out, FieldSet f, float sdt) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
@@ -45,8 +45,8 @@ __global__ void __launch_bounds__(kThreads) advect_fused_kernel(TopoView t, cons
     const float3 vf = tri_v(tb, vel);
     taps_at(tf, t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt);
     // Face neighbours in the reference's clamp order: x-1, x+1, y-1, y+1, z-1, z+1.
-    const int64_t ns[6] = {slot_of(t, L, i - 1, j, k), slot_of(t, L, i + 1, j, k), slot_of(t, L, i, j - 1, k),
-                           slot_of(t, L, i, j + 1, k), slot_of(t, L, i, j, k - 1), slot_of(t, L, i, j, k + 1)};
+    int64_t ns[6];
+    face_slots(L, s, v.n, ns);
     if (vel_out != nullptr) {
         const float3 vb = tri_v(tf, vel);
         float3 corr = make_float3(vf.x + 0.5f * (vo.x - vb.x), vf.y + 0.5f * (vo.y - vb.y), vf.z + 0.5f * (vo.z - vb.z));

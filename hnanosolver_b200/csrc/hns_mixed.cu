@@ -106,7 +106,7 @@ struct FieldSetT {
 // advect_vector + advect_scalar along one shared trace (as advect_fused_kernel), reading and
 // writing reduced-precision storage.
 template <typename V, typename S>
-__global__ void __launch_bounds__(kThreads) advect_mixed_kernel(TopoView t, const V* __restrict__ vel,
+__global__ void __launch_bounds__(kThreads, 3) advect_mixed_kernel(TopoView t, const V* __restrict__ vel,
                                                                  V* __restrict__ vel_out, FieldSetT<S> f, float sdt) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(kThreads) advect_mixed_kernel(TopoView t, cons
     taps_at(tb, t, L, bx, by, bz);
     const float3 vf = tri3(tb, vel);
     taps_at(tf, t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt);
-    const int64_t ns[6] = {slot_of(t, L, i - 1, j, k), slot_of(t, L, i + 1, j, k), slot_of(t, L, i, j - 1, k),
-                           slot_of(t, L, i, j + 1, k), slot_of(t, L, i, j, k - 1), slot_of(t, L, i, j, k + 1)};
+    int64_t ns[6];
+    face_slots(L, s, v.n, ns);
     if (vel_out != nullptr) {
         const float3 vb = tri3(tf, vel);
         float3 corr = make_float3(vf.x + 0.5f * (vo.x - vb.x), vf.y + 0.5f * (vo.y - vb.y), vf.z + 0.5f * (vo.z - vb.z));

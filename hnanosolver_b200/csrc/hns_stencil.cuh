@@ -118,13 +118,50 @@ struct Taps {
     float tx, ty, tz;
 };
 
+// The cell's two planes along each axis are resolved once: when both lie in the CTA leaf's
+// 3x3x3 neighbourhood (every trace shorter than a leaf), each corner's leaf is one
+// shared-memory lookup at a precomputed index and its slot an OR of precomputed local
+// offsets; otherwise every corner goes through slot_of (and the leaf table).
 __device__ __forceinline__ void taps_at(Taps& T, const TopoView& t, const LeafNbhd& L, float x, float y, float z) {
     const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
     T.tx = x - (float)i;
     T.ty = y - (float)j;
     T.tz = z - (float)k;
+    const int a0 = (i >> 3) - L.lx + 1, a1 = ((i + 1) >> 3) - L.lx + 1;
+    const int b0 = (j >> 3) - L.ly + 1, b1 = ((j + 1) >> 3) - L.ly + 1;
+    const int c0 = (k >> 3) - L.lz + 1, c1 = ((k + 1) >> 3) - L.lz + 1;
+    if ((unsigned)a0 < 3u && (unsigned)a1 < 3u && (unsigned)b0 < 3u && (unsigned)b1 < 3u && (unsigned)c0 < 3u &&
+        (unsigned)c1 < 3u) {
+        const int na[2] = {a0 * 9, a1 * 9}, nb[2] = {b0 * 3, b1 * 3}, nc[2] = {c0, c1};
+        const int la[2] = {(i & 7) << 6, ((i + 1) & 7) << 6}, lb[2] = {(j & 7) << 3, ((j + 1) & 7) << 3};
+        const int lc[2] = {k & 7, (k + 1) & 7};
 #pragma unroll
-    for (int q = 0; q < 8; ++q) T.s[q] = slot_of(t, L, i + (q >> 2), j + ((q >> 1) & 1), k + (q & 1));
+        for (int q = 0; q < 8; ++q) {
+            const int A = q >> 2, B = (q >> 1) & 1, C = q & 1;
+            const int l = L.nb[na[A] + nb[B] + nc[C]];
+            T.s[q] = l < 0 ? -1 : ((int64_t)l << 9) + (la[A] | lb[B] | lc[C]);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) T.s[q] = slot_of(t, L, i + (q >> 2), j + ((q >> 1) & 1), k + (q & 1));
+    }
+}
+
+// Slots of the six face neighbours of local voxel n of the CTA's leaf (slot s), -1 outside the
+// domain, in the order x-1, x+1, y-1, y+1, z-1, z+1: the leaf's own slots unless the
+// neighbour is across a face, then the face neighbour from the staged neighbourhood.
+__device__ __forceinline__ void face_slots(const LeafNbhd& L, int64_t s, int n, int64_t ns[6]) {
+    const int a = n >> 6, b = (n >> 3) & 7, c = n & 7;
+    auto across = [&](int idx, int local) -> int64_t {
+        const int l = L.nb[idx];
+        return l < 0 ? -1 : ((int64_t)l << 9) + local;
+    };
+    ns[0] = a > 0 ? s - 64 : across(4, n | (7 << 6));
+    ns[1] = a < 7 ? s + 64 : across(22, n & 63);
+    ns[2] = b > 0 ? s - 8 : across(10, n | (7 << 3));
+    ns[3] = b < 7 ? s + 8 : across(16, n & ~(7 << 3));
+    ns[4] = c > 0 ? s - 1 : across(12, n | 7);
+    ns[5] = c < 7 ? s + 1 : across(14, n & ~7);
 }
 
 __device__ __forceinline__ float tap_s(const float* __restrict__ d, int64_t s) { return s < 0 ? 0.f : __ldg(d + s); }
