@@ -213,6 +213,86 @@ def _timed_steps(torch, stream, fn, steps):
     return e0.elapsed_time(e1)
 
 
+# Pass-model bytes per voxel-step of the adjoint plain step in FP32 (transposes of the forward
+# passes, scatters counted as read-modify-write): gradient^T 16, adjoint copies and zeroing 16,
+# red-black^T 12 per half-sweep (read lambda, write lambda, read-modify-write of div_bar on the
+# colour) x 2 x iterations, divergence^T 28, velocity advection^T 48, scalar advection^T 52.
+def adjoint_step_bytes(iters):
+    return 16 + 16 + 24 * iters + 28 + 48 + 52
+
+
+def adjoint_rollout(torch, hl, synth, dev, steps=16, every=4, iters=60):
+    """Reverse pass of a checkpointed rollout through the C ABI, for the differentiable-rollout
+    configuration: 128^3 fully active (2,097,152 voxels), K = 16 plain steps of advect (velocity
+    and density) + project with 60 red-black iterations (omega 1, from p = 0), the state kept
+    every 4 steps, loss 1/2 |rho_K - rho_target|^2 (target: seed-1 smoothed noise). The forward
+    keeps the checkpoints; the backward recomputes each segment's step inputs from its
+    checkpoint and runs hns_adjoint_step_plain on them in reverse. CUDA events on the grid's
+    stream; one untimed pass first."""
+    origins = synth.topology("box128")
+    dens, vel = synth.smoothed_fields(origins, seed=0, box_passes=3)
+    target, _ = synth.smoothed_fields(origins, seed=1, box_passes=3)
+    n = len(dens)
+    g = hl.Grid(origins, voxel_size=0.1)
+    stream = torch.cuda.Stream(device=dev)
+    g.set_stream(stream.cuda_stream)
+    desc = hl.StepDesc(dt=0.1, max_iterations=iters, omega=1.0, tolerance=0.0, check_every=0, flags=0)
+    v0, d0 = torch.from_numpy(vel).to(dev), torch.from_numpy(dens).to(dev)
+    tg = torch.from_numpy(target).to(dev)
+    torch.cuda.synchronize()
+
+    def step(v, d):
+        v2, d2 = torch.empty_like(v), torch.empty_like(d)
+        g.step_plain(v, v2, [d], [d2], desc)
+        return v2, d2
+
+    def forward():
+        ckpt, v, d = [], v0, d0
+        for k in range(steps):
+            if k % every == 0:
+                ckpt.append((v, d))  # each step writes new tensors, so no copy is needed
+            v, d = step(v, d)
+        return ckpt, d
+
+    def backward(ckpt, dk):
+        vb, db = torch.zeros_like(v0), dk - tg
+        for seg in reversed(range(len(ckpt))):
+            k0 = seg * every
+            states = [ckpt[seg]]
+            for _ in range(k0, min(k0 + every, steps) - 1):
+                states.append(step(*states[-1]))
+            for v_in, d_in in reversed(states):
+                vi, di = torch.zeros_like(vb), torch.zeros_like(db)
+                g.adjoint_step_plain(v_in, [d_in], vb, [db], vi, [di], desc.dt, iters, desc.omega)
+                vb, db = vi, di
+        return vb, db
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    with torch.cuda.stream(stream):
+        backward(*forward())
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        ckpt, dk = forward()
+        ev[1].record(stream)
+        backward(ckpt, dk)
+        ev[2].record(stream)
+    torch.cuda.synchronize()
+    f_ms, b_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    g.close()
+    recomputed = steps - (steps + every - 1) // every
+    # The forward plain step's pass model (FP32, one scalar): advect velocity 24, divergence 16,
+    # 12 per red-black iteration, gradient 28, the velocity written once more 12, density 8.
+    fwd_bytes = 24 + 16 + 12 * iters + 28 + 12 + 8
+    moved = (adjoint_step_bytes(iters) * steps + fwd_bytes * recomputed) * n
+    return {"workload": "box128 rollout: 128^3 fully active, 16 steps of advect + project, 60 red-black iterations, "
+                        "checkpoint every 4 steps, loss 1/2 |rho_K - rho_target|^2",
+            "voxels": n, "steps": steps, "checkpoint_every": every, "iterations": iters,
+            "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
+            "value": n * steps / (b_ms / 1e3), "unit": "voxel-steps/s (reverse pass, recomputation included)",
+            "adjoint_step_bytes_per_voxel": adjoint_step_bytes(iters), "recomputed_steps": recomputed,
+            "achieved_gbs": moved / (b_ms / 1e3) / 1e9}
+
+
 def ours(args, wl):
     import torch
 
@@ -379,6 +459,9 @@ def ours(args, wl):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, wl, info32.iterations)
+    adjoint = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adjoint = adjoint_rollout(torch, hl, synth, dev)
 
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
@@ -411,6 +494,7 @@ def ours(args, wl):
                     "path": ("hns_step_mixed_host" if mixed else "hns_step_plain_host") + " (C ABI, pinned FP32 host buffers)"},
             "gpu_launches": args.steps * launches_per_step,
             "clocks": clk,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     g.close()
@@ -427,6 +511,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="shell512")
     ap.add_argument("--precision", choices=["mixed", "fp32"], default="mixed")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout measured beside the step")
     ap.add_argument("--no-fp32-comparison", action="store_true",
                     help="skip the FP32 forms measured beside the mixed one (profiling runs)")
     args = ap.parse_args()

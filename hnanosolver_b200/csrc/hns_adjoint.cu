@@ -345,28 +345,70 @@ __global__ void __launch_bounds__(kThreads) adj_gradient_kernel(TopoView t, cons
     p_bar[s] += h * g;
 }
 
-// Adjoint of one colour-c half-sweep of redBlackGaussSeidelUpdate, lam_in (the adjoint after
-// the half-sweep) -> lam_out (before): a colour-c voxel's update p = (1 - omega) p +
-// omega / 6 (sum of neighbours - div dx^2) gives it lam (1 - omega), gives each of its (other
-// colour) neighbours omega / 6 lam, and gives div_bar -dx^2 omega / 6 lam.
-__global__ void __launch_bounds__(kThreads) adj_rbgs_half_kernel(TopoView t, const float* __restrict__ lam_in,
-                                                                 float* __restrict__ lam_out, float* __restrict__ div_bar,
-                                                                 int colour, float omega, float dx2, int64_t n) {
-    const int64_t s = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-    if (s >= n) return;
-    int i, j, k;
-    coords_of(t, s, i, j, k);
-    const float a = omega * dev::kInv6;
-    const float l = __ldg(lam_in + s);
-    if (((i + j + k) & 1) == colour) {
-        lam_out[s] = (1.f - omega) * l;
-        div_bar[s] -= dx2 * a * l;
-    } else {
-        const float sum = val_s(lam_in, slot_at(t, i + 1, j, k)) + val_s(lam_in, slot_at(t, i - 1, j, k)) +
-                          val_s(lam_in, slot_at(t, i, j + 1, k)) + val_s(lam_in, slot_at(t, i, j - 1, k)) +
-                          val_s(lam_in, slot_at(t, i, j, k + 1)) + val_s(lam_in, slot_at(t, i, j, k - 1));
-        lam_out[s] = l + a * sum;
+// Adjoint of one colour-c half-sweep of redBlackGaussSeidelUpdate, in place on lam. The forward
+// half-sweep sets p(c) = (1 - omega) p(c) + omega / 6 (sum of the neighbours - div dx^2) on
+// colour c and keeps colour c'; its transpose, from the adjoint lam' after it, gives
+//   lam(c') = lam'(c') + omega / 6 sum of the (colour c) neighbours of lam',
+//   div_bar(c) -= dx^2 omega / 6 lam'(c),   lam(c) = (1 - omega) lam'(c).
+// The last factor is uniform over a colour, so the caller keeps it as a scale per colour: the
+// true lam is scale_colour x the stored values. This launch writes colour c' fully scaled
+// (keep = the old scale of c', nbr = omega / 6 x the scale of c) and only reads colour c, so it
+// runs in place; the caller then sets the scale of c' to 1 and multiplies that of c by
+// (1 - omega).
+//
+// One thread per z-row of a leaf (64 per leaf, 4 leaves per CTA): it loads its row and the four
+// x/y neighbour rows as 32-byte vectors (the neighbour leaf's row across a face, zeros for a
+// missing leaf) and the two values across the z faces, updates the 4 voxels of colour c' and
+// stores them one by one (the row's colour-c values are read by other threads), and updates
+// div_bar on the 4 voxels of colour c of its row, which only it touches.
+constexpr int kRowLeavesPerBlock = 4;
+
+__device__ __forceinline__ void ld_row(const float* __restrict__ p, float v[8]) {
+    const float4 lo = *reinterpret_cast<const float4*>(p), hi = *reinterpret_cast<const float4*>(p + 4);
+    v[0] = lo.x, v[1] = lo.y, v[2] = lo.z, v[3] = lo.w, v[4] = hi.x, v[5] = hi.y, v[6] = hi.z, v[7] = hi.w;
+}
+
+__global__ void __launch_bounds__(64 * kRowLeavesPerBlock) adj_rbgs_colour_kernel(TopoView t, float* lam,
+                                                                                  float* __restrict__ div_bar,
+                                                                                  int colour, float keep, float nbr,
+                                                                                  float dmul) {
+    const int64_t leaf = (int64_t)blockIdx.x * kRowLeavesPerBlock + (threadIdx.x >> 6);
+    if (leaf >= t.num_leaves) return;
+    const int r = threadIdx.x & 63, a = r >> 3, b = r & 7;
+    const int* nb = t.nbr27 + leaf * 27;
+    // nbr27: (dx+1)*9 + (dy+1)*3 + (dz+1); entry 13 is the leaf itself.
+    const int nx = __ldg(nb + (a == 7 ? 22 : a == 0 ? 4 : 13)), ny = __ldg(nb + (b == 7 ? 16 : b == 0 ? 10 : 13));
+    const int nzm = __ldg(nb + 12), nzp = __ldg(nb + 14);
+    const int64_t own = (leaf << 9) + 8 * r;
+    // Rows (a +- 1, b) and (a, b +- 1): in this leaf, or across the face (missing: this row, zeroed).
+    auto across = [&](int n, int row) -> int64_t { return n < 0 ? own : ((int64_t)n << 9) + 8 * row; };
+    const int64_t oxp = a < 7 ? own + 64 : across(nx, b), oxm = a > 0 ? own - 64 : across(nx, 56 + b);
+    const int64_t oyp = b < 7 ? own + 8 : across(ny, 8 * a), oym = b > 0 ? own - 8 : across(ny, 8 * a + 7);
+    const bool zxp = a == 7 && nx < 0, zxm = a == 0 && nx < 0, zyp = b == 7 && ny < 0, zym = b == 0 && ny < 0;
+    float c[8], xp[8], xm[8], yp[8], ym[8];
+    ld_row(lam + own, c);
+    ld_row(lam + oxp, xp);
+    ld_row(lam + oxm, xm);
+    ld_row(lam + oyp, yp);
+    ld_row(lam + oym, ym);
+    const float zlo = nzm < 0 ? 0.f : lam[((int64_t)nzm << 9) + 8 * r + 7];
+    const float zhi = nzp < 0 ? 0.f : lam[((int64_t)nzp << 9) + 8 * r];
+    float d[8];
+    ld_row(div_bar + own, d);
+    const int pc = (a + b + colour) & 1;  // z parity of colour c in this row
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+        if ((z & 1) == pc) {
+            d[z] -= dmul * c[z];
+        } else {
+            const float sx = (zxp ? 0.f : xp[z]) + (zxm ? 0.f : xm[z]);
+            const float sy = (zyp ? 0.f : yp[z]) + (zym ? 0.f : ym[z]);
+            const float sz = (z < 7 ? c[z + 1] : zhi) + (z > 0 ? c[z - 1] : zlo);
+            lam[own + z] = keep * c[z] + nbr * (sx + sy + sz);
+        }
     }
+    *reinterpret_cast<float4*>(div_bar + own) = make_float4(d[0], d[1], d[2], d[3]);
+    *reinterpret_cast<float4*>(div_bar + own + 4) = make_float4(d[4], d[5], d[6], d[7]);
 }
 
 // ---- vorticity confinement ------------------------------------------------------------------
@@ -501,11 +543,11 @@ void launch_adj_gradient(const Context& c, const float* out_bar, float* p_bar) {
     HNS_LAUNCHED();
 }
 
-void launch_adj_rbgs_half(const Context& c, const float* lam_in, float* lam_out, float* div_bar, int colour, float omega) {
-    const int64_t n = c.num_voxels();
-    if (n == 0) return;
-    adj_rbgs_half_kernel<<<blocks_for(n), kThreads, 0, c.stream>>>(c.topo.view, lam_in, lam_out, div_bar, colour, omega,
-                                                                   c.dx * c.dx, n);
+void launch_adj_rbgs_colour(const Context& c, float* lam, float* div_bar, int colour, float keep, float nbr, float dmul) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0) return;
+    adj_rbgs_colour_kernel<<<(unsigned)((L + kRowLeavesPerBlock - 1) / kRowLeavesPerBlock), 64 * kRowLeavesPerBlock, 0,
+                             c.stream>>>(c.topo.view, lam, div_bar, colour, keep, nbr, dmul);
     HNS_LAUNCHED();
 }
 
@@ -526,19 +568,24 @@ namespace hns {
 namespace {
 
 // The adjoint of `iterations` red-black iterations from p = 0 (the forward's
-// HNS_SOLVE_ZERO_INIT): the iterations' transposes in reverse order, black half first.
+// HNS_SOLVE_ZERO_INIT): the half-sweeps' transposes in reverse order, black first, in place on
+// a copy of p_bar with one scale per colour (adj_rbgs_colour_kernel). The adjoint with respect
+// to the initial p is not needed (p starts at 0), so lam is never rescaled at the end.
 void adj_rbgs(Context& c, const float* p_bar, float* div_bar, int iterations, float omega) {
     if (iterations <= 0) return;
     const size_t n = (size_t)c.num_voxels();
-    float* lam[2] = {c.scratch_f32("adjoint_lam0", n), c.scratch_f32("adjoint_lam1", n)};
-    HNS_CUDA(cudaMemcpyAsync(lam[0], p_bar, n * sizeof(float), cudaMemcpyDeviceToDevice, c.stream));
-    int cur = 0;
-    for (int it = 0; it < iterations; ++it) {
-        launch_adj_rbgs_half(c, lam[cur], lam[cur ^ 1], div_bar, 1, omega);
-        cur ^= 1;
-        launch_adj_rbgs_half(c, lam[cur], lam[cur ^ 1], div_bar, 0, omega);
-        cur ^= 1;
-    }
+    float* lam = c.scratch_f32("adjoint_lam", n);
+    HNS_CUDA(cudaMemcpyAsync(lam, p_bar, n * sizeof(float), cudaMemcpyDeviceToDevice, c.stream));
+    const float a = omega * dev::kInv6;
+    const float dx2 = c.dx * c.dx;
+    float scale[2] = {1.f, 1.f};  // red, black
+    for (int it = 0; it < iterations; ++it)
+        for (int colour = 1; colour >= 0; --colour) {
+            const int other = colour ^ 1;
+            launch_adj_rbgs_colour(c, lam, div_bar, colour, scale[other], a * scale[colour], dx2 * a * scale[colour]);
+            scale[other] = 1.f;
+            scale[colour] *= 1.f - omega;
+        }
 }
 
 // vel_bar (the adjoint of the projected velocity) -> the adjoint of the velocity before the

@@ -233,7 +233,7 @@ void launch_adj_advect_scalar(const Context& c, const float* vel, const float* i
 void launch_adj_advect_vec3(const Context& c, const float* vel, const float* out_bar, float* vel_bar, float dt);
 void launch_adj_divergence(const Context& c, const float* div_bar, float* vel_bar);
 void launch_adj_gradient(const Context& c, const float* out_bar, float* p_bar);
-void launch_adj_rbgs_half(const Context& c, const float* lam_in, float* lam_out, float* div_bar, int colour, float omega);
+void launch_adj_rbgs_colour(const Context& c, float* lam, float* div_bar, int colour, float keep, float nbr, float dmul);
 void launch_adj_confinement(const Context& c, const float* vel, const float* out_bar, float* vel_bar, float dt,
                             float scale, float factor_scale);
 void launch_adj_accumulate(const Context& c, const float* src, float* dst, int64_t n);
