@@ -40,7 +40,10 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     "shell512": dict(desc="512^3 box, 16-voxel band (+ leaf half-diagonal) around a seeded radius-200 sphere, "
                           "fields: value-noise density, value-noise velocity in (-1,1)",
-                     dx=0.1, dt=0.1, omega=1.8, omega_refined=1.9, inner=30, tolerance=1e-5, cap=3000, check_every=10,
+                     # omega_refined / inner: the refinement's inner SOR factor and iterations per outer step,
+                     # the fastest to 1e-5 in a sweep of 1.85-1.96 x 16-90 (they also serve the FP32 refinement).
+                     # omega: plain FP32 SOR, the fastest that reaches 1e-5 (1.84 and above stall near 1.2e-5).
+                     dx=0.1, dt=0.1, omega=1.82, omega_refined=1.92, inner=36, tolerance=1e-5, cap=3000, check_every=10,
                      fp32_iterations=620),
     "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60",
                      dx=0.1, dt=1.0 / 24.0, omega=1.8, omega_refined=1.9, inner=30, tolerance=1e-5, cap=3000,
