@@ -195,6 +195,11 @@ double* Context::reduce_slots(int count) {
     return d_reduce.as<double>();
 }
 
+void Context::ensure_aux() {
+    if (aux_stream == nullptr) HNS_CUDA(cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking));
+    if (aux_ready == nullptr) HNS_CUDA(cudaEventCreateWithFlags(&aux_ready, cudaEventDisableTiming));
+}
+
 void Context::phase_begin(int phase) {
     if (!profiling) return;
     PhaseEvent e{phase, nullptr, nullptr};
@@ -351,6 +356,11 @@ HNS_API hns_status hns_destroy(hns_ctx* ctx) {
         Context& c = ctx->impl;
         DeviceGuard g(c.device);
         if (c.stream) (void)cudaStreamSynchronize(c.stream);
+        if (c.aux_stream) {
+            (void)cudaStreamSynchronize(c.aux_stream);
+            (void)cudaStreamDestroy(c.aux_stream);
+        }
+        if (c.aux_ready) (void)cudaEventDestroy(c.aux_ready);
         for (auto& e : c.phase_events) {
             (void)cudaEventDestroy(e.start);
             (void)cudaEventDestroy(e.stop);

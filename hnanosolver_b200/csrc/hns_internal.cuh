@@ -132,6 +132,11 @@ struct Context {
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    // A second stream for copies that can overlap the step (the host-buffer forms), made on
+    // first use, and the event that orders it after the main stream.
+    cudaStream_t aux_stream = nullptr;
+    cudaEvent_t aux_ready = nullptr;
+    void ensure_aux();
     float dx = 0.f;
     Topology topo;
     // Scratch owned by the context, grown on demand and reused across calls.

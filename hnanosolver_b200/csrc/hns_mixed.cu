@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -203,10 +204,22 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
 
 // ---- refinement --------------------------------------------------------------------------
 
-// r = b - L p (FP64; p null means p = 0, and p_zero_out then receives zeros), stored FP32;
-// acc += {sum r^2, sum b^2}. One block per leaf: the leaf's p and its six one-voxel face halos
-// (0 where the neighbour leaf does not exist) are read with coalesced loads into a 10^3 tile,
-// and each thread forms the Laplacian of two voxels from it, in the order of residual_kernel.
+// r = b - L p (FP64 arithmetic, r stored FP32) with b = div dx^2 and p = 0 outside the domain,
+// plus sum r^2 and sum b^2 into acc. p null: p = 0 (r = b), and p_zero_out, when set, is
+// cleared. One thread per z-row of a leaf (64 per leaf, kResidualLeaves leaves per CTA): its
+// row and the four x/y neighbour rows (the neighbour leaf's row across a face, 0 for a missing
+// leaf) as 16-byte loads and the two values across the z faces, with the Laplacian summed in
+// the order +x, -x, +y, -y, +z, -z, -6 p.
+constexpr int kResidualLeaves = kThreads / 64;
+
+__device__ __forceinline__ void ld_row8(const double* __restrict__ q, double v[8]) {
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+        const double2 x = __ldg(reinterpret_cast<const double2*>(q) + h);
+        v[2 * h] = x.x, v[2 * h + 1] = x.y;
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, const float* __restrict__ div,
                                                                     const double* __restrict__ p,
                                                                     double* __restrict__ p_zero_out,
@@ -214,51 +227,55 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
                                                                     const double* __restrict__ check, double tol2,
                                                                     double* __restrict__ acc) {
     if (converged(check, tol2)) return;
-    __shared__ double P[10][10][10];  // (a + 1, b + 1, z + 1)
-    const int64_t leaf = blockIdx.x;
-    const int tid = threadIdx.x;
-    if (p != nullptr) {
-        const double* pl = p + (leaf << 9);
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int n = tid + h * kThreads;
-            P[(n >> 6) + 1][((n >> 3) & 7) + 1][(n & 7) + 1] = __ldg(pl + n);
-        }
-        for (int f = tid; f < 6 * 64; f += kThreads) {
-            const int face = f >> 6, u = (f >> 3) & 7, v = f & 7;
-            int q, slot;
-            double* dst;
-            switch (face) {
-                case 0: q = 4, slot = 7 * 64 + u * 8 + v, dst = &P[0][u + 1][v + 1]; break;    // -x: x = 7
-                case 1: q = 22, slot = u * 8 + v, dst = &P[9][u + 1][v + 1]; break;            // +x: x = 0
-                case 2: q = 10, slot = u * 64 + 7 * 8 + v, dst = &P[u + 1][0][v + 1]; break;   // -y: y = 7
-                case 3: q = 16, slot = u * 64 + v, dst = &P[u + 1][9][v + 1]; break;           // +y: y = 0
-                case 4: q = 12, slot = u * 64 + v * 8 + 7, dst = &P[u + 1][v + 1][0]; break;   // -z: z = 7
-                default: q = 14, slot = u * 64 + v * 8, dst = &P[u + 1][v + 1][9]; break;      // +z: z = 0
-            }
-            const int l = __ldg(t.nbr27 + leaf * 27 + q);
-            *dst = l >= 0 ? __ldg(p + ((int64_t)l << 9) + slot) : 0.0;
-        }
-        __syncthreads();
-    }
+    const int64_t leaf = (int64_t)blockIdx.x * kResidualLeaves + (threadIdx.x >> 6);
+    const int row = threadIdx.x & 63, a = row >> 3, b = row & 7;
     double r2 = 0.0, b2 = 0.0;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int n = tid + h * kThreads;
-        const int a = (n >> 6) + 1, b = ((n >> 3) & 7) + 1, z = (n & 7) + 1;
-        const int64_t s = (leaf << 9) + n;
-        const double bb = (double)__ldg(div + s) * h2;
-        double res = bb;
+    if (leaf < t.num_leaves) {
+        const int64_t own = (leaf << 9) + 8 * row;
+        const float4 d0 = __ldg(reinterpret_cast<const float4*>(div + own));
+        const float4 d1 = __ldg(reinterpret_cast<const float4*>(div + own) + 1);
+        const float dv[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+        double res[8];
         if (p != nullptr) {
-            const double lap = P[a + 1][b][z] + P[a - 1][b][z] + P[a][b + 1][z] + P[a][b - 1][z] + P[a][b][z + 1] +
-                               P[a][b][z - 1] - 6.0 * P[a][b][z];
-            res = bb - lap;
-        } else if (p_zero_out != nullptr) {
-            p_zero_out[s] = 0.0;
+            const int* nb = t.nbr27 + leaf * 27;
+            // nbr27: (dx+1)*9 + (dy+1)*3 + (dz+1); entry 13 is the leaf itself.
+            const int nx = __ldg(nb + (a == 7 ? 22 : a == 0 ? 4 : 13)), ny = __ldg(nb + (b == 7 ? 16 : b == 0 ? 10 : 13));
+            const int nzm = __ldg(nb + 12), nzp = __ldg(nb + 14);
+            auto across = [&](int n, int rw) -> int64_t { return n < 0 ? own : ((int64_t)n << 9) + 8 * rw; };
+            double c[8], xp[8], xm[8], yp[8], ym[8];
+            ld_row8(p + own, c);
+            ld_row8(p + (a < 7 ? own + 64 : across(nx, b)), xp);
+            ld_row8(p + (a > 0 ? own - 64 : across(nx, 56 + b)), xm);
+            ld_row8(p + (b < 7 ? own + 8 : across(ny, 8 * a)), yp);
+            ld_row8(p + (b > 0 ? own - 8 : across(ny, 8 * a + 7)), ym);
+            const double zlo = nzm < 0 ? 0.0 : __ldg(p + ((int64_t)nzm << 9) + 8 * row + 7);
+            const double zhi = nzp < 0 ? 0.0 : __ldg(p + ((int64_t)nzp << 9) + 8 * row);
+            const bool zxp = a == 7 && nx < 0, zxm = a == 0 && nx < 0, zyp = b == 7 && ny < 0, zym = b == 0 && ny < 0;
+#pragma unroll
+            for (int z = 0; z < 8; ++z) {
+                const double lap = (zxp ? 0.0 : xp[z]) + (zxm ? 0.0 : xm[z]) + (zyp ? 0.0 : yp[z]) +
+                                   (zym ? 0.0 : ym[z]) + (z < 7 ? c[z + 1] : zhi) + (z > 0 ? c[z - 1] : zlo) -
+                                   6.0 * c[z];
+                res[z] = (double)dv[z] * h2 - lap;
+            }
+        } else {
+#pragma unroll
+            for (int z = 0; z < 8; ++z) res[z] = (double)dv[z] * h2;
+            if (p_zero_out != nullptr) {
+                double2* pz = reinterpret_cast<double2*>(p_zero_out + own);
+#pragma unroll
+                for (int h = 0; h < 4; ++h) pz[h] = make_double2(0.0, 0.0);
+            }
         }
-        r[s] = (float)res;
-        r2 += res * res;
-        b2 += bb * bb;
+        float4* ro = reinterpret_cast<float4*>(r + own);
+        ro[0] = make_float4((float)res[0], (float)res[1], (float)res[2], (float)res[3]);
+        ro[1] = make_float4((float)res[4], (float)res[5], (float)res[6], (float)res[7]);
+#pragma unroll
+        for (int z = 0; z < 8; ++z) {
+            const double bb = (double)dv[z] * h2;
+            r2 += res[z] * res[z];
+            b2 += bb * bb;
+        }
     }
     block_sum2(r2, b2, acc);
 }
@@ -308,6 +325,10 @@ __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restr
     const double sc = (double)*scale;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
         p[q] += sc * (double)sload(e, inner_slot<kLayout>(q));
+}
+
+unsigned residual_blocks(const Context& c) {
+    return (unsigned)((c.topo.num_leaves + kResidualLeaves - 1) / kResidualLeaves);
 }
 
 unsigned stream_blocks(const Context& c, int64_t n) {
@@ -431,7 +452,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         faces[1] = c.scratch_f32("refine_faces1", leaves * kPackedFaceBytes / 4);
         halo = c.scratch_f32("refine_rhs_halo", leaves * kPackedHaloBytes / 4);
     }
-    refine_residual_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2,
+    refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2,
                                                                                    nullptr, tol2, plan.slots);
     HNS_LAUNCHED();
     for (int k = 0; k < plan.max_outer; ++k) {
@@ -473,7 +494,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         else
             refine_update_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
         HNS_LAUNCHED();
-        refine_residual_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+        refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(
             c.topo.view, div, p, nullptr, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
         HNS_LAUNCHED();
     }
@@ -561,12 +582,15 @@ hns_status mixed_info(Context& c, const RefinePlan& plan, const hns_mixed_desc& 
     return HNS_OK;
 }
 
+// after_advect, when given, runs on the host once the advection is enqueued (the scalars'
+// outputs are final from then on; the velocity is not).
 RefinePlan mixed_step_device(Context& c, const void* vel_in, void* vel_out, const void* const* sin, void* const* sout, int ns,
-                             const hns_mixed_desc& d) {
+                             const hns_mixed_desc& d, const std::function<void()>& after_advect = {}) {
     const size_t n = (size_t)c.num_voxels();
     c.phase_begin(HNS_PHASE_ADVECT);
     launch_advect_mixed(c, vel_in, vel_out, sin, sout, ns, d.dt);
     c.phase_end();
+    if (after_advect) after_advect();
     float* div = c.scratch_f32("project_div", n);
     double* p = reinterpret_cast<double*>(c.scratch_f32("refine_p", 2 * n));
     c.phase_begin(HNS_PHASE_DIVERGENCE);
@@ -641,13 +665,31 @@ HNS_API hns_status hns_step_mixed_host(hns_ctx* ctx, float* vel, float* const* s
             HNS_CUDA(cudaMemcpyAsync(stage, scalars[q], n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
             convert_array(*c, stage, HNS_DTYPE_F32, a, HNS_DTYPE_F16, (int64_t)n);
         }
-        const RefinePlan plan = mixed_step_device(*c, v_in, v_out, sin.data(), sout.data(), nscalars, *desc);
+        // The advected scalars are final before the pressure solve: they are converted and
+        // downloaded on the auxiliary stream while the main stream projects the velocity.
+        float* stage_aux = nscalars > 0 ? c->scratch_f32("mixed_host_stage_aux", n) : nullptr;
+        if (nscalars > 0) c->ensure_aux();
+        auto download_scalars = [&] {
+            HNS_CUDA(cudaEventRecord(c->aux_ready, c->stream));
+            HNS_CUDA(cudaStreamWaitEvent(c->aux_stream, c->aux_ready, 0));
+            // The conversions below launch on the auxiliary stream; the main one is restored on exit.
+            struct StreamSwap {
+                Context& ctx;
+                cudaStream_t saved;
+                ~StreamSwap() { ctx.stream = saved; }
+            } swap{*c, c->stream};
+            c->stream = c->aux_stream;
+            for (int q = 0; q < nscalars; ++q) {
+                convert_array(*c, sout[q], HNS_DTYPE_F16, stage_aux, HNS_DTYPE_F32, (int64_t)n);
+                HNS_CUDA(cudaMemcpyAsync(scalars[q], stage_aux, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+            }
+        };
+        const RefinePlan plan = mixed_step_device(*c, v_in, v_out, sin.data(), sout.data(), nscalars, *desc,
+                                                  nscalars > 0 ? std::function<void()>(download_scalars)
+                                                               : std::function<void()>());
         convert_array(*c, v_out, HNS_DTYPE_BF16, stage, HNS_DTYPE_F32, (int64_t)(3 * n));
         HNS_CUDA(cudaMemcpyAsync(vel, stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-        for (int q = 0; q < nscalars; ++q) {
-            convert_array(*c, sout[q], HNS_DTYPE_F16, stage, HNS_DTYPE_F32, (int64_t)n);
-            HNS_CUDA(cudaMemcpyAsync(scalars[q], stage, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-        }
+        if (nscalars > 0) HNS_CUDA(cudaStreamSynchronize(c->aux_stream));
         HNS_CUDA(cudaStreamSynchronize(c->stream));
         st = mixed_info(*c, plan, *desc, info);
     });
