@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <string>
 #include <unordered_map>
@@ -267,11 +268,10 @@ void check_ptr(const void* p, const char* what) {
     if (!p) fail(HNS_ERR_INVALID_ARG, std::string("null ") + what);
 }
 
-hns_status create_impl(hns_ctx** out, const int32_t* origins, int64_t num_leaves, float voxel_size, int device) {
+hns_status create_impl(hns_ctx** out, float voxel_size, int device, const std::function<void(Context&)>& build_topology) {
     return guarded([&] {
         check_ptr(out, "output pointer");
         *out = nullptr;
-        check_ptr(origins, "leaf origins");
         if (!(voxel_size > 0.f) || !std::isfinite(voxel_size)) fail(HNS_ERR_INVALID_ARG, "voxel size must be positive and finite");
         int count = 0;
         HNS_CUDA(cudaGetDeviceCount(&count));
@@ -284,7 +284,7 @@ hns_status create_impl(hns_ctx** out, const int32_t* origins, int64_t num_leaves
         HNS_CUDA(cudaStreamCreateWithFlags(&c.own_stream, cudaStreamNonBlocking));
         c.stream = c.own_stream;
         try {
-            c.topo.build(origins, num_leaves, c.stream);
+            build_topology(c);
             c.d_counters.alloc(sizeof(unsigned long long) * 8);
             c.counters = c.d_counters.as<unsigned long long>();
             HNS_CUDA(cudaMemsetAsync(c.counters, 0, c.d_counters.bytes, c.stream));
@@ -322,7 +322,16 @@ HNS_API const char* hns_status_string(hns_status s) {
 HNS_API const char* hns_last_error(void) { return g_last_error.c_str(); }
 
 HNS_API hns_status hns_create(hns_ctx** out, const int32_t* leaf_origins, int64_t num_leaves, float voxel_size, int device) {
-    return create_impl(out, leaf_origins, num_leaves, voxel_size, device);
+    if (!leaf_origins) return record_error(HNS_ERR_INVALID_ARG, "null leaf origins");
+    return create_impl(out, voxel_size, device, [&](Context& c) { c.topo.build(leaf_origins, num_leaves, c.stream); });
+}
+
+HNS_API hns_status hns_create_from_voxels(hns_ctx** out, const int32_t* ijk, int64_t num_voxels, int padding,
+                                          int ijk_on_device, float voxel_size, int device) {
+    if (!ijk) return record_error(HNS_ERR_INVALID_ARG, "null voxel coordinates");
+    return create_impl(out, voxel_size, device, [&](Context& c) {
+        c.topo.build_from_voxels(ijk, num_voxels, ijk_on_device != 0, padding, c.stream);
+    });
 }
 
 HNS_API hns_status hns_create_from_coords(hns_ctx** out, const int32_t* coords, int64_t num_voxels, float voxel_size,
@@ -347,7 +356,8 @@ HNS_API hns_status hns_create_from_coords(hns_ctx** out, const int32_t* coords, 
         }
     });
     if (s != HNS_OK) return s;
-    return create_impl(out, origins.data(), (int64_t)origins.size() / 3, voxel_size, device);
+    return create_impl(out, voxel_size, device,
+                       [&](Context& c) { c.topo.build(origins.data(), (int64_t)origins.size() / 3, c.stream); });
 }
 
 HNS_API hns_status hns_destroy(hns_ctx* ctx) {

@@ -91,6 +91,10 @@ struct Topology {
     TopoView view{};
     bool nanovdb_order = false;
     void build(const int32_t* leaf_origins, int64_t n, cudaStream_t stream);
+    // The leaves that the active voxels ijk (int32 [3 n], host or device) touch after a
+    // 26-neighbour dilation by `padding` voxels, in NanoVDB order, built on the device
+    // (hns_topology.cu).
+    void build_from_voxels(const int32_t* ijk, int64_t n, bool ijk_on_device, int padding, cudaStream_t stream);
 };
 
 bool leaves_in_nanovdb_order(const int32_t* origins, int64_t n);

@@ -93,6 +93,7 @@ def _load():
     _sig(lib, "hns_last_error", ctypes.c_char_p)
     _sig(lib, "hns_create", _i, ctypes.POINTER(_p), _p, _i64, _f, _i)
     _sig(lib, "hns_create_from_coords", _i, ctypes.POINTER(_p), _p, _i64, _f, _i)
+    _sig(lib, "hns_create_from_voxels", _i, ctypes.POINTER(_p), _p, _i64, _i, _i, _f, _i)
     _sig(lib, "hns_destroy", _i, _p)
     _sig(lib, "hns_set_stream", _i, _p, _p)
     _sig(lib, "hns_get_stream", _p, _p)
@@ -170,9 +171,24 @@ def _dptr(t) -> int:
 class Grid:
     """A leaf-dense sparse domain on one GPU (an hns_ctx)."""
 
-    def __init__(self, leaf_origins=None, voxel_size: float = 1.0, device: int = 0, coords=None):
+    def __init__(self, leaf_origins=None, voxel_size: float = 1.0, device: int = 0, coords=None, voxels=None,
+                 padding: int = 0):
+        """leaf_origins (hns_create), coords of a leaf-dense layout (hns_create_from_coords), or
+        voxels: active voxel coordinates (N, 3), a numpy array or a CUDA tensor on `device`,
+        whose touched leaves after a `padding`-voxel dilation form the grid
+        (hns_create_from_voxels)."""
         self._h = _p()
-        if coords is not None:
+        if voxels is not None:
+            if hasattr(voxels, "is_cuda") and voxels.is_cuda:
+                if voxels.dtype != __import__("torch").int32 or not voxels.is_contiguous():
+                    raise ValueError("voxels on the device must be a contiguous int32 tensor")
+                check(lib.hns_create_from_voxels(ctypes.byref(self._h), voxels.data_ptr(), voxels.numel() // 3, padding, 1,
+                                                 voxel_size, device))
+            else:
+                v = np.ascontiguousarray(np.asarray(voxels, dtype=np.int32).reshape(-1, 3))
+                check(lib.hns_create_from_voxels(ctypes.byref(self._h), v.ctypes.data, len(v), padding, 0, voxel_size,
+                                                 device))
+        elif coords is not None:
             c = np.ascontiguousarray(np.asarray(coords, dtype=np.int32).reshape(-1, 3))
             check(lib.hns_create_from_coords(ctypes.byref(self._h), c.ctypes.data, len(c), voxel_size, device))
         else:

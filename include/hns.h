@@ -69,6 +69,15 @@ HNS_API hns_status hns_create(hns_ctx** out, const int32_t* leaf_origins, int64_
  * of 512); HNS_ERR_LAYOUT otherwise. This is the coordinate block of GridIndexedData. */
 HNS_API hns_status hns_create_from_coords(hns_ctx** out, const int32_t* coords, int64_t num_voxels,
                                           float voxel_size, int device);
+/* The domain set-up of the HNanoSolver SOP (src/SOP/HNanoSolver/SOP_HNanoSolver.cpp:280-285: the
+ * velocity grid's active voxels dilated by `padding` voxels, face, edge and vertex neighbours)
+ * with the grid built from the voxel list (CreateIndexGrid, src/Cuda/HNanoSolver.cu:498-510),
+ * on the device: the context's leaves are every leaf that a dilated voxel touches, in NanoVDB
+ * order. ijk: int32[3 * num_voxels], on the host, or on this context's device when
+ * ijk_on_device is nonzero; repeats allowed; |coordinate| < 2^23 - 64; padding in [0, 8].
+ * hns_leaf_origins returns the leaves. */
+HNS_API hns_status hns_create_from_voxels(hns_ctx** out, const int32_t* ijk, int64_t num_voxels, int padding,
+                                          int ijk_on_device, float voxel_size, int device);
 HNS_API hns_status hns_destroy(hns_ctx* ctx);
 /* Use a caller-owned cudaStream_t (NULL restores the context's own stream). */
 HNS_API hns_status hns_set_stream(hns_ctx* ctx, void* cuda_stream);
