@@ -14,6 +14,9 @@
 //   [divergence, rbgs x max(2, iterations/2)]  when disturbanceEnable > 0
 //   subtract_gradient     adv3, p -> velocity
 //   advect_scalars        the persistent scalars, with the projected velocity
+// With a "collision_sdf" field the collider enters as in the reference: enforced on the
+// velocity before the substeps and after each projection, trace points inside it pulled back
+// in both advections, and the near-wall blend after the velocity advection and the gradient.
 // Each fusion applies the reference's per-voxel operations in the reference's order, so
 // every output equals the reference's (the confinement race aside: it runs out of place).
 #include <cuda_runtime.h>
@@ -195,12 +198,17 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
     float* div = c.scratch_f32("advance_div", n);
     float* p = c.scratch_f32("advance_p", n);
     const float omega = 2.0f / (1.0f + sinf(3.14159f * dx));  // host sinf, as :365
+    // A collider: the "collision_sdf" field (HNS_EnsureContext stores it when the SOP has one,
+    // :121-133), enforced on the velocity before the substeps (:241-244).
+    Field* sdff = c.find_field("collision_sdf");
+    const float* sdf = (sdff && sdff->components == 1) ? sdff->buf.as<float>() : nullptr;
+    if (sdf) launch_collision_enforce(c, c.find_field(vel_name)->buf.as<float>(), sdf);
 
     for (int s = 0; s < subs; ++s) {
         float* vel = c.find_field(vel_name)->buf.as<float>();
         c.phase_begin(HNS_PHASE_ADVECT);
         FieldSet none{};
-        launch_advect_fused(c, vel, adv, none, dt_sub);
+        launch_advect_fused(c, vel, adv, none, dt_sub, sdf);
         c.phase_end();
 
         Field* sv = c.find_field("src_vel");
@@ -248,7 +256,8 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
         c.phase_end();
         c.phase_begin(HNS_PHASE_GRADIENT);
         vel = c.find_field(vel_name)->buf.as<float>();
-        launch_subtract_gradient(c, adv3, p, vel);
+        launch_subtract_gradient(c, adv3, p, vel, sdf);
+        if (sdf) launch_collision_enforce(c, vel, sdf);  // :411-414
         c.phase_end();
 
         if (!adv_names.empty()) {
@@ -262,7 +271,7 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
                     f.in[q] = c.find_field(adv_names[base + q])->buf.as<float>();
                     f.out[q] = c.scratch_f32("advance_twin:" + adv_names[base + q], n);
                 }
-                launch_advect_scalars(c, vel, f, dt_sub);
+                launch_advect_scalars(c, vel, f, dt_sub, sdf);
             }
             for (const auto& name : adv_names) std::swap(c.find_field(name)->buf, c.scratch["advance_twin:" + name]);
             c.phase_end();

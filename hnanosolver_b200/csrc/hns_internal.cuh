@@ -192,8 +192,11 @@ struct FieldSet {
 };
 
 // Velocity (vel_out, may be null) and HNanoAdvect scalars (f) along one shared trace.
-void launch_advect_fused(const Context& c, const float* vel, float* vel_out, const FieldSet& f, float dt);
-void launch_advect_scalars(const Context& c, const float* vel, const FieldSet& f, float dt);
+// sdf (or null): the collision SDF of HNS_Advance's step.
+void launch_advect_fused(const Context& c, const float* vel, float* vel_out, const FieldSet& f, float dt,
+                         const float* sdf = nullptr);
+void launch_advect_scalars(const Context& c, const float* vel, const FieldSet& f, float dt, const float* sdf = nullptr);
+void launch_collision_enforce(const Context& c, float* vel, const float* sdf);
 void launch_divergence(const Context& c, const float* vel, float* div);
 // One fused red+black iteration: p_in -> p_out (ping-pong). p_in == nullptr means p = 0.
 // check/tol2: skip when check[0] <= tol2 * check[1]; resid_out: accumulate the residual of
@@ -209,7 +212,7 @@ void launch_rbgs_bulk(const Context& c, const float* div, const float* p_in, flo
 // mixed-precision refinement, L e = rhs. e_in null means e = 0.
 void launch_rbgs_bulk_half(const Context& c, const void* rhs, const void* e_in, void* e_out, float omega,
                            const double* check, double tol2);
-void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out);
+void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out, const float* sdf = nullptr);
 void launch_vorticity(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale);
 // acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).
 void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags);

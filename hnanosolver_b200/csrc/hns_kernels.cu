@@ -31,7 +31,8 @@ constexpr int kThreads = 256;
 // computed once and every field is sampled from them. vel_out may be null (scalars only) and
 // f.count may be 0 (velocity only); each output equals the reference kernel's.
 __global__ void __launch_bounds__(kThreads, 3) advect_fused_kernel(TopoView t, const float* __restrict__ vel,
-                                                                 float* __restrict__ vel_out, FieldSet f, float sdt) {
+                                                                    float* __restrict__ vel_out, FieldSet f, float sdt,
+                                                                    const float* __restrict__ sdf, float inv_dx) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
     load_nbhd(L, t, v.leaf);
@@ -39,11 +40,16 @@ __global__ void __launch_bounds__(kThreads, 3) advect_fused_kernel(TopoView t, c
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
     const int64_t s = (v.leaf << 9) + v.n;
     const float3 vo = ld3(vel, s);
-    const float bx = (float)i - vo.x * sdt, by = (float)j - vo.y * sdt, bz = (float)k - vo.z * sdt;
+    float bx = (float)i - vo.x * sdt, by = (float)j - vo.y * sdt, bz = (float)k - vo.z * sdt;
+    // A collider pulls trace points inside it back: the back position to the voxel, the forward
+    // one to the back position (advect_vector, src/Cuda/Kernel.cu:373-383).
+    if (sdf != nullptr && sdf_inside(t, L, sdf, bx, by, bz)) bx = (float)i, by = (float)j, bz = (float)k;
     Taps tb, tf;
     taps_at(tb, t, L, bx, by, bz);
     const float3 vf = tri_v(tb, vel);
-    taps_at(tf, t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt);
+    float fx = bx + vf.x * sdt, fy = by + vf.y * sdt, fz = bz + vf.z * sdt;
+    if (sdf != nullptr && sdf_inside(t, L, sdf, fx, fy, fz)) fx = bx, fy = by, fz = bz;
+    taps_at(tf, t, L, fx, fy, fz);
     // Face neighbours in the reference's clamp order: x-1, x+1, y-1, y+1, z-1, z+1.
     int64_t ns[6];
     face_slots(L, s, v.n, ns);
@@ -62,6 +68,7 @@ __global__ void __launch_bounds__(kThreads, 3) advect_fused_kernel(TopoView t, c
         corr.x = fmaxf(mn.x, fminf(corr.x, mx.x));
         corr.y = fmaxf(mn.y, fminf(corr.y, mx.y));
         corr.z = fmaxf(mn.z, fminf(corr.z, mx.z));
+        if (sdf != nullptr) collide(t, L, sdf, s, i, j, k, inv_dx, 1.5f, corr);  // Kernel.cu:409-419
         st3(vel_out, s, corr);
     }
     for (int c = 0; c < f.count; ++c) {
@@ -83,10 +90,11 @@ __global__ void __launch_bounds__(kThreads, 3) advect_fused_kernel(TopoView t, c
     }
 }
 
-// advect_scalars (src/Cuda/Kernel.cu:163-289) without collision: taps, weights and the
-// re-traced position are computed once and shared by every field.
+// advect_scalars (src/Cuda/Kernel.cu:163-289): taps, weights and the re-traced position are
+// computed once and shared by every field. sdf (or null): a collider pulls trace points
+// inside it back (Kernel.cu:192-195, 245-248).
 __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(TopoView t, const float* __restrict__ vel, FieldSet f,
-                                                                   float sdt) {
+                                                                   float sdt, const float* __restrict__ sdf) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
     load_nbhd(L, t, v.leaf);
@@ -94,7 +102,8 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(TopoView t, co
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
     const int64_t s = (v.leaf << 9) + v.n;
     const float3 vc = ld3(vel, s);
-    const float bx = (float)i - vc.x * sdt, by = (float)j - vc.y * sdt, bz = (float)k - vc.z * sdt;
+    float bx = (float)i - vc.x * sdt, by = (float)j - vc.y * sdt, bz = (float)k - vc.z * sdt;
+    if (sdf != nullptr && sdf_inside(t, L, sdf, bx, by, bz)) bx = (float)i, by = (float)j, bz = (float)k;
     int64_t bi[8], fi[8], ni[6];
     float bw[8], fw[8];
     interp_setup(t, L, bx, by, bz, bi, bw);
@@ -106,7 +115,8 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(TopoView t, co
         vf.y = vf.y + a.y * bw[q];
         vf.z = vf.z + a.z * bw[q];
     }
-    const float fx = bx + vf.x * sdt, fy = by + vf.y * sdt, fz = bz + vf.z * sdt;
+    float fx = bx + vf.x * sdt, fy = by + vf.y * sdt, fz = bz + vf.z * sdt;
+    if (sdf != nullptr && sdf_inside(t, L, sdf, fx, fy, fz)) fx = bx, fy = by, fz = bz;
     interp_setup(t, L, fx, fy, fz, fi, fw);
     ni[0] = tap_slot(t, L, i - 1, j, k);
     ni[1] = tap_slot(t, L, i + 1, j, k);
@@ -274,10 +284,12 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
     }
 }
 
-// subtractPressureGradient (src/Cuda/Kernel.cu:495-541) without collision.
+// subtractPressureGradient (src/Cuda/Kernel.cu:495-541); sdf (or null): the collision
+// treatment of the result (Kernel.cu:528-538).
 __global__ void __launch_bounds__(kThreads) subtract_gradient_kernel(TopoView t, const float* __restrict__ vel,
                                                                       const float* __restrict__ p,
-                                                                      float* __restrict__ out, float inv_dx) {
+                                                                      float* __restrict__ out, float inv_dx,
+                                                                      const float* __restrict__ sdf) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
     load_nbhd(L, t, v.leaf);
@@ -289,7 +301,24 @@ __global__ void __launch_bounds__(kThreads) subtract_gradient_kernel(TopoView t,
     const float gy = (near_s(t, L, p, i, j + 1, k) - near_s(t, L, p, i, j - 1, k)) * h;
     const float gz = (near_s(t, L, p, i, j, k + 1) - near_s(t, L, p, i, j, k - 1)) * h;
     const float3 u = ld3(vel, s);
-    st3(out, s, make_float3(u.x - gx, u.y - gy, u.z - gz));
+    float3 r = make_float3(u.x - gx, u.y - gy, u.z - gz);
+    if (sdf != nullptr) collide(t, L, sdf, s, i, j, k, inv_dx, 0.1f, r);
+    st3(out, s, r);
+}
+
+// enforceCollisionBoundaries (src/Cuda/Kernel.cu:133-158), in place: every voxel reads only
+// its own velocity.
+__global__ void __launch_bounds__(kThreads) collision_enforce_kernel(TopoView t, float* __restrict__ vel,
+                                                                      const float* __restrict__ sdf, float inv_dx) {
+    __shared__ LeafNbhd L;
+    const VoxelIdx v = voxel_of_block();
+    load_nbhd(L, t, v.leaf);
+    __syncthreads();
+    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
+    const int64_t s = (v.leaf << 9) + v.n;
+    float3 u = make_float3(vel[3 * s], vel[3 * s + 1], vel[3 * s + 2]);
+    collide(t, L, sdf, s, i, j, k, inv_dx, 0.1f, u);
+    st3(vel, s, u);
 }
 
 // FP64 residual of the relaxed system: r = div dx^2 - (sum of 6 neighbours - 6 p).
@@ -377,13 +406,19 @@ unsigned leaf_blocks(const Context& c) { return (unsigned)(c.topo.num_leaves * 2
 
 }  // namespace
 
-void launch_advect_fused(const Context& c, const float* vel, float* vel_out, const FieldSet& f, float dt) {
-    advect_fused_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, vel_out, f, dt * (1.0f / c.dx));
+void launch_advect_fused(const Context& c, const float* vel, float* vel_out, const FieldSet& f, float dt, const float* sdf) {
+    advect_fused_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, vel_out, f, dt * (1.0f / c.dx), sdf,
+                                                                   1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
-void launch_advect_scalars(const Context& c, const float* vel, const FieldSet& f, float dt) {
-    advect_scalars_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, f, dt * (1.0f / c.dx));
+void launch_advect_scalars(const Context& c, const float* vel, const FieldSet& f, float dt, const float* sdf) {
+    advect_scalars_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, f, dt * (1.0f / c.dx), sdf);
+    HNS_LAUNCHED();
+}
+
+void launch_collision_enforce(const Context& c, float* vel, const float* sdf) {
+    collision_enforce_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, sdf, 1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
@@ -404,8 +439,8 @@ void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in
     HNS_LAUNCHED();
 }
 
-void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out) {
-    subtract_gradient_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, out, 1.0f / c.dx);
+void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out, const float* sdf) {
+    subtract_gradient_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, out, 1.0f / c.dx, sdf);
     HNS_LAUNCHED();
 }
 

@@ -238,6 +238,41 @@ __device__ __forceinline__ float vort_mag(const TopoView& t, const LeafNbhd& L, 
     return __fsqrt_rn(ox * ox + oy * oy + oz * oz);
 }
 
+// ---- collision (src/Cuda/Kernel.cu:81-158) ----
+
+// isInCollision: the trilinear SDF sample (0 outside the domain) below 0.
+__device__ __forceinline__ bool sdf_inside(const TopoView& t, const LeafNbhd& L, const float* __restrict__ sdf, float x,
+                                           float y, float z) {
+    return tri_s(t, L, sdf, x, y, z) < 0.f;
+}
+
+// The collision treatment of a velocity at voxel (i, j, k), slot s: 0 inside the collider
+// (sdf < 0); within the 0.1 margin, the normal component blended out with weight
+// 1 - sdf / ramp (applyNoSlipBoundary; ramp 0.1 in enforceCollisionBoundaries and
+// subtractPressureGradient, 1.5 in advect_vector). The normal is getSDFNormal: central
+// differences of the SDF times 0.5 inv_dx, scaled by 1 / length (NanoVDB's Vec3f / s) when
+// the length exceeds 1e-6.
+__device__ __forceinline__ void collide(const TopoView& t, const LeafNbhd& L, const float* __restrict__ sdf, int64_t s, int i,
+                                        int j, int k, float inv_dx, float ramp, float3& v) {
+    const float d = __ldg(sdf + s);
+    if (d < 0.f) {
+        v = make_float3(0.f, 0.f, 0.f);
+    } else if (d < 0.1f) {
+        const float h = 0.5f * inv_dx;
+        const float gx = h * (near_s(t, L, sdf, i + 1, j, k) - near_s(t, L, sdf, i - 1, j, k));
+        const float gy = h * (near_s(t, L, sdf, i, j + 1, k) - near_s(t, L, sdf, i, j - 1, k));
+        const float gz = h * (near_s(t, L, sdf, i, j, k + 1) - near_s(t, L, sdf, i, j, k - 1));
+        const float len = __fsqrt_rn(gx * gx + gy * gy + gz * gz);
+        const float r = len > 1e-6f ? __frcp_rn(len) : 0.f;
+        const float nx = r * gx, ny = r * gy, nz = r * gz;
+        const float vdotn = v.x * nx + v.y * ny + v.z * nz;
+        const float tx = v.x - vdotn * nx, ty = v.y - vdotn * ny, tz = v.z - vdotn * nz;
+        const float blend = 1.f - __fdiv_rn(d, ramp);
+        const float keep = 1.f - blend;
+        v = make_float3(keep * v.x + blend * tx, keep * v.y + blend * ty, keep * v.z + blend * tz);
+    }
+}
+
 // Voxel handled by this thread in the "two CTAs per leaf" kernels.
 struct VoxelIdx {
     int64_t leaf;

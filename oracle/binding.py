@@ -63,13 +63,15 @@ class AdvanceFields(ctypes.Structure):
         ("n", _i64), ("velocity", _p), ("nscalars", _i), ("names", ctypes.POINTER(ctypes.c_char_p)),
         ("scalars", ctypes.POINTER(_p)), ("created", _p * 4), ("src_vel", _p), ("src_vel_x", _p),
         ("src_vel_y", _p), ("src_vel_z", _p), ("src_temperature", _p), ("src_density", _p), ("src_fuel", _p),
+        ("collision_sdf", _p),
     ]
 
 
 def make_advance_fields(n, velocity, scalars: dict, created: dict, sources: dict):
     """Keep-alive tuple (struct, refs) for an HNS_Advance call. `scalars` is the ordered
     name->array dict of persistent fields present at call start; `created` maps any of
-    fuel/waste/temperature/flame absent from it to an output buffer."""
+    fuel/waste/temperature/flame absent from it to an output buffer. `sources` may also hold
+    "collision_sdf", the collider's signed distance per voxel."""
     names = list(scalars)
     cnames = (ctypes.c_char_p * max(1, len(names)))(*[s.encode() for s in names])
     cptrs = (_p * max(1, len(names)))(*[scalars[s].ctypes.data for s in names])
@@ -81,7 +83,8 @@ def make_advance_fields(n, velocity, scalars: dict, created: dict, sources: dict
     f.scalars = ctypes.cast(cptrs, ctypes.POINTER(_p))
     for k, nm in enumerate(("fuel", "waste", "temperature", "flame")):
         f.created[k] = created[nm].ctypes.data if nm in created else None
-    for key in ("src_vel", "src_vel_x", "src_vel_y", "src_vel_z", "src_temperature", "src_density", "src_fuel"):
+    for key in ("src_vel", "src_vel_x", "src_vel_y", "src_vel_z", "src_temperature", "src_density", "src_fuel",
+                "collision_sdf"):
         setattr(f, key, sources[key].ctypes.data if key in sources else None)
     return f, (cnames, cptrs, velocity, scalars, created, sources)
 

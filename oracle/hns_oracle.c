@@ -145,14 +145,15 @@ void hnso_sort_leaves_nanovdb(int32_t* leaf_origins, int64_t num_leaves) {
 #undef INV6
 
 /* ---- HNS_Advance ------------------------------------------------------------------------
- * The kernel sequence of one HNS_Advance call (src/Cuda/HNanoSolver.cu:223-456), without
- * collision: per substep advect velocity, confinement (run out of place; the reference's
+ * The kernel sequence of one HNS_Advance call (src/Cuda/HNanoSolver.cu:223-456): with a
+ * collision SDF, enforceCollisionBoundaries on the velocity first (:241-244); per substep advect velocity, confinement (run out of place; the reference's
  * in-place launch at :279-281 races), velocity and scalar sources, gravity, divergence,
  * oxygen combustion (adds expansion to the divergence), buoyancy from the burned
  * temperature, iteration x (red, black) from p = 0 with omega = 2/(1+sin(3.14159 dx)), the
  * disturbance re-solve (divergence again, p = 0, max(2, iteration/2) sweeps) when enabled,
- * gradient subtraction into the velocity, then advection of the persistent scalars with
- * the projected velocity. */
+ * gradient subtraction into the velocity (with the SDF, then enforceCollisionBoundaries again,
+ * :411-414), then advection of the persistent scalars with the projected velocity; the SDF
+ * also enters the velocity and scalar advection and the gradient subtraction. */
 static float* find_scalar(const hnso_advance_fields* f, const char* name) {
     for (int i = 0; i < f->nscalars; ++i)
         if (strcmp(f->names[i], name) == 0) return f->scalars[i];
@@ -174,8 +175,10 @@ void hnso_hns_advance_f32(const hnso_topo* t, const hnso_advance_fields* F, floa
     float* o[4];
     for (int q = 0; q < 4; ++q) o[q] = (float*)calloc((size_t)N, sizeof(float));
 
+    const float* sdf = F->collision_sdf;
+    if (sdf) hnso_enforce_collision_f32(t, F->velocity, sdf, inv_dx);
     for (int s = 0; s < SUBS; ++s) {
-        hnso_advect_vector_f32(t, F->velocity, adv, dt_sub, inv_dx);
+        advect_vector_impl_f32(t, F->velocity, adv, dt_sub, inv_dx, sdf);
         hnso_vorticity_confinement_f32(t, adv, adv2, dt_sub, inv_dx, P->vorticityScale, P->factorScale);
         float* sw = adv;
         adv = adv2;
@@ -222,12 +225,13 @@ void hnso_hns_advance_f32(const hnso_topo* t, const hnso_advance_fields* F, floa
             memset(p, 0, sizeof(float) * (size_t)N);
             hnso_rbgs_f32(t, div, p, dx, iteration / 2 > 2 ? iteration / 2 : 2, omega);
         }
-        hnso_subtract_gradient_f32(t, adv, p, F->velocity, inv_dx);
+        subtract_gradient_impl_f32(t, adv, p, F->velocity, inv_dx, sdf);
+        if (sdf) hnso_enforce_collision_f32(t, F->velocity, sdf, inv_dx);
 
         if (F->nscalars > 0) {
             float** outs = (float**)malloc(sizeof(float*) * (size_t)F->nscalars);
             for (int k = 0; k < F->nscalars; ++k) outs[k] = (float*)calloc((size_t)N, sizeof(float));
-            hnso_advect_scalars_f32(t, F->velocity, (const float* const*)F->scalars, outs, F->nscalars, dt_sub, inv_dx);
+            advect_scalars_impl_f32(t, F->velocity, (const float* const*)F->scalars, outs, F->nscalars, dt_sub, inv_dx, sdf);
             for (int k = 0; k < F->nscalars; ++k) {
                 memcpy(F->scalars[k], outs[k], sizeof(float) * (size_t)N);
                 free(outs[k]);

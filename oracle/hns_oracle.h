@@ -85,7 +85,8 @@ typedef struct {
     void hnso_add_velocity_source##S(int64_t n, R* vel, const R* src, R dt);                                       \
     void hnso_add_velocity_source_xyz##S(int64_t n, R* vel, const R* sx, const R* sy, const R* sz, R dt);          \
     void hnso_add_gravity##S(int64_t n, R* vel, R g, R dt);                                                        \
-    void hnso_project##S(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterations, R omega);
+    void hnso_project##S(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterations, R omega);                \
+    void hnso_enforce_collision##S(const hnso_topo* t, R* vel, const R* sdf, R inv_dx);
 
 HNSO_DECLARE(float, _f32)
 HNSO_DECLARE(double, _f64)
@@ -108,6 +109,7 @@ typedef struct {
     const float* src_temperature;
     const float* src_density;
     const float* src_fuel;
+    const float* collision_sdf; /* n, or NULL: no collider */
 } hnso_advance_fields;
 
 void hnso_hns_advance_f32(const hnso_topo* t, const hnso_advance_fields* f, float dx, int iteration, float dt,

@@ -77,10 +77,63 @@ static inline void FN(coord_of)(const hnso_topo* t, int64_t slot, int32_t* i, in
 static inline R FN(fmin_)(R a, R b) { return a < b ? a : (b < a ? b : (a != a ? b : a)); }
 static inline R FN(fmax_)(R a, R b) { return a > b ? a : (b > a ? b : (a != a ? b : a)); }
 
-/* advect_vector (src/Cuda/Kernel.cu:349-426), no collision: MacCormack back/forward trace
- * with trilinear velocity, clamped to [min,max] of centre, 6 face neighbours and the
- * forward sample. */
-void FN(hnso_advect_vector)(const hnso_topo* t, const R* vel, R* out, R dt, R inv_dx) {
+/* ---- collision (src/Cuda/Kernel.cu:81-158) ----
+ * isInCollision: the trilinear SDF sample (0 outside the domain) below 0. */
+static int FN(in_collision)(const hnso_topo* t, const R* sdf, R x, R y, R z) { return FN(tri_s)(t, sdf, x, y, z) < (R)0; }
+
+/* getSDFNormal: central differences of the SDF at the voxel's face neighbours times
+ * 0.5 inv_dx, normalised when longer than 1e-6, else 0. */
+static void FN(sdf_normal)(const hnso_topo* t, const R* sdf, int32_t i, int32_t j, int32_t k, R inv_dx, R n[3]) {
+    const R h = (R)0.5 * inv_dx;
+    const R g[3] = {(FN(near_s)(t, sdf, i + 1, j, k) - FN(near_s)(t, sdf, i - 1, j, k)) * h,
+                    (FN(near_s)(t, sdf, i, j + 1, k) - FN(near_s)(t, sdf, i, j - 1, k)) * h,
+                    (FN(near_s)(t, sdf, i, j, k + 1) - FN(near_s)(t, sdf, i, j, k - 1)) * h};
+    const R len = SQRT(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+    const R inv = len > (R)1e-6f ? (R)1 / len : (R)0; /* Vec3f / s is (1 / s) * v */
+    for (int q = 0; q < 3; ++q) n[q] = inv * g[q];
+}
+
+/* v (1 - blend) + blend (v - n (v . n)): applyNoSlipBoundary blended in. */
+static void FN(no_slip_blend)(R v[3], const R n[3], R blend) {
+    const R vdotn = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
+    R tg[3];
+    for (int q = 0; q < 3; ++q) tg[q] = v[q] - n[q] * vdotn;
+    for (int q = 0; q < 3; ++q) v[q] = v[q] * ((R)1 - blend) + tg[q] * blend;
+}
+
+/* The velocity treatment after advect_vector (margin 0.1, blend 1 - sdf / 1.5) and after
+ * subtractPressureGradient and in enforceCollisionBoundaries (margin 0.1, blend
+ * 1 - sdf / 0.1): inside the collider (sdf < 0) the velocity is 0; within the margin the
+ * normal component is blended out. */
+static void FN(collide)(const hnso_topo* t, const R* sdf, int64_t s, int32_t i, int32_t j, int32_t k, R inv_dx, R ramp,
+                        R v[3]) {
+    const R d = sdf[s];
+    if (d < (R)0) {
+        v[0] = v[1] = v[2] = (R)0;
+    } else if (d < (R)0.1f) {
+        R n[3];
+        FN(sdf_normal)(t, sdf, i, j, k, inv_dx, n);
+        FN(no_slip_blend)(v, n, (R)1 - d / ramp);
+    }
+}
+
+/* enforceCollisionBoundaries (src/Cuda/Kernel.cu:133-158), in place. */
+void FN(hnso_enforce_collision)(const hnso_topo* t, R* vel, const R* sdf, R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        FN(collide)(t, sdf, s, i, j, k, inv_dx, (R)0.1f, vel + 3 * s);
+    }
+}
+
+/* advect_vector (src/Cuda/Kernel.cu:349-426): MacCormack back/forward trace with trilinear
+ * velocity, clamped to [min,max] of centre, 6 face neighbours and the forward sample. With a
+ * collision SDF (sdf non-NULL): a trace point inside the collider is pulled back (the back
+ * position to the voxel, the forward one to the back position) and the result gets the
+ * collision treatment (margin 0.1, blend 1 - sdf / 1.5). */
+static void FN(advect_vector_impl)(const hnso_topo* t, const R* vel, R* out, R dt, R inv_dx, const R* sdf) {
     const int64_t N = hnso_topo_num_voxels(t);
     const R sdt = dt * inv_dx;
 #pragma omp parallel for schedule(static)
@@ -92,8 +145,11 @@ void FN(hnso_advect_vector)(const hnso_topo* t, const R* vel, R* out, R dt, R in
         back[0] = (R)i - vo[0] * sdt;
         back[1] = (R)j - vo[1] * sdt;
         back[2] = (R)k - vo[2] * sdt;
+        if (sdf && FN(in_collision)(t, sdf, back[0], back[1], back[2])) back[0] = (R)i, back[1] = (R)j, back[2] = (R)k;
         FN(tri_v)(t, vel, back[0], back[1], back[2], vf);
         for (int q = 0; q < 3; ++q) fwd[q] = back[q] + vf[q] * sdt;
+        if (sdf && FN(in_collision)(t, sdf, fwd[0], fwd[1], fwd[2]))
+            for (int q = 0; q < 3; ++q) fwd[q] = back[q];
         FN(tri_v)(t, vel, fwd[0], fwd[1], fwd[2], vb);
         for (int q = 0; q < 3; ++q) {
             corr[q] = vf[q] + (R)0.5 * (vo[q] - vb[q]);
@@ -112,9 +168,15 @@ void FN(hnso_advect_vector)(const hnso_topo* t, const R* vel, R* out, R dt, R in
         for (int q = 0; q < 3; ++q) {
             mn[q] = FN(fmin_)(mn[q], vf[q]);
             mx[q] = FN(fmax_)(mx[q], vf[q]);
-            out[3 * s + q] = FN(fmax_)(mn[q], FN(fmin_)(corr[q], mx[q]));
+            corr[q] = FN(fmax_)(mn[q], FN(fmin_)(corr[q], mx[q]));
         }
+        if (sdf) FN(collide)(t, sdf, s, i, j, k, inv_dx, (R)1.5f, corr);
+        for (int q = 0; q < 3; ++q) out[3 * s + q] = corr[q];
     }
+}
+
+void FN(hnso_advect_vector)(const hnso_topo* t, const R* vel, R* out, R dt, R inv_dx) {
+    FN(advect_vector_impl)(t, vel, out, dt, inv_dx, NULL);
 }
 
 /* Index of a tap for advect_scalars: offset 0 (outside the domain) reads array index 0,
@@ -151,8 +213,8 @@ static void FN(interp_setup)(const hnso_topo* t, R x, R y, R z, int64_t idx[8], 
 /* advect_scalars (src/Cuda/Kernel.cu:163-289), no collision: the back-trace uses the
  * voxel's own velocity, the re-trace the weight-sum trilinear velocity; per field a
  * fused-multiply-add weight sum, MacCormack correction and 7+1 point clamp. */
-void FN(hnso_advect_scalars)(const hnso_topo* t, const R* vel, const R* const* in, R* const* out, int nfields, R dt,
-                             R inv_dx) {
+static void FN(advect_scalars_impl)(const hnso_topo* t, const R* vel, const R* const* in, R* const* out, int nfields,
+                                    R dt, R inv_dx, const R* sdf) {
     const int64_t N = hnso_topo_num_voxels(t);
     const R sdt = dt * inv_dx;
     static const int offs[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
@@ -162,14 +224,18 @@ void FN(hnso_advect_scalars)(const hnso_topo* t, const R* vel, const R* const* i
         FN(coord_of)(t, s, &i, &j, &k);
         const int64_t orig = FN(tap)(t, i, j, k);
         const R* vc = vel + 3 * orig;
-        const R back[3] = {(R)i - vc[0] * sdt, (R)j - vc[1] * sdt, (R)k - vc[2] * sdt};
+        R back[3] = {(R)i - vc[0] * sdt, (R)j - vc[1] * sdt, (R)k - vc[2] * sdt};
+        /* With a collision SDF, trace points inside the collider are pulled back (Kernel.cu:192-195, 245-248). */
+        if (sdf && FN(in_collision)(t, sdf, back[0], back[1], back[2])) back[0] = (R)i, back[1] = (R)j, back[2] = (R)k;
         int64_t bi[8], fi[8], nb[6];
         R bw[8], fw[8];
         FN(interp_setup)(t, back[0], back[1], back[2], bi, bw);
         R vf[3] = {0, 0, 0};
         for (int q = 0; q < 8; ++q)
             for (int c = 0; c < 3; ++c) vf[c] = vf[c] + vel[3 * bi[q] + c] * bw[q];
-        const R fwd[3] = {back[0] + vf[0] * sdt, back[1] + vf[1] * sdt, back[2] + vf[2] * sdt};
+        R fwd[3] = {back[0] + vf[0] * sdt, back[1] + vf[1] * sdt, back[2] + vf[2] * sdt};
+        if (sdf && FN(in_collision)(t, sdf, fwd[0], fwd[1], fwd[2]))
+            for (int q = 0; q < 3; ++q) fwd[q] = back[q];
         FN(interp_setup)(t, fwd[0], fwd[1], fwd[2], fi, fw);
         for (int q = 0; q < 6; ++q) nb[q] = FN(tap)(t, i + offs[q][0], j + offs[q][1], k + offs[q][2]);
         for (int f = 0; f < nfields; ++f) {
@@ -191,6 +257,11 @@ void FN(hnso_advect_scalars)(const hnso_topo* t, const R* vel, const R* const* i
             out[f][s] = FN(fmax_)(mn, FN(fmin_)(corr, mx));
         }
     }
+}
+
+void FN(hnso_advect_scalars)(const hnso_topo* t, const R* vel, const R* const* in, R* const* out, int nfields, R dt,
+                             R inv_dx) {
+    FN(advect_scalars_impl)(t, vel, in, out, nfields, dt, inv_dx, NULL);
 }
 
 /* advect_scalar (src/Cuda/Kernel.cu:294-344), the HNanoAdvect kernel: samplers read 0
@@ -304,7 +375,7 @@ void FN(hnso_residual)(const hnso_topo* t, const R* div, const R* p, R dx, doubl
 
 /* subtractPressureGradient (src/Cuda/Kernel.cu:495-541), no collision: u = u* - grad p,
  * central differences, p = 0 outside. */
-void FN(hnso_subtract_gradient)(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx) {
+static void FN(subtract_gradient_impl)(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx, const R* sdf) {
     const int64_t N = hnso_topo_num_voxels(t);
     const R h = (R)0.5 * inv_dx;
 #pragma omp parallel for schedule(static)
@@ -314,10 +385,17 @@ void FN(hnso_subtract_gradient)(const hnso_topo* t, const R* vel, const R* p, R*
         const R gx = (FN(near_s)(t, p, i + 1, j, k) - FN(near_s)(t, p, i - 1, j, k)) * h;
         const R gy = (FN(near_s)(t, p, i, j + 1, k) - FN(near_s)(t, p, i, j - 1, k)) * h;
         const R gz = (FN(near_s)(t, p, i, j, k + 1) - FN(near_s)(t, p, i, j, k - 1)) * h;
-        out[3 * s] = vel[3 * s] - gx;
-        out[3 * s + 1] = vel[3 * s + 1] - gy;
-        out[3 * s + 2] = vel[3 * s + 2] - gz;
+        R u[3] = {vel[3 * s] - gx, vel[3 * s + 1] - gy, vel[3 * s + 2] - gz};
+        /* With a collision SDF: the collision treatment, margin 0.1, blend 1 - sdf / 0.1 (Kernel.cu:528-538). */
+        if (sdf) FN(collide)(t, sdf, s, i, j, k, inv_dx, (R)0.1f, u);
+        out[3 * s] = u[0];
+        out[3 * s + 1] = u[1];
+        out[3 * s + 2] = u[2];
     }
+}
+
+void FN(hnso_subtract_gradient)(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx) {
+    FN(subtract_gradient_impl)(t, vel, p, out, inv_dx, NULL);
 }
 
 /* computeVorticityMag (src/Cuda/Utils.cuh:226-243): |curl u| at a voxel. */

@@ -299,6 +299,7 @@ struct RefAdvanceFields {
     const float* src_temperature;
     const float* src_density;
     const float* src_fuel;
+    const float* collision_sdf;  // n, or NULL: no collider
 };
 
 static float* find_scalar(const RefAdvanceFields* f, const char* name) {
@@ -307,7 +308,8 @@ static float* find_scalar(const RefAdvanceFields* f, const char* name) {
     return nullptr;
 }
 
-// Restates HNS_Advance (src/Cuda/HNanoSolver.cu:223-456) without collision.
+// Restates HNS_Advance (src/Cuda/HNanoSolver.cu:223-456), with the reference's collision
+// kernels and branches when F->collision_sdf is set (:241-244, :273-275, :406-414, :438-441).
 void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, float dx, int iteration, float dt,
                      const CombustionParams* params) {
     const IndexGrid* grid = static_cast<RefGrid*>(g)->grid;
@@ -320,10 +322,13 @@ void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, 
     bool made[4] = {false, false, false, false};
     static const char* special[4] = {"fuel", "waste", "temperature", "flame"};
     const nanovdb::Coord* cc = C(coords);
+    const float* sdf = F->collision_sdf;
+    const bool hc = sdf != nullptr;
+    if (hc) launch(N, [&] { enforceCollisionBoundaries(grid, cc, V(F->velocity), sdf, dx, (size_t)N); });
 
     for (int s = 0; s < SUBS; ++s) {
         // build_activity_mask writes 1 everywhere (Kernel.cu:75): no masking below.
-        launch(N, [&] { advect_vector(grid, cc, V(F->velocity), V(adv.data()), nullptr, false, nullptr, (size_t)N, dt_sub, inv_dx); });
+        launch(N, [&] { advect_vector(grid, cc, V(F->velocity), V(adv.data()), sdf, hc, nullptr, (size_t)N, dt_sub, inv_dx); });
         launch(N, [&] { vorticityConfinement(grid, cc, V(adv.data()), V(adv2.data()), dt_sub, inv_dx, params->vorticityScale, params->factorScale, nullptr, (size_t)N); });
         adv.swap(adv2);
         if (F->src_vel) {
@@ -382,7 +387,8 @@ void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, 
             std::fill(p.begin(), p.end(), 0.0f);
             ref_rbgs(g, coords, N, div.data(), p.data(), dx, std::max(2, iteration / 2), omega);
         }
-        launch(N, [&] { subtractPressureGradient(grid, cc, (size_t)N, V(adv.data()), p.data(), V(F->velocity), nullptr, false, inv_dx, nullptr); });
+        launch(N, [&] { subtractPressureGradient(grid, cc, (size_t)N, V(adv.data()), p.data(), V(F->velocity), sdf, hc, inv_dx, nullptr); });
+        if (hc) launch(N, [&] { enforceCollisionBoundaries(grid, cc, V(F->velocity), sdf, dx, (size_t)N); });
 
         if (F->nscalars > 0) {
             std::vector<std::vector<float>> outs(F->nscalars, std::vector<float>(N, 0.0f));
@@ -394,7 +400,7 @@ void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, 
             float** pin = ins.data();
             float** pout = outp.data();
             const int ns = F->nscalars;
-            launch(N, [&] { advect_scalars(grid, cc, V(F->velocity), pin, pout, ns, nullptr, false, nullptr, (size_t)N, dt_sub, inv_dx); });
+            launch(N, [&] { advect_scalars(grid, cc, V(F->velocity), pin, pout, ns, sdf, hc, nullptr, (size_t)N, dt_sub, inv_dx); });
             for (int k = 0; k < F->nscalars; ++k) std::copy(outs[k].begin(), outs[k].end(), F->scalars[k]);
         }
     }
