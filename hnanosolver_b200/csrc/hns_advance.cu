@@ -297,10 +297,12 @@ HNS_API hns_status hns_field_set(hns_ctx* ctx, const char* name, int components,
             f = nullptr;
         }
         Field& fld = c->ensure_field(name, components, data == nullptr);
-        if (data)
-            HNS_CUDA(cudaMemcpyAsync(fld.buf.ptr, data, fld.buf.bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                     c->stream));
-        if (!on_device) HNS_CUDA(cudaStreamSynchronize(c->stream));  // host buffer may be reused on return
+        if (data && on_device)
+            HNS_CUDA(cudaMemcpyAsync(fld.buf.ptr, data, fld.buf.bytes, cudaMemcpyDeviceToDevice, c->stream));
+        else if (data)
+            copy_h2d(*c, fld.buf.ptr, data, fld.buf.bytes);  // pinned staging; the host buffer may be reused on return
+        else
+            HNS_CUDA(cudaStreamSynchronize(c->stream));
     });
 }
 
@@ -311,9 +313,10 @@ HNS_API hns_status hns_field_get(hns_ctx* ctx, const char* name, float* out, int
         Field* f = c->find_field(name);
         if (!f) fail(HNS_ERR_NOT_FOUND, std::string("no field '") + name + "'");
         DeviceGuard g(c->device);
-        HNS_CUDA(cudaMemcpyAsync(out, f->buf.ptr, f->buf.bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                 c->stream));
-        if (!on_device) HNS_CUDA(cudaStreamSynchronize(c->stream));
+        if (on_device)
+            HNS_CUDA(cudaMemcpyAsync(out, f->buf.ptr, f->buf.bytes, cudaMemcpyDeviceToDevice, c->stream));
+        else
+            copy_d2h(*c, out, f->buf.ptr, f->buf.bytes);  // pinned staging
     });
 }
 

@@ -371,6 +371,7 @@ HNS_API hns_status hns_destroy(hns_ctx* ctx) {
             (void)cudaStreamDestroy(c.aux_stream);
         }
         if (c.aux_ready) (void)cudaEventDestroy(c.aux_ready);
+        c.release_staging();
         for (auto& e : c.phase_events) {
             (void)cudaEventDestroy(e.start);
             (void)cudaEventDestroy(e.stop);

@@ -141,6 +141,12 @@ struct Context {
     cudaStream_t aux_stream = nullptr;
     cudaEvent_t aux_ready = nullptr;
     void ensure_aux();
+    // Two pinned staging buffers for host copies (hns_transfer.cpp), made on first use, and the
+    // events that order their reuse.
+    void* staging[2] = {nullptr, nullptr};
+    cudaEvent_t staging_done[2] = {nullptr, nullptr};
+    void ensure_staging();
+    void release_staging();
     float dx = 0.f;
     Topology topo;
     // Scratch owned by the context, grown on demand and reused across calls.
@@ -229,6 +235,10 @@ void launch_rhs_halo_pack(const Context& c, const void* rhs, void* halo, const d
 // (8 ints per leaf, missing neighbours = the zero leaf L) and one in-place half-sweep (colour 0
 // red, 1 black). e holds L + 1 leaves, the last all zeros. e_zero: e = 0 before this red
 // half-sweep (the first of a solve).
+// Host <-> device copies of `bytes` through pinned staging, overlapping the host-side copy with
+// the DMA (hns_transfer.cpp). Both return when the data has arrived.
+void copy_h2d(Context& c, void* dev, const void* host, size_t bytes);
+void copy_d2h(Context& c, void* host, const void* dev, size_t bytes);
 void launch_split_face_table(const Context& c, int* nb8);
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
                             float omega, const double* check, double tol2);
