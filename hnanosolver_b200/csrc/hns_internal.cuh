@@ -239,6 +239,8 @@ void launch_rhs_halo_pack(const Context& c, const void* rhs, void* halo, const d
 // the DMA (hns_transfer.cpp). Both return when the data has arrived.
 void copy_h2d(Context& c, void* dev, const void* host, size_t bytes);
 void copy_d2h(Context& c, void* host, const void* dev, size_t bytes);
+// One multigrid V-cycle (hns_multigrid.cu): u0 (n FP32) ~ A^-1 b0 for the unit-spacing system.
+void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, double tol2);
 void launch_split_face_table(const Context& c, int* nb8);
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
                             float omega, const double* check, double tol2);
@@ -263,7 +265,9 @@ void launch_adj_accumulate(const Context& c, const float* src, float* dst, int64
 // ---- mixed precision and refinement (hns_mixed.cu) ----
 void convert_array(const Context& c, const void* src, int src_dt, void* dst, int dst_dt, int64_t n);
 template <typename TI>
-RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol);
+// flags: HNS_SOLVE_MULTIGRID selects a multigrid V-cycle as the inner solve.
+RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol,
+                        unsigned flags = 0);
 void refine_result(Context& c, const RefinePlan& plan, int* outer, double* residual);
 void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
                          float dt);

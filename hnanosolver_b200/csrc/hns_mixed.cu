@@ -412,7 +412,8 @@ void convert_array(const Context& c, const void* src, int src_dt, void* dst, int
 // (inner storage TI), stopping on the device at ||r|| <= tol ||b||. p (FP64, n values) is
 // overwritten. Returns the schedule for refine_result().
 template <typename TI>
-RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol) {
+RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol,
+                        unsigned flags) {
     const int64_t n = c.num_voxels();
     RefinePlan plan;
     plan.max_outer = std::max(1, max_outer);
@@ -457,6 +458,22 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     HNS_LAUNCHED();
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
+        if (flags & HNS_SOLVE_MULTIGRID) {
+            // One V-cycle on the scaled residual in FP32 (slot order), then p += s e.
+            float* rm = c.scratch_f32("mg_rhat", (size_t)n);
+            float* em = c.scratch_f32("mg_e", (size_t)n);
+            refine_scale_kernel<float, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(r, rm, n, chk, tol2, scales + k);
+            HNS_LAUNCHED();
+            c.phase_begin(HNS_PHASE_INNER);
+            mg_vcycle(c, rm, em, chk, tol2);
+            c.phase_end();
+            refine_update_kernel<float, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, em, n, scales + k, chk, tol2);
+            HNS_LAUNCHED();
+            refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(
+                c.topo.view, div, p, nullptr, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
+            HNS_LAUNCHED();
+            continue;
+        }
         if (layout == HNS_INNER_PACKED)
             refine_scale_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         else if (layout == HNS_INNER_SPLIT)
@@ -501,8 +518,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     return plan;
 }
 
-template RefinePlan refine_solve<__half>(Context&, const float*, double*, int, int, float, double);
-template RefinePlan refine_solve<float>(Context&, const float*, double*, int, int, float, double);
+template RefinePlan refine_solve<__half>(Context&, const float*, double*, int, int, float, double, unsigned);
+template RefinePlan refine_solve<float>(Context&, const float*, double*, int, int, float, double, unsigned);
 
 void refine_result(Context& c, const RefinePlan& plan, int* outer, double* residual) {
     std::vector<double> h(2 * (size_t)(plan.max_outer + 1));
@@ -598,7 +615,7 @@ RefinePlan mixed_step_device(Context& c, const void* vel_in, void* vel_out, cons
     c.phase_end();
     c.phase_begin(HNS_PHASE_SOLVE);
     const float omega = d.omega > 0.f ? d.omega : 1.9f;
-    RefinePlan plan = refine_solve<__half>(c, div, p, d.max_outer, d.inner_iterations, omega, d.tolerance);
+    RefinePlan plan = refine_solve<__half>(c, div, p, d.max_outer, d.inner_iterations, omega, d.tolerance, d.flags);
     c.phase_end();
     c.last_refine = plan;
     c.phase_begin(HNS_PHASE_GRADIENT);

@@ -118,7 +118,8 @@ SolveOutcome project_in_place(Context& c, float* vel, const hns_step_desc& d) {
         double* p64 = reinterpret_cast<double*>(c.scratch_f32("refine_p", 2 * n));
         o.refined = true;
         o.rplan = refine_solve<float>(c, o.div, p64, d.max_outer > 0 ? d.max_outer : 8,
-                                      d.inner_iterations > 0 ? d.inner_iterations : 60, resolve_omega(c, d.omega), d.tolerance);
+                                      d.inner_iterations > 0 ? d.inner_iterations : 60, resolve_omega(c, d.omega), d.tolerance,
+                                      d.flags);
         c.last_refine = o.rplan;
         c.phase_end();
         c.phase_begin(HNS_PHASE_GRADIENT);

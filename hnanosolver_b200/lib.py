@@ -55,6 +55,7 @@ class MixedDesc(ctypes.Structure):
 
 DTYPE_F32, DTYPE_F16, DTYPE_BF16, DTYPE_F64 = 0, 1, 2, 3
 SOLVE_REFINE = 4
+SOLVE_MULTIGRID = 8
 
 
 class CombustionParams(ctypes.Structure):

@@ -163,6 +163,12 @@ HNS_API hns_status hns_project_static(hns_ctx* ctx, float* vel, int iterations, 
 #define HNS_SOLVE_REFINE 4u /* hns_step_plain: FP64 iterative refinement around FP32 red-black
                                inner solves (max_outer x inner_iterations) instead of one plain
                                FP32 solve; removes the FP32 rounding floor of the residual */
+#define HNS_SOLVE_MULTIGRID 8u /* with refinement (HNS_SOLVE_REFINE in hns_step_desc.flags; always in
+                                    hns_mixed_desc.flags): each outer step's inner solve is one geometric
+                                    multigrid V-cycle (FP32, levels of 8, 4, 2 and 1 cells per leaf side)
+                                    instead of inner_iterations red-black iterations. The reference
+                                    declares this preconditioner (src/Cuda/Kernels.cuh:52-60) but does not
+                                    implement it. */
 
 typedef struct hns_step_desc {
     float dt;
@@ -216,7 +222,7 @@ typedef struct hns_mixed_desc {
     double tolerance;     /* target ||b - L p|| / ||b|| in FP64 (> 0) */
     int max_outer;        /* outer refinement cap */
     int inner_iterations; /* red-black iterations per outer refinement */
-    unsigned flags;       /* reserved, 0 */
+    unsigned flags;       /* 0, or HNS_SOLVE_MULTIGRID */
 } hns_mixed_desc;
 
 /* hns_step_plain on reduced-precision storage: vel_in/vel_out BF16 (3 per slot), scalars

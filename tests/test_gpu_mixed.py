@@ -166,3 +166,44 @@ def test_inner_solve_layouts_bit_exact(dev, shell, grid):
         assert torch.equal(a[2], b[2])
         assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
         assert b[4] <= 1e-5
+
+
+@pytest.mark.parametrize("grid", ["spheres", "box"])
+def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
+    """HNS_SOLVE_MULTIGRID: one V-cycle per outer step in place of the red-black iterations. The
+    FP64 residual of the returned pressure, recomputed by the oracle, is within the tolerance,
+    and the projected velocity agrees with the red-black refinement's to the accuracy that a
+    1e-5 relative residual allows; the FP32 refined step takes the flag too."""
+    from hnanosolver_b200 import lib as hl
+
+    if grid == "spheres":
+        origins = synth.spheres_topology(96, 3, 8.0, 20.0, seed=11)
+    else:
+        origins = synth.topology("box64")
+    dens, vel = synth.noise_fields(origins, seed=7)
+    g = hl.Grid(origins, voxel_size=0.1)
+    vb = torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous()
+    dh = torch.from_numpy(dens).to(dev).to(torch.float16).contiguous()
+    outs = {}
+    for flags in (0, hl.SOLVE_MULTIGRID):
+        vo, do = torch.empty_like(vb), torch.empty_like(dh)
+        desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=40, inner_iterations=30, flags=flags)
+        info = g.step_mixed(vb, vo, [dh], [do], desc, info=True)
+        assert info.residual <= 1e-5
+        p = torch.empty(g.num_voxels, dtype=torch.float64, device=dev)
+        g.refine_pressure(p)
+        torch.cuda.synchronize()
+        outs[flags] = (vo.float().cpu().numpy(), p.cpu().numpy())
+    t = oracle.topo(origins)
+    adv = torch.from_numpy(t.advect_vector(vb.float().cpu().numpy(), 0.1, 10.0)).to(torch.bfloat16).float().numpy()
+    div = t.divergence(adv, np.float32(10.0)).astype(np.float64)
+    r2, b2 = t.residual(div, outs[hl.SOLVE_MULTIGRID][1], float(np.float32(0.1)))  # the library's voxel size is a float
+    assert np.sqrt(r2 / b2) <= 1e-5 * (1 + 1e-6)
+    assert rel_err(outs[hl.SOLVE_MULTIGRID][0], outs[0][0]) <= 2e-2
+    v = torch.from_numpy(vel).to(dev)
+    d = torch.from_numpy(dens).to(dev)
+    sd = hl.StepDesc(dt=0.1, max_iterations=0, omega=1.9, tolerance=1e-5, check_every=0,
+                     flags=hl.SOLVE_REFINE | hl.SOLVE_MULTIGRID, max_outer=40, inner_iterations=30)
+    info = g.step_plain(v, torch.empty_like(v), [d], [torch.empty_like(d)], sd, info=True)
+    assert info.residual <= 1e-5
+    g.close()
