@@ -76,19 +76,51 @@ def profiled_traffic(workload: str, kind: str):
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    """SM clock and clock-event reasons sampled while the timed region runs: NVML polled every
+    20 ms from a thread (the device matched by PCI bus id), else `nvidia-smi -lms 200`."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+    PERIOD_S = 0.02
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
         self.lines = []
         self.thread = None
+        self.nvml = None
+        self.sm = []
+        self.smax = None
+        self.reasons = set()
+        self.halt = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.dev)
+        bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = (nv, h, {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap})
+            self._poll_once()
+        except Exception:  # no NVML binding or no matching device: fall back to nvidia-smi
+            self.nvml = None
+        if self.nvml is not None:
+            self.sm.clear()
+            self.reasons.clear()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
@@ -99,11 +131,37 @@ class ClockSampler:
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
 
+    def _poll_once(self):
+        nv, h, bits = self.nvml
+        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        for name, bit in bits.items():
+            if mask & bit:
+                self.reasons.add(name)
+
+    def _poll(self):
+        while not self.halt.is_set():
+            try:
+                self._poll_once()
+            except Exception:
+                return
+            self.halt.wait(self.PERIOD_S)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.halt.set()
+            if self.thread:
+                self.thread.join(timeout=2)
+            try:
+                self._poll_once()  # the state at the end of the timed region
+            except Exception:
+                pass
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                    "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "nvml, 20 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -114,7 +172,6 @@ class ClockSampler:
         if self.thread:
             self.thread.join(timeout=2)
         sm, smax, reasons = [], None, set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
@@ -124,11 +181,11 @@ class ClockSampler:
                 smax = float(parts[2])
             except ValueError:
                 continue
-            for name, val in zip(names, parts[5:9]):
+            for name, val in zip(self.NAMES, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 def dist_info():

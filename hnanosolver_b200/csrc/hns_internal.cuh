@@ -231,16 +231,18 @@ void launch_index_offsets(const Context& c, const int32_t* ijk, int64_t n, uint6
 constexpr int kPackedFaceBytes = 1024;
 constexpr int kPackedHaloBytes = 640;
 void launch_rhs_halo_pack(const Context& c, const void* rhs, void* halo, const double* check, double tol2);
-// The FP16 inner solve on colour-split leaves (hns_rbgs_split.cu): the face-neighbour table
-// (8 ints per leaf, missing neighbours = the zero leaf L) and one in-place half-sweep (colour 0
-// red, 1 black). e holds L + 1 leaves, the last all zeros. e_zero: e = 0 before this red
-// half-sweep (the first of a solve).
 // Host <-> device copies of `bytes` through pinned staging, overlapping the host-side copy with
 // the DMA (hns_transfer.cpp). Both return when the data has arrived.
 void copy_h2d(Context& c, void* dev, const void* host, size_t bytes);
 void copy_d2h(Context& c, void* host, const void* dev, size_t bytes);
 // One multigrid V-cycle (hns_multigrid.cu): u0 (n FP32) ~ A^-1 b0 for the unit-spacing system.
 void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, double tol2);
+// The FP16 inner solve on colour-split leaves (hns_rbgs_split.cu): the face-neighbour table
+// (8 ints per leaf, missing neighbours = the zero leaf L) and one in-place half-sweep (colour 0
+// red, 1 black). e holds L + 1 leaves, the last all zeros. e_zero: e = 0 before this red
+// half-sweep (the first of a solve); a launch with e_zero false is a programmatic dependent
+// launch, so the preceding kernel on the stream must be a half-sweep, and rhs, nb8 and check
+// must have been written by kernels that finished before that one started.
 void launch_split_face_table(const Context& c, int* nb8);
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
                             float omega, const double* check, double tol2);

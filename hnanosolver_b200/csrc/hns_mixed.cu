@@ -206,18 +206,18 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
 
 // r = b - L p (FP64 arithmetic, r stored FP32) with b = div dx^2 and p = 0 outside the domain,
 // plus sum r^2 and sum b^2 into acc. p null: p = 0 (r = b), and p_zero_out, when set, is
-// cleared. One thread per z-row of a leaf (64 per leaf, kResidualLeaves leaves per CTA): its
-// row and the four x/y neighbour rows (the neighbour leaf's row across a face, 0 for a missing
-// leaf) as 16-byte loads and the two values across the z faces, with the Laplacian summed in
-// the order +x, -x, +y, -y, +z, -z, -6 p.
-constexpr int kResidualLeaves = kThreads / 64;
+// cleared. One thread per half z-row of a leaf (z = 4h .. 4h + 3; 128 threads per leaf,
+// kResidualLeaves leaves per CTA): its four values and those of the four x/y neighbour rows
+// (the neighbour leaf's row across a face, 0 for a missing leaf) as 16-byte loads, and the two
+// z neighbours past its ends (the other half of the row, or the leaf across the z face), with
+// the Laplacian summed in the order +x, -x, +y, -y, +z, -z, -6 p. Half rows keep the kernel
+// under 64 registers, twice the resident warps of whole rows.
+constexpr int kResidualLeaves = kThreads / 128;
 
-__device__ __forceinline__ void ld_row8(const double* __restrict__ q, double v[8]) {
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-        const double2 x = __ldg(reinterpret_cast<const double2*>(q) + h);
-        v[2 * h] = x.x, v[2 * h + 1] = x.y;
-    }
+__device__ __forceinline__ void ld_half4(const double* __restrict__ q, double v[4]) {
+    const double2 x0 = __ldg(reinterpret_cast<const double2*>(q));
+    const double2 x1 = __ldg(reinterpret_cast<const double2*>(q) + 1);
+    v[0] = x0.x, v[1] = x0.y, v[2] = x1.x, v[3] = x1.y;
 }
 
 __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, const float* __restrict__ div,
@@ -227,51 +227,51 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
                                                                     const double* __restrict__ check, double tol2,
                                                                     double* __restrict__ acc) {
     if (converged(check, tol2)) return;
-    const int64_t leaf = (int64_t)blockIdx.x * kResidualLeaves + (threadIdx.x >> 6);
-    const int row = threadIdx.x & 63, a = row >> 3, b = row & 7;
+    const int64_t leaf = (int64_t)blockIdx.x * kResidualLeaves + (threadIdx.x >> 7);
+    const int row = (threadIdx.x >> 1) & 63, h = threadIdx.x & 1, a = row >> 3, b = row & 7;
     double r2 = 0.0, b2 = 0.0;
     if (leaf < t.num_leaves) {
-        const int64_t own = (leaf << 9) + 8 * row;
-        const float4 d0 = __ldg(reinterpret_cast<const float4*>(div + own));
-        const float4 d1 = __ldg(reinterpret_cast<const float4*>(div + own) + 1);
-        const float dv[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
-        double res[8];
+        const int64_t own = (leaf << 9) + 8 * row + 4 * h;
+        const float4 d = __ldg(reinterpret_cast<const float4*>(div + own));
+        const float dv[4] = {d.x, d.y, d.z, d.w};
+        double res[4];
         if (p != nullptr) {
             const int* nb = t.nbr27 + leaf * 27;
-            // nbr27: (dx+1)*9 + (dy+1)*3 + (dz+1); entry 13 is the leaf itself.
+            // nbr27: (dx+1)*9 + (dy+1)*3 + (dz+1); entry 13 is the leaf itself. The z face this
+            // half row touches: -z for h = 0, +z for h = 1.
             const int nx = __ldg(nb + (a == 7 ? 22 : a == 0 ? 4 : 13)), ny = __ldg(nb + (b == 7 ? 16 : b == 0 ? 10 : 13));
-            const int nzm = __ldg(nb + 12), nzp = __ldg(nb + 14);
-            auto across = [&](int n, int rw) -> int64_t { return n < 0 ? own : ((int64_t)n << 9) + 8 * rw; };
-            double c[8], xp[8], xm[8], yp[8], ym[8];
-            ld_row8(p + own, c);
-            ld_row8(p + (a < 7 ? own + 64 : across(nx, b)), xp);
-            ld_row8(p + (a > 0 ? own - 64 : across(nx, 56 + b)), xm);
-            ld_row8(p + (b < 7 ? own + 8 : across(ny, 8 * a)), yp);
-            ld_row8(p + (b > 0 ? own - 8 : across(ny, 8 * a + 7)), ym);
-            const double zlo = nzm < 0 ? 0.0 : __ldg(p + ((int64_t)nzm << 9) + 8 * row + 7);
-            const double zhi = nzp < 0 ? 0.0 : __ldg(p + ((int64_t)nzp << 9) + 8 * row);
+            const int nz = __ldg(nb + (h ? 14 : 12));
+            auto across = [&](int n, int rw) -> int64_t { return n < 0 ? own : ((int64_t)n << 9) + 8 * rw + 4 * h; };
+            double c[4], xp[4], xm[4], yp[4], ym[4];
+            ld_half4(p + own, c);
+            ld_half4(p + (a < 7 ? own + 64 : across(nx, b)), xp);
+            ld_half4(p + (a > 0 ? own - 64 : across(nx, 56 + b)), xm);
+            ld_half4(p + (b < 7 ? own + 8 : across(ny, 8 * a)), yp);
+            ld_half4(p + (b > 0 ? own - 8 : across(ny, 8 * a + 7)), ym);
+            // The row's other half (inside the leaf) and the value across the z face.
+            const double zin = __ldg(p + (h ? own - 1 : own + 4));
+            const double zface = nz < 0 ? 0.0 : __ldg(p + ((int64_t)nz << 9) + 8 * row + (h ? 0 : 7));
+            const double zlo = h ? zin : zface, zhi = h ? zface : zin;
             const bool zxp = a == 7 && nx < 0, zxm = a == 0 && nx < 0, zyp = b == 7 && ny < 0, zym = b == 0 && ny < 0;
 #pragma unroll
-            for (int z = 0; z < 8; ++z) {
+            for (int z = 0; z < 4; ++z) {
                 const double lap = (zxp ? 0.0 : xp[z]) + (zxm ? 0.0 : xm[z]) + (zyp ? 0.0 : yp[z]) +
-                                   (zym ? 0.0 : ym[z]) + (z < 7 ? c[z + 1] : zhi) + (z > 0 ? c[z - 1] : zlo) -
+                                   (zym ? 0.0 : ym[z]) + (z < 3 ? c[z + 1] : zhi) + (z > 0 ? c[z - 1] : zlo) -
                                    6.0 * c[z];
                 res[z] = (double)dv[z] * h2 - lap;
             }
         } else {
 #pragma unroll
-            for (int z = 0; z < 8; ++z) res[z] = (double)dv[z] * h2;
+            for (int z = 0; z < 4; ++z) res[z] = (double)dv[z] * h2;
             if (p_zero_out != nullptr) {
                 double2* pz = reinterpret_cast<double2*>(p_zero_out + own);
-#pragma unroll
-                for (int h = 0; h < 4; ++h) pz[h] = make_double2(0.0, 0.0);
+                pz[0] = make_double2(0.0, 0.0);
+                pz[1] = make_double2(0.0, 0.0);
             }
         }
-        float4* ro = reinterpret_cast<float4*>(r + own);
-        ro[0] = make_float4((float)res[0], (float)res[1], (float)res[2], (float)res[3]);
-        ro[1] = make_float4((float)res[4], (float)res[5], (float)res[6], (float)res[7]);
+        *reinterpret_cast<float4*>(r + own) = make_float4((float)res[0], (float)res[1], (float)res[2], (float)res[3]);
 #pragma unroll
-        for (int z = 0; z < 8; ++z) {
+        for (int z = 0; z < 4; ++z) {
             const double bb = (double)dv[z] * h2;
             r2 += res[z] * res[z];
             b2 += bb * bb;

@@ -108,6 +108,10 @@ __global__ void __launch_bounds__(kThreads) rbgs_split_half_kernel(const int* __
                                                                     unsigned long long* __restrict__ counters) {
     if (check != nullptr && check[0] <= tol2 * check[1]) return;  // the refinement has converged
     if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, 1ull);  // launches that ran
+    // The next half-sweep may be scheduled as soon as every block of this one has started: its
+    // blocks take the SM slots this launch's last wave frees and load what no sweep writes
+    // before they wait for this launch to finish.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
     const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
     const int p = (w + colour) & 1;  // z parity of this colour in the warp's rows
@@ -146,6 +150,9 @@ __global__ void __launch_bounds__(kThreads) rbgs_split_half_kernel(const int* __
             ny[k] = (uint32_t)__ldg(nb + sy);
             nz[k] = (uint32_t)__ldg(nb + sz);  // -z leaf for p = 0, +z for p = 1
         }
+        // e is written by the preceding half-sweep: wait until it has finished (a no-op for a
+        // launch without the programmatic-serialization attribute).
+        asm volatile("griddepcontrol.wait;" ::: "memory");
         uint2 C[kLeavesPerThread], K[kLeavesPerThread], XP[kLeavesPerThread], XM[kLeavesPerThread],
             YP[kLeavesPerThread], YM[kLeavesPerThread];
         uint32_t ZC[kLeavesPerThread];
@@ -192,12 +199,28 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     const unsigned blocks = (unsigned)((L + per_block - 1) / per_block);
     const auto* r = static_cast<const __half*>(rhs);
     auto* x = static_cast<__half*>(e);
-    if (e_zero)
+    if (e_zero) {
         rbgs_split_half_kernel<true><<<blocks, kThreads, 0, c.stream>>>(nb8, r, x, (int)L, colour, omega, check, tol2,
                                                                          c.counters);
-    else
-        rbgs_split_half_kernel<false><<<blocks, kThreads, 0, c.stream>>>(nb8, r, x, (int)L, colour, omega, check, tol2,
-                                                                          c.counters);
+        HNS_LAUNCHED();
+        return;
+    }
+    // Programmatic dependent launch: the sweep's prologue (the convergence check, the face table
+    // and the right-hand side) overlaps the tail of the preceding half-sweep, and e is read after
+    // griddepcontrol.wait. The caller guarantees that the preceding kernel on the stream is a
+    // half-sweep and that rhs, nb8 and check were written before it started.
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<false>, nb8, r, x, (int)L, colour, omega, check, tol2,
+                                c.counters));
     HNS_LAUNCHED();
 }
 
