@@ -159,66 +159,183 @@ __global__ void __launch_bounds__(kThreads, 3) advect_mixed_kernel(TopoView t, c
     }
 }
 
-// Divergence (divergence, src/Cuda/Kernel.cu:432-453) of a reduced-precision velocity into
-// FP32, with sum (div dx^2)^2 accumulated in FP64 when `acc` is set.
-template <typename V>
-__global__ void __launch_bounds__(kThreads) divergence_mixed_kernel(TopoView t, const V* __restrict__ vel,
-                                                                     float* __restrict__ div, float inv_dx, double h2) {
-    __shared__ LeafNbhd L;
-    const VoxelIdx v = voxel_of_block();
-    load_nbhd(L, t, v.leaf);
-    __syncthreads();
-    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
-    const int64_t s = (v.leaf << 9) + v.n;
-    const float3 c = vload(vel, s);
-    const float xp = (c.x + tap3(vel, slot_of(t, L, i + 1, j, k)).x) * 0.5f;
-    const float xm = (c.x + tap3(vel, slot_of(t, L, i - 1, j, k)).x) * 0.5f;
-    const float yp = (c.y + tap3(vel, slot_of(t, L, i, j + 1, k)).y) * 0.5f;
-    const float ym = (c.y + tap3(vel, slot_of(t, L, i, j - 1, k)).y) * 0.5f;
-    const float zp = (c.z + tap3(vel, slot_of(t, L, i, j, k + 1)).z) * 0.5f;
-    const float zm = (c.z + tap3(vel, slot_of(t, L, i, j, k - 1)).z) * 0.5f;
-    div[s] = (xp - xm + yp - ym + zp - zm) * inv_dx;
+// ---- stencils over half z-rows ------------------------------------------------------------
+//
+// The divergence, the gradient subtraction and the refinement residual are 7-point stencils in
+// leaf slot order, where a leaf's z-row (x, y) = (a, b) is 8 contiguous slots. Thread (leaf, row,
+// h) of a 256-thread CTA covers z = 4h .. 4h + 3 of one row (128 threads per leaf, kRowLeaves
+// leaves per CTA): it loads its half row and the same half of the four x/y neighbour rows (the
+// row of the leaf across a face at the leaf's edge; a missing leaf reads 0) as vector loads,
+// and the two z neighbours past its ends (the row's other half, or the leaf across the z face).
+// The leaves' face neighbours come straight from the 27-neighbour table: no staging, no barrier.
+constexpr int kRowLeaves = kThreads / 128;
+
+struct HalfRow {
+    int64_t leaf, own;   // own: slot of the half row's first voxel (a multiple of 4)
+    int row, h, a, b;    // row = 8 a + b
+    int nx, ny, nz;      // leaf across the x face / y face this row touches (itself inside), across
+                         // the z face this half touches (-z for h = 0, +z for h = 1); -1 missing
+};
+
+__device__ __forceinline__ bool half_row(const TopoView& t, HalfRow& r) {
+    r.leaf = (int64_t)blockIdx.x * kRowLeaves + (threadIdx.x >> 7);
+    if (r.leaf >= t.num_leaves) return false;
+    r.row = (threadIdx.x >> 1) & 63, r.h = threadIdx.x & 1, r.a = r.row >> 3, r.b = r.row & 7;
+    r.own = (r.leaf << 9) + 8 * r.row + 4 * r.h;
+    const int* nb = t.nbr27 + r.leaf * 27;
+    // nbr27: (dx+1)*9 + (dy+1)*3 + (dz+1); entry 13 is the leaf itself.
+    r.nx = __ldg(nb + (r.a == 7 ? 22 : r.a == 0 ? 4 : 13));
+    r.ny = __ldg(nb + (r.b == 7 ? 16 : r.b == 0 ? 10 : 13));
+    r.nz = __ldg(nb + (r.h ? 14 : 12));
+    return true;
 }
 
-// u -= grad p with p in FP64 (0 outside the domain), velocity in reduced precision, in place.
-template <typename V>
-__global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V* __restrict__ vel,
-                                                                   const double* __restrict__ p, float inv_dx) {
-    __shared__ LeafNbhd L;
-    const VoxelIdx v = voxel_of_block();
-    load_nbhd(L, t, v.leaf);
-    __syncthreads();
-    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
-    const int64_t s = (v.leaf << 9) + v.n;
-    auto P = [&](int a, int b, int c) {
-        const int64_t q = slot_of(t, L, a, b, c);
-        return q < 0 ? 0.0 : __ldg(p + q);
-    };
-    const double h = 0.5 * (double)inv_dx;
-    const float gx = (float)((P(i + 1, j, k) - P(i - 1, j, k)) * h);
-    const float gy = (float)((P(i, j + 1, k) - P(i, j - 1, k)) * h);
-    const float gz = (float)((P(i, j, k + 1) - P(i, j, k - 1)) * h);
-    const float3 u = vload(vel, s);
-    vstore(vel, s, make_float3(u.x - gx, u.y - gy, u.z - gz));
+// Slots of the same half row in the four x/y neighbour rows (the half row itself where the
+// neighbour leaf is missing: its values are then replaced by 0).
+struct NbrRows {
+    int64_t xp, xm, yp, ym;
+    bool zxp, zxm, zyp, zym;  // missing neighbour: read as 0
+};
+
+__device__ __forceinline__ NbrRows nbr_rows(const HalfRow& r) {
+    auto across = [&](int n, int rw) -> int64_t { return n < 0 ? r.own : ((int64_t)n << 9) + 8 * rw + 4 * r.h; };
+    NbrRows q;
+    q.xp = r.a < 7 ? r.own + 64 : across(r.nx, r.b);
+    q.xm = r.a > 0 ? r.own - 64 : across(r.nx, 56 + r.b);
+    q.yp = r.b < 7 ? r.own + 8 : across(r.ny, 8 * r.a);
+    q.ym = r.b > 0 ? r.own - 8 : across(r.ny, 8 * r.a + 7);
+    q.zxp = r.a == 7 && r.nx < 0, q.zxm = r.a == 0 && r.nx < 0, q.zyp = r.b == 7 && r.ny < 0, q.zym = r.b == 0 && r.ny < 0;
+    return q;
 }
 
-// ---- refinement --------------------------------------------------------------------------
-
-// r = b - L p (FP64 arithmetic, r stored FP32) with b = div dx^2 and p = 0 outside the domain,
-// plus sum r^2 and sum b^2 into acc. p null: p = 0 (r = b), and p_zero_out, when set, is
-// cleared. One thread per half z-row of a leaf (z = 4h .. 4h + 3; 128 threads per leaf,
-// kResidualLeaves leaves per CTA): its four values and those of the four x/y neighbour rows
-// (the neighbour leaf's row across a face, 0 for a missing leaf) as 16-byte loads, and the two
-// z neighbours past its ends (the other half of the row, or the leaf across the z face), with
-// the Laplacian summed in the order +x, -x, +y, -y, +z, -z, -6 p. Half rows keep the kernel
-// under 64 registers, twice the resident warps of whole rows.
-constexpr int kResidualLeaves = kThreads / 128;
+// Slots of the z neighbours past the half row's ends: the row's other half, and the voxel
+// across the z face (-1 when that leaf is missing).
+__device__ __forceinline__ void z_ends(const HalfRow& r, int64_t& zin, int64_t& zface) {
+    zin = r.h ? r.own - 1 : r.own + 4;
+    zface = r.nz < 0 ? -1 : ((int64_t)r.nz << 9) + 8 * r.row + (r.h ? 0 : 7);
+}
 
 __device__ __forceinline__ void ld_half4(const double* __restrict__ q, double v[4]) {
     const double2 x0 = __ldg(reinterpret_cast<const double2*>(q));
     const double2 x1 = __ldg(reinterpret_cast<const double2*>(q) + 1);
     v[0] = x0.x, v[1] = x0.y, v[2] = x1.x, v[3] = x1.y;
 }
+
+// Velocity of four voxels from slot s (a multiple of 4): 12 interleaved components, 24 bytes in
+// BF16 (three 8-byte loads) or 48 in FP32 (three 16-byte loads).
+__device__ __forceinline__ float bf16_bits(uint32_t w, int hi) { return __uint_as_float(hi ? (w & 0xFFFF0000u) : (w << 16)); }
+
+__device__ __forceinline__ void vel_half_row(const __nv_bfloat16* __restrict__ v, int64_t s, float3 u[4]) {
+    const uint2* q = reinterpret_cast<const uint2*>(v + 3 * s);
+    const uint2 w0 = __ldg(q), w1 = __ldg(q + 1), w2 = __ldg(q + 2);
+    const uint32_t w[6] = {w0.x, w0.y, w1.x, w1.y, w2.x, w2.y};
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+        const int e = 3 * z;
+        u[z] = make_float3(bf16_bits(w[e >> 1], e & 1), bf16_bits(w[(e + 1) >> 1], (e + 1) & 1),
+                           bf16_bits(w[(e + 2) >> 1], (e + 2) & 1));
+    }
+}
+__device__ __forceinline__ void vel_half_row(const float* __restrict__ v, int64_t s, float3 u[4]) {
+    const float4* q = reinterpret_cast<const float4*>(v + 3 * s);
+    const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    u[0] = make_float3(a.x, a.y, a.z);
+    u[1] = make_float3(a.w, b.x, b.y);
+    u[2] = make_float3(b.z, b.w, c.x);
+    u[3] = make_float3(c.y, c.z, c.w);
+}
+
+__device__ __forceinline__ uint32_t bf16x2_bits(float lo, float hi) {
+    const __nv_bfloat162 r = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&r);
+}
+__device__ __forceinline__ void store_vel_half_row(__nv_bfloat16* v, int64_t s, const float3 u[4]) {
+    uint2* q = reinterpret_cast<uint2*>(v + 3 * s);
+    q[0] = make_uint2(bf16x2_bits(u[0].x, u[0].y), bf16x2_bits(u[0].z, u[1].x));
+    q[1] = make_uint2(bf16x2_bits(u[1].y, u[1].z), bf16x2_bits(u[2].x, u[2].y));
+    q[2] = make_uint2(bf16x2_bits(u[2].z, u[3].x), bf16x2_bits(u[3].y, u[3].z));
+}
+__device__ __forceinline__ void store_vel_half_row(float* v, int64_t s, const float3 u[4]) {
+    float4* q = reinterpret_cast<float4*>(v + 3 * s);
+    q[0] = make_float4(u[0].x, u[0].y, u[0].z, u[1].x);
+    q[1] = make_float4(u[1].y, u[1].z, u[2].x, u[2].y);
+    q[2] = make_float4(u[2].z, u[3].x, u[3].y, u[3].z);
+}
+
+__device__ __forceinline__ float vel_z(const __nv_bfloat16* __restrict__ v, int64_t s) {
+    return __bfloat162float(__ldg(v + 3 * s + 2));
+}
+
+// Divergence (divergence, src/Cuda/Kernel.cu:432-453) of a reduced-precision velocity into
+// FP32: per voxel the face velocities are the means of the centre and the neighbour (0 for a
+// missing neighbour), div = (xp - xm + yp - ym + zp - zm) / dx.
+template <typename V>
+__global__ void __launch_bounds__(kThreads) divergence_mixed_kernel(TopoView t, const V* __restrict__ vel,
+                                                                     float* __restrict__ div, float inv_dx) {
+    HalfRow r;
+    if (!half_row(t, r)) return;
+    const NbrRows q = nbr_rows(r);
+    float3 c[4], xp[4], xm[4], yp[4], ym[4];
+    vel_half_row(vel, r.own, c);
+    vel_half_row(vel, q.xp, xp);
+    vel_half_row(vel, q.xm, xm);
+    vel_half_row(vel, q.yp, yp);
+    vel_half_row(vel, q.ym, ym);
+    int64_t zin_s, zface_s;
+    z_ends(r, zin_s, zface_s);
+    const float zin = vel_z(vel, zin_s), zface = zface_s < 0 ? 0.f : vel_z(vel, zface_s);
+    const float zlo = r.h ? zin : zface, zhi = r.h ? zface : zin;
+    float d[4];
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+        const float vxp = (c[z].x + (q.zxp ? 0.f : xp[z].x)) * 0.5f;
+        const float vxm = (c[z].x + (q.zxm ? 0.f : xm[z].x)) * 0.5f;
+        const float vyp = (c[z].y + (q.zyp ? 0.f : yp[z].y)) * 0.5f;
+        const float vym = (c[z].y + (q.zym ? 0.f : ym[z].y)) * 0.5f;
+        const float vzp = (c[z].z + (z < 3 ? c[z + 1].z : zhi)) * 0.5f;
+        const float vzm = (c[z].z + (z > 0 ? c[z - 1].z : zlo)) * 0.5f;
+        d[z] = (vxp - vxm + vyp - vym + vzp - vzm) * inv_dx;
+    }
+    *reinterpret_cast<float4*>(div + r.own) = make_float4(d[0], d[1], d[2], d[3]);
+}
+
+// u -= grad p with p in FP64 (0 outside the domain), central differences
+// (subtractPressureGradient, src/Cuda/Kernel.cu:495-541), velocity in reduced precision or
+// FP32, in place.
+template <typename V>
+__global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V* __restrict__ vel,
+                                                                   const double* __restrict__ p, float inv_dx) {
+    HalfRow r;
+    if (!half_row(t, r)) return;
+    const NbrRows q = nbr_rows(r);
+    double c[4], xp[4], xm[4], yp[4], ym[4];
+    ld_half4(p + r.own, c);
+    ld_half4(p + q.xp, xp);
+    ld_half4(p + q.xm, xm);
+    ld_half4(p + q.yp, yp);
+    ld_half4(p + q.ym, ym);
+    int64_t zin_s, zface_s;
+    z_ends(r, zin_s, zface_s);
+    const double zin = __ldg(p + zin_s), zface = zface_s < 0 ? 0.0 : __ldg(p + zface_s);
+    const double zlo = r.h ? zin : zface, zhi = r.h ? zface : zin;
+    float3 u[4];
+    vel_half_row(vel, r.own, u);
+    const double hh = 0.5 * (double)inv_dx;
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+        const float gx = (float)(((q.zxp ? 0.0 : xp[z]) - (q.zxm ? 0.0 : xm[z])) * hh);
+        const float gy = (float)(((q.zyp ? 0.0 : yp[z]) - (q.zym ? 0.0 : ym[z])) * hh);
+        const float gz = (float)(((z < 3 ? c[z + 1] : zhi) - (z > 0 ? c[z - 1] : zlo)) * hh);
+        u[z] = make_float3(u[z].x - gx, u[z].y - gy, u[z].z - gz);
+    }
+    store_vel_half_row(vel, r.own, u);
+}
+
+// ---- refinement --------------------------------------------------------------------------
+
+// r = b - L p (FP64 arithmetic, r stored FP32) with b = div dx^2 and p = 0 outside the domain,
+// plus sum r^2 and sum b^2 into acc, over half z-rows, with the Laplacian summed in the order
+// +x, -x, +y, -y, +z, -z, -6 p. p null: p = 0 (r = b), and p_zero_out, when set, is cleared.
 
 __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, const float* __restrict__ div,
                                                                     const double* __restrict__ p,
@@ -227,36 +344,28 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
                                                                     const double* __restrict__ check, double tol2,
                                                                     double* __restrict__ acc) {
     if (converged(check, tol2)) return;
-    const int64_t leaf = (int64_t)blockIdx.x * kResidualLeaves + (threadIdx.x >> 7);
-    const int row = (threadIdx.x >> 1) & 63, h = threadIdx.x & 1, a = row >> 3, b = row & 7;
     double r2 = 0.0, b2 = 0.0;
-    if (leaf < t.num_leaves) {
-        const int64_t own = (leaf << 9) + 8 * row + 4 * h;
-        const float4 d = __ldg(reinterpret_cast<const float4*>(div + own));
+    HalfRow w;
+    if (half_row(t, w)) {
+        const float4 d = __ldg(reinterpret_cast<const float4*>(div + w.own));
         const float dv[4] = {d.x, d.y, d.z, d.w};
         double res[4];
         if (p != nullptr) {
-            const int* nb = t.nbr27 + leaf * 27;
-            // nbr27: (dx+1)*9 + (dy+1)*3 + (dz+1); entry 13 is the leaf itself. The z face this
-            // half row touches: -z for h = 0, +z for h = 1.
-            const int nx = __ldg(nb + (a == 7 ? 22 : a == 0 ? 4 : 13)), ny = __ldg(nb + (b == 7 ? 16 : b == 0 ? 10 : 13));
-            const int nz = __ldg(nb + (h ? 14 : 12));
-            auto across = [&](int n, int rw) -> int64_t { return n < 0 ? own : ((int64_t)n << 9) + 8 * rw + 4 * h; };
+            const NbrRows q = nbr_rows(w);
             double c[4], xp[4], xm[4], yp[4], ym[4];
-            ld_half4(p + own, c);
-            ld_half4(p + (a < 7 ? own + 64 : across(nx, b)), xp);
-            ld_half4(p + (a > 0 ? own - 64 : across(nx, 56 + b)), xm);
-            ld_half4(p + (b < 7 ? own + 8 : across(ny, 8 * a)), yp);
-            ld_half4(p + (b > 0 ? own - 8 : across(ny, 8 * a + 7)), ym);
-            // The row's other half (inside the leaf) and the value across the z face.
-            const double zin = __ldg(p + (h ? own - 1 : own + 4));
-            const double zface = nz < 0 ? 0.0 : __ldg(p + ((int64_t)nz << 9) + 8 * row + (h ? 0 : 7));
-            const double zlo = h ? zin : zface, zhi = h ? zface : zin;
-            const bool zxp = a == 7 && nx < 0, zxm = a == 0 && nx < 0, zyp = b == 7 && ny < 0, zym = b == 0 && ny < 0;
+            ld_half4(p + w.own, c);
+            ld_half4(p + q.xp, xp);
+            ld_half4(p + q.xm, xm);
+            ld_half4(p + q.yp, yp);
+            ld_half4(p + q.ym, ym);
+            int64_t zin_s, zface_s;
+            z_ends(w, zin_s, zface_s);
+            const double zin = __ldg(p + zin_s), zface = zface_s < 0 ? 0.0 : __ldg(p + zface_s);
+            const double zlo = w.h ? zin : zface, zhi = w.h ? zface : zin;
 #pragma unroll
             for (int z = 0; z < 4; ++z) {
-                const double lap = (zxp ? 0.0 : xp[z]) + (zxm ? 0.0 : xm[z]) + (zyp ? 0.0 : yp[z]) +
-                                   (zym ? 0.0 : ym[z]) + (z < 3 ? c[z + 1] : zhi) + (z > 0 ? c[z - 1] : zlo) -
+                const double lap = (q.zxp ? 0.0 : xp[z]) + (q.zxm ? 0.0 : xm[z]) + (q.zyp ? 0.0 : yp[z]) +
+                                   (q.zym ? 0.0 : ym[z]) + (z < 3 ? c[z + 1] : zhi) + (z > 0 ? c[z - 1] : zlo) -
                                    6.0 * c[z];
                 res[z] = (double)dv[z] * h2 - lap;
             }
@@ -264,12 +373,12 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
 #pragma unroll
             for (int z = 0; z < 4; ++z) res[z] = (double)dv[z] * h2;
             if (p_zero_out != nullptr) {
-                double2* pz = reinterpret_cast<double2*>(p_zero_out + own);
+                double2* pz = reinterpret_cast<double2*>(p_zero_out + w.own);
                 pz[0] = make_double2(0.0, 0.0);
                 pz[1] = make_double2(0.0, 0.0);
             }
         }
-        *reinterpret_cast<float4*>(r + own) = make_float4((float)res[0], (float)res[1], (float)res[2], (float)res[3]);
+        *reinterpret_cast<float4*>(r + w.own) = make_float4((float)res[0], (float)res[1], (float)res[2], (float)res[3]);
 #pragma unroll
         for (int z = 0; z < 4; ++z) {
             const double bb = (double)dv[z] * h2;
@@ -327,9 +436,8 @@ __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restr
         p[q] += sc * (double)sload(e, inner_slot<kLayout>(q));
 }
 
-unsigned residual_blocks(const Context& c) {
-    return (unsigned)((c.topo.num_leaves + kResidualLeaves - 1) / kResidualLeaves);
-}
+unsigned row_blocks(const Context& c) { return (unsigned)((c.topo.num_leaves + kRowLeaves - 1) / kRowLeaves); }
+unsigned residual_blocks(const Context& c) { return row_blocks(c); }
 
 unsigned stream_blocks(const Context& c, int64_t n) {
     const int64_t b = (n + kThreads * 4 - 1) / (kThreads * 4);
@@ -554,20 +662,23 @@ void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const
 }
 
 void launch_divergence_mixed(const Context& c, const void* vel, float* div) {
-    divergence_mixed_kernel<__nv_bfloat16><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-        c.topo.view, static_cast<const __nv_bfloat16*>(vel), div, 1.0f / c.dx, (double)c.dx * (double)c.dx);
+    if (c.topo.num_leaves == 0) return;
+    divergence_mixed_kernel<__nv_bfloat16><<<row_blocks(c), kThreads, 0, c.stream>>>(
+        c.topo.view, static_cast<const __nv_bfloat16*>(vel), div, 1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
 void launch_gradient_mixed(const Context& c, void* vel, const double* p) {
-    gradient_mixed_kernel<__nv_bfloat16><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view,
+    if (c.topo.num_leaves == 0) return;
+    gradient_mixed_kernel<__nv_bfloat16><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view,
                                                                                      static_cast<__nv_bfloat16*>(vel), p,
                                                                                      1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
 void launch_gradient_f64(const Context& c, float* vel, const double* p) {
-    gradient_mixed_kernel<float><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, 1.0f / c.dx);
+    if (c.topo.num_leaves == 0) return;
+    gradient_mixed_kernel<float><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, 1.0f / c.dx);
     HNS_LAUNCHED();
 }
 

@@ -82,6 +82,22 @@ def test_mixed_step_against_fp64_oracle(dev, oracle, shell):
     r2, b2 = t.residual(div32.astype(np.float64), p.cpu().numpy(), dx32)
     assert np.sqrt(r2 / b2) <= 1e-5
     assert np.sqrt(r2 / b2) == pytest.approx(res, rel=1e-6)
+    # The gradient subtraction to the bit: the BF16 advected velocity minus the FP32-rounded
+    # FP64 central difference of the returned pressure (0 outside the domain), rounded to BF16.
+    p64 = p.cpu().numpy()
+    ijk = t.coords()
+    hh = 0.5 * float(np.float32(10.0))
+    expect = adv.astype(np.float32).copy()
+    for ax in range(3):
+        e = np.zeros(3, dtype=np.int32)
+        e[ax] = 1
+        off_p = t.offsets(ijk + e).astype(np.int64)
+        off_m = t.offsets(ijk - e).astype(np.int64)
+        pp = np.where(off_p == 0, 0.0, p64[np.maximum(off_p - 1, 0)])
+        pm = np.where(off_m == 0, 0.0, p64[np.maximum(off_m - 1, 0)])
+        expect[:, ax] = expect[:, ax] - ((pp - pm) * hh).astype(np.float32)
+    expect_bf16 = torch.from_numpy(expect).to(torch.bfloat16)
+    assert torch.equal(vo.cpu().view(-1, 3), expect_bf16)
     # Field error against the FP64 oracle (same BF16/FP16 inputs, FP64 advection, FP64 solve
     # to a residual far below 1e-5).
     v64 = v_in.astype(np.float64)
