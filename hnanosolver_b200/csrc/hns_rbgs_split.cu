@@ -16,7 +16,7 @@
 // the -z leaf's entry 3 of that row and entry 4 the +z leaf's entry 0. A missing leaf reads 0
 // (the reference's p = 0 outside the domain).
 //
-// Work: a thread relaxes the four voxels of one colour of a row, in two leaves, from eight
+// Work: a thread relaxes the four voxels of one colour of a row, in four leaves, from eight
 // 8-byte loads per leaf (the row's two colours, its right-hand side, the four neighbour rows)
 // and one of 2 bytes, and one 8-byte store. A half-sweep reads both colours of e and the
 // colour's right-hand side and writes the colour in place: about 3 bytes per voxel from DRAM,
@@ -37,8 +37,11 @@ namespace {
 
 using namespace relax16;
 
-constexpr int kLeavesPerBlock = 4;   // leaves whose rows one block's threads cover
-constexpr int kLeavesPerThread = 2;  // leaves a thread relaxes its row in
+// Measured on a 45,198-leaf grid (us per half-sweep): 4 x 2 (256 threads) 18.3, 4 x 3 17.4,
+// 2 x 3 17.1, 1 x 5 16.8, 2 x 4 16.7, 2 x 6 17.4, 1 x 1 22.2: more leaves per thread keep more
+// loads in flight, and small blocks leave a shorter tail to the last wave.
+constexpr int kLeavesPerBlock = 2;   // leaves whose rows one block's threads cover
+constexpr int kLeavesPerThread = 4;  // leaves a thread relaxes its row in
 constexpr int kThreads = 64 * kLeavesPerBlock;
 
 // nbr27 indices of the six face neighbours: (dx+1)*9 + (dy+1)*3 + (dz+1).
@@ -97,7 +100,7 @@ __device__ __forceinline__ uint2 relax_row(uint2 XP, uint2 XM, uint2 YP, uint2 Y
 // (a = l / 4, b = 2 (l % 4) + ((a + w) & 1)), so the z parity of the colour is uniform in a warp
 // and the z neighbours need no selects. A thread relaxes its row in kLeavesPerThread leaves
 // (kLeavesPerBlock apart), issuing every load before any arithmetic: the kernel is bound by
-// memory latency, and this doubles the bytes each thread has in flight. Loads are
+// memory latency, and this multiplies the bytes each thread has in flight. Loads are
 // unconditional: a row on a leaf face reads the neighbour leaf's row, a missing neighbour the
 // zero leaf. Offsets are 32-bit element counts (fewer than 2^22 leaves).
 template <bool kZero>
