@@ -42,9 +42,10 @@ __device__ __forceinline__ bool converged(const double* check, double tol2) {
     return check != nullptr && check[0] <= tol2 * check[1];
 }
 
-// Block-wide FP64 sum of two values into acc[0], acc[1] (256 threads).
+// Block-wide FP64 sum of two values into acc[0], acc[1] (kBlock threads).
+template <int kBlock = kThreads>
 __device__ __forceinline__ void block_sum2(double a, double b, double* acc) {
-    __shared__ double red[2][kThreads / 32];
+    __shared__ double red[2][kBlock / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -53,8 +54,8 @@ __device__ __forceinline__ void block_sum2(double a, double b, double* acc) {
     if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = a, red[1][threadIdx.x >> 5] = b;
     __syncthreads();
     if (threadIdx.x < 32) {
-        a = threadIdx.x < kThreads / 32 ? red[0][threadIdx.x] : 0.0;
-        b = threadIdx.x < kThreads / 32 ? red[1][threadIdx.x] : 0.0;
+        a = threadIdx.x < kBlock / 32 ? red[0][threadIdx.x] : 0.0;
+        b = threadIdx.x < kBlock / 32 ? red[1][threadIdx.x] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -69,17 +70,22 @@ __device__ __forceinline__ void block_sum2(double a, double b, double* acc) {
 
 // ---- advection on reduced-precision storage ---------------------------------------------
 
-template <typename V>
-__device__ __forceinline__ float3 tap3(const V* d, int64_t s) {
-    return s < 0 ? make_float3(0.f, 0.f, 0.f) : vload(d, s);
+// Reduced-precision loads at a 32- or 64-bit slot (-1: outside the domain, read as 0). A 32-bit
+// slot is widened in the multiply (one IMAD.WIDE per address).
+__device__ __forceinline__ int64_t wide(int32_t s) { return (int64_t)(uint32_t)s; }
+__device__ __forceinline__ int64_t wide(int64_t s) { return s; }
+
+template <typename V, typename I>
+__device__ __forceinline__ float3 tap3(const V* d, I s) {
+    return s < 0 ? make_float3(0.f, 0.f, 0.f) : vload(d, wide(s));
 }
-template <typename S>
-__device__ __forceinline__ float tap1(const S* d, int64_t s) {
-    return s < 0 ? 0.f : sload(d, s);
+template <typename S, typename I>
+__device__ __forceinline__ float tap1(const S* d, I s) {
+    return s < 0 ? 0.f : sload(d, wide(s));
 }
 
-template <typename V>
-__device__ __forceinline__ float3 tri3(const Taps& T, const V* d) {
+template <typename V, typename I>
+__device__ __forceinline__ float3 tri3(const TapsT<I>& T, const V* d) {
     float x[8], y[8], z[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -89,8 +95,8 @@ __device__ __forceinline__ float3 tri3(const Taps& T, const V* d) {
     return make_float3(tri_lerp(T, x), tri_lerp(T, y), tri_lerp(T, z));
 }
 
-template <typename S>
-__device__ __forceinline__ float tri1(const Taps& T, const S* d) {
+template <typename S, typename I>
+__device__ __forceinline__ float tri1(const TapsT<I>& T, const S* d) {
     float v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = tap1(d, T.s[q]);
@@ -106,7 +112,8 @@ struct FieldSetT {
 
 // advect_vector + advect_scalar along one shared trace (as advect_fused_kernel), reading and
 // writing reduced-precision storage.
-template <typename V, typename S>
+// I: the slot type (int32_t for fewer than 2^22 leaves).
+template <typename V, typename S, typename I>
 __global__ void __launch_bounds__(kThreads, 3) advect_mixed_kernel(TopoView t, const V* __restrict__ vel,
                                                                  V* __restrict__ vel_out, FieldSetT<S> f, float sdt) {
     __shared__ LeafNbhd L;
@@ -114,14 +121,14 @@ __global__ void __launch_bounds__(kThreads, 3) advect_mixed_kernel(TopoView t, c
     load_nbhd(L, t, v.leaf);
     __syncthreads();
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
-    const int64_t s = (v.leaf << 9) + v.n;
-    const float3 vo = vload(vel, s);
+    const I s = (I(v.leaf) << 9) + I(v.n);
+    const float3 vo = vload(vel, wide(s));
     const float bx = (float)i - vo.x * sdt, by = (float)j - vo.y * sdt, bz = (float)k - vo.z * sdt;
-    Taps tb, tf;
+    TapsT<I> tb, tf;
     taps_at(tb, t, L, bx, by, bz);
     const float3 vf = tri3(tb, vel);
     taps_at(tf, t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt);
-    int64_t ns[6];
+    I ns[6];
     face_slots(L, s, v.n, ns);
     if (vel_out != nullptr) {
         const float3 vb = tri3(tf, vel);
@@ -138,11 +145,11 @@ __global__ void __launch_bounds__(kThreads, 3) advect_mixed_kernel(TopoView t, c
         corr.x = fmaxf(mn.x, fminf(corr.x, mx.x));
         corr.y = fmaxf(mn.y, fminf(corr.y, mx.y));
         corr.z = fmaxf(mn.z, fminf(corr.z, mx.z));
-        vstore(vel_out, s, corr);
+        vstore(vel_out, wide(s), corr);
     }
     for (int c = 0; c < f.count; ++c) {
         const S* __restrict__ d = f.in[c];
-        const float po = sload(d, s);
+        const float po = sload(d, wide(s));
         const float pf = tri1(tb, d);
         const float pb = tri1(tf, d);
         const float corr = pf + 0.5f * (po - pb);
@@ -155,19 +162,21 @@ __global__ void __launch_bounds__(kThreads, 3) advect_mixed_kernel(TopoView t, c
         }
         mn = fminf(mn, pf);
         mx = fmaxf(mx, pf);
-        sstore(f.out[c], s, fmaxf(mn, fminf(corr, mx)));
+        sstore(f.out[c], wide(s), fmaxf(mn, fminf(corr, mx)));
     }
 }
 
 // ---- stencils over half z-rows ------------------------------------------------------------
 //
 // The divergence, the gradient subtraction and the refinement residual are 7-point stencils in
-// leaf slot order, where a leaf's z-row (x, y) = (a, b) is 8 contiguous slots. Thread (leaf, row,
-// h) of a 256-thread CTA covers z = 4h .. 4h + 3 of one row (128 threads per leaf, kRowLeaves
-// leaves per CTA): it loads its half row and the same half of the four x/y neighbour rows (the
-// row of the leaf across a face at the leaf's edge; a missing leaf reads 0) as vector loads,
-// and the two z neighbours past its ends (the row's other half, or the leaf across the z face).
-// The leaves' face neighbours come straight from the 27-neighbour table: no staging, no barrier.
+// leaf slot order, where a leaf's z-row (x, y) = (a, b) is 8 contiguous slots. A thread covers
+// z = 4h .. 4h + 3 of one row (128 threads per leaf, kRowLeaves leaves per 256-thread CTA): it
+// loads its half row and the same half of the four x/y neighbour rows (the row of the leaf
+// across a face at the leaf's edge; a missing leaf reads 0) as vector loads, and the two z
+// neighbours past its ends (the row's other half, or the leaf across the z face). The leaves'
+// face neighbours come straight from the 27-neighbour table: no staging, no barrier. Measured
+// on a 45,198-leaf grid, one leaf per thread in 256-thread CTAs beat 128- and 512-thread CTAs
+// and two or three leaves per thread for all three stencils.
 constexpr int kRowLeaves = kThreads / 128;
 
 struct HalfRow {
@@ -177,8 +186,10 @@ struct HalfRow {
                          // the z face this half touches (-z for h = 0, +z for h = 1); -1 missing
 };
 
-__device__ __forceinline__ bool half_row(const TopoView& t, HalfRow& r) {
-    r.leaf = (int64_t)blockIdx.x * kRowLeaves + (threadIdx.x >> 7);
+// The half row of this thread in leaf group g (the kRowLeaves leaves one CTA covers); false
+// past the last leaf.
+__device__ __forceinline__ bool half_row(const TopoView& t, HalfRow& r, int64_t g) {
+    r.leaf = g * kRowLeaves + (threadIdx.x >> 7);
     if (r.leaf >= t.num_leaves) return false;
     r.row = (threadIdx.x >> 1) & 63, r.h = threadIdx.x & 1, r.a = r.row >> 3, r.b = r.row & 7;
     r.own = (r.leaf << 9) + 8 * r.row + 4 * r.h;
@@ -273,7 +284,7 @@ template <typename V>
 __global__ void __launch_bounds__(kThreads) divergence_mixed_kernel(TopoView t, const V* __restrict__ vel,
                                                                      float* __restrict__ div, float inv_dx) {
     HalfRow r;
-    if (!half_row(t, r)) return;
+    if (!half_row(t, r, blockIdx.x)) return;
     const NbrRows q = nbr_rows(r);
     float3 c[4], xp[4], xm[4], yp[4], ym[4];
     vel_half_row(vel, r.own, c);
@@ -306,7 +317,7 @@ template <typename V>
 __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V* __restrict__ vel,
                                                                    const double* __restrict__ p, float inv_dx) {
     HalfRow r;
-    if (!half_row(t, r)) return;
+    if (!half_row(t, r, blockIdx.x)) return;
     const NbrRows q = nbr_rows(r);
     double c[4], xp[4], xm[4], yp[4], ym[4];
     ld_half4(p + r.own, c);
@@ -336,7 +347,9 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
 // r = b - L p (FP64 arithmetic, r stored FP32) with b = div dx^2 and p = 0 outside the domain,
 // plus sum r^2 and sum b^2 into acc, over half z-rows, with the Laplacian summed in the order
 // +x, -x, +y, -y, +z, -z, -6 p. p null: p = 0 (r = b), and p_zero_out, when set, is cleared.
-
+// The grid is a few CTAs per SM, each looping over leaf groups and adding its two sums to acc
+// once: the FP64 atomics on the two sums serialise in one L2 slice, and one per leaf pair cost
+// more than a tenth of the kernel.
 __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, const float* __restrict__ div,
                                                                     const double* __restrict__ p,
                                                                     double* __restrict__ p_zero_out,
@@ -345,8 +358,11 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
                                                                     double* __restrict__ acc) {
     if (converged(check, tol2)) return;
     double r2 = 0.0, b2 = 0.0;
-    HalfRow w;
-    if (half_row(t, w)) {
+    const int64_t groups = (t.num_leaves + kRowLeaves - 1) / kRowLeaves;
+#pragma unroll 1
+    for (int64_t g = blockIdx.x; g < groups; g += gridDim.x) {
+        HalfRow w;
+        if (!half_row(t, w, g)) continue;
         const float4 d = __ldg(reinterpret_cast<const float4*>(div + w.own));
         const float dv[4] = {d.x, d.y, d.z, d.w};
         double res[4];
@@ -437,7 +453,17 @@ __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restr
 }
 
 unsigned row_blocks(const Context& c) { return (unsigned)((c.topo.num_leaves + kRowLeaves - 1) / kRowLeaves); }
-unsigned residual_blocks(const Context& c) { return row_blocks(c); }
+
+// Residual grid: one wave, kResidualCtasPerSm CTAs per SM (the register limit at 62 registers),
+// at most one per leaf group. Measured on a 45,198-leaf grid, six refinement residuals per step:
+// one CTA per leaf pair 1.35 ms of refinement work outside the inner solves, 6 CTAs per SM 1.28,
+// 12 per SM 1.18, 4 per SM 1.15 ms.
+constexpr int kResidualCtasPerSm = 4;
+unsigned residual_blocks(const Context& c) {
+    int sms = 0;
+    HNS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+    return std::max(1u, std::min(row_blocks(c), (unsigned)(sms * kResidualCtasPerSm)));
+}
 
 unsigned stream_blocks(const Context& c, int64_t n) {
     const int64_t b = (n + kThreads * 4 - 1) / (kThreads * 4);
@@ -653,9 +679,14 @@ void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const
             f.in[q] = static_cast<const __half*>(sin[base + q]);
             f.out[q] = static_cast<__half*>(sout[base + q]);
         }
-        advect_mixed_kernel<__nv_bfloat16, __half><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-            c.topo.view, static_cast<const __nv_bfloat16*>(vel), base == 0 ? static_cast<__nv_bfloat16*>(vel_out) : nullptr, f,
-            dt * (1.0f / c.dx));
+        const auto* vi = static_cast<const __nv_bfloat16*>(vel);
+        auto* vo = base == 0 ? static_cast<__nv_bfloat16*>(vel_out) : nullptr;
+        if (c.topo.num_leaves < (int64_t(1) << 22))
+            advect_mixed_kernel<__nv_bfloat16, __half, int32_t>
+                <<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vi, vo, f, dt * (1.0f / c.dx));
+        else
+            advect_mixed_kernel<__nv_bfloat16, __half, int64_t>
+                <<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vi, vo, f, dt * (1.0f / c.dx));
         HNS_LAUNCHED();
         base += f.count;
     } while (base < ns);

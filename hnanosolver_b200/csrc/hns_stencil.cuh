@@ -113,16 +113,21 @@ __device__ __forceinline__ float3 tri_v(const TopoView& t, const LeafNbhd& L, co
 // The eight taps of a trilinear sample at (x,y,z): slots (-1 outside the domain) of the
 // corners v[a][b][c] = (i+a, j+b, k+c) and the fractional position. Computing them once
 // lets several fields be sampled at the same point with shared addressing.
-struct Taps {
-    int64_t s[8];  // index a*4 + b*2 + c
+// I: the slot type, int64_t in general, int32_t where the grid has fewer than 2^22 leaves
+// (32-bit address arithmetic, half the integer instructions per tap).
+template <typename I>
+struct TapsT {
+    I s[8];  // index a*4 + b*2 + c
     float tx, ty, tz;
 };
+using Taps = TapsT<int64_t>;
 
 // The cell's two planes along each axis are resolved once: when both lie in the CTA leaf's
 // 3x3x3 neighbourhood (every trace shorter than a leaf), each corner's leaf is one
 // shared-memory lookup at a precomputed index and its slot an OR of precomputed local
 // offsets; otherwise every corner goes through slot_of (and the leaf table).
-__device__ __forceinline__ void taps_at(Taps& T, const TopoView& t, const LeafNbhd& L, float x, float y, float z) {
+template <typename I>
+__device__ __forceinline__ void taps_at(TapsT<I>& T, const TopoView& t, const LeafNbhd& L, float x, float y, float z) {
     const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
     T.tx = x - (float)i;
     T.ty = y - (float)j;
@@ -139,22 +144,23 @@ __device__ __forceinline__ void taps_at(Taps& T, const TopoView& t, const LeafNb
         for (int q = 0; q < 8; ++q) {
             const int A = q >> 2, B = (q >> 1) & 1, C = q & 1;
             const int l = L.nb[na[A] + nb[B] + nc[C]];
-            T.s[q] = l < 0 ? -1 : ((int64_t)l << 9) + (la[A] | lb[B] | lc[C]);
+            T.s[q] = l < 0 ? I(-1) : (I(l) << 9) + I(la[A] | lb[B] | lc[C]);
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) T.s[q] = slot_of(t, L, i + (q >> 2), j + ((q >> 1) & 1), k + (q & 1));
+        for (int q = 0; q < 8; ++q) T.s[q] = (I)slot_of(t, L, i + (q >> 2), j + ((q >> 1) & 1), k + (q & 1));
     }
 }
 
 // Slots of the six face neighbours of local voxel n of the CTA's leaf (slot s), -1 outside the
 // domain, in the order x-1, x+1, y-1, y+1, z-1, z+1: the leaf's own slots unless the
 // neighbour is across a face, then the face neighbour from the staged neighbourhood.
-__device__ __forceinline__ void face_slots(const LeafNbhd& L, int64_t s, int n, int64_t ns[6]) {
+template <typename I>
+__device__ __forceinline__ void face_slots(const LeafNbhd& L, I s, int n, I ns[6]) {
     const int a = n >> 6, b = (n >> 3) & 7, c = n & 7;
-    auto across = [&](int idx, int local) -> int64_t {
+    auto across = [&](int idx, int local) -> I {
         const int l = L.nb[idx];
-        return l < 0 ? -1 : ((int64_t)l << 9) + local;
+        return l < 0 ? I(-1) : (I(l) << 9) + I(local);
     };
     ns[0] = a > 0 ? s - 64 : across(4, n | (7 << 6));
     ns[1] = a < 7 ? s + 64 : across(22, n & 63);
@@ -171,7 +177,8 @@ __device__ __forceinline__ float3 tap_v(const float* __restrict__ d, int64_t s) 
 }
 
 // Lerp along z, then y, then x of the staged corners (TrilinearSampler::sample order).
-__device__ __forceinline__ float tri_lerp(const Taps& T, const float v[8]) {
+template <typename I>
+__device__ __forceinline__ float tri_lerp(const TapsT<I>& T, const float v[8]) {
     const float z0 = lerp1(v[0], v[1], T.tz), z1 = lerp1(v[2], v[3], T.tz);
     const float z2 = lerp1(v[4], v[5], T.tz), z3 = lerp1(v[6], v[7], T.tz);
     return lerp1(lerp1(z0, z1, T.ty), lerp1(z2, z3, T.ty), T.tx);

@@ -98,6 +98,11 @@ def test_mixed_step_against_fp64_oracle(dev, oracle, shell):
         expect[:, ax] = expect[:, ax] - ((pp - pm) * hh).astype(np.float32)
     expect_bf16 = torch.from_numpy(expect).to(torch.bfloat16)
     assert torch.equal(vo.cpu().view(-1, 3), expect_bf16)
+    # The scalar advection to the bit: the oracle's FP32 MacCormack step of the FP16 density
+    # along the BF16 velocity, rounded to FP16.
+    d_in = dh.float().cpu().numpy()
+    expect_d = torch.from_numpy(t.advect_scalar(v_in, d_in, 0.1, 10.0)).to(torch.float16)
+    assert torch.equal(do.cpu(), expect_d)
     # Field error against the FP64 oracle (same BF16/FP16 inputs, FP64 advection, FP64 solve
     # to a residual far below 1e-5).
     v64 = v_in.astype(np.float64)
