@@ -346,13 +346,12 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
 
 // r = b - L p (FP64 arithmetic, r stored FP32) with b = div dx^2 and p = 0 outside the domain,
 // plus sum r^2 and sum b^2 into acc, over half z-rows, with the Laplacian summed in the order
-// +x, -x, +y, -y, +z, -z, -6 p. p null: p = 0 (r = b), and p_zero_out, when set, is cleared.
+// +x, -x, +y, -y, +z, -z, -6 p. p null: p = 0 (r = b).
 // The grid is a few CTAs per SM, each looping over leaf groups and adding its two sums to acc
 // once: the FP64 atomics on the two sums serialise in one L2 slice, and one per leaf pair cost
 // more than a tenth of the kernel.
 __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, const float* __restrict__ div,
                                                                     const double* __restrict__ p,
-                                                                    double* __restrict__ p_zero_out,
                                                                     float* __restrict__ r, double h2,
                                                                     const double* __restrict__ check, double tol2,
                                                                     double* __restrict__ acc) {
@@ -388,11 +387,6 @@ __global__ void __launch_bounds__(kThreads) refine_residual_kernel(TopoView t, c
         } else {
 #pragma unroll
             for (int z = 0; z < 4; ++z) res[z] = (double)dv[z] * h2;
-            if (p_zero_out != nullptr) {
-                double2* pz = reinterpret_cast<double2*>(p_zero_out + w.own);
-                pz[0] = make_double2(0.0, 0.0);
-                pz[1] = make_double2(0.0, 0.0);
-            }
         }
         *reinterpret_cast<float4*>(r + w.own) = make_float4((float)res[0], (float)res[1], (float)res[2], (float)res[3]);
 #pragma unroll
@@ -441,15 +435,25 @@ __global__ void __launch_bounds__(kThreads) refine_scale_kernel(const float* __r
         sstore(rhat, inner_slot<kLayout>(q), __ldg(r + q) * inv);
 }
 
-// p += s e (FP64), pointwise; e in the inner solve's layout kLayout.
+// p += s e (FP64), pointwise; e in the inner solve's layout kLayout. first: the first outer
+// iteration, where p = 0 before it: p = 0 + s e without reading p (and p = 0 if the solve had
+// converged before any correction), so that p needs no clearing pass.
 template <typename TI, int kLayout>
 __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restrict__ p, const TI* __restrict__ e,
                                                                   int64_t n, const float* __restrict__ scale,
-                                                                  const double* __restrict__ check, double tol2) {
-    if (converged(check, tol2)) return;
+                                                                  const double* __restrict__ check, double tol2,
+                                                                  bool first) {
+    const int64_t q0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, dq = (int64_t)gridDim.x * blockDim.x;
+    if (converged(check, tol2)) {
+        if (first)
+            for (int64_t q = q0; q < n; q += dq) p[q] = 0.0;
+        return;
+    }
     const double sc = (double)*scale;
-    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
-        p[q] += sc * (double)sload(e, inner_slot<kLayout>(q));
+    if (first)
+        for (int64_t q = q0; q < n; q += dq) p[q] = 0.0 + sc * (double)sload(e, inner_slot<kLayout>(q));
+    else
+        for (int64_t q = q0; q < n; q += dq) p[q] += sc * (double)sload(e, inner_slot<kLayout>(q));
 }
 
 unsigned row_blocks(const Context& c) { return (unsigned)((c.topo.num_leaves + kRowLeaves - 1) / kRowLeaves); }
@@ -587,8 +591,9 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         faces[1] = c.scratch_f32("refine_faces1", leaves * kPackedFaceBytes / 4);
         halo = c.scratch_f32("refine_rhs_halo", leaves * kPackedHaloBytes / 4);
     }
-    refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, p, r, h2,
-                                                                                   nullptr, tol2, plan.slots);
+    // r = b; p is written by the first update (refine_update_kernel with first set).
+    refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, r, h2, nullptr,
+                                                                         tol2, plan.slots);
     HNS_LAUNCHED();
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
@@ -601,10 +606,11 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
             c.phase_begin(HNS_PHASE_INNER);
             mg_vcycle(c, rm, em, chk, tol2);
             c.phase_end();
-            refine_update_kernel<float, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, em, n, scales + k, chk, tol2);
+            refine_update_kernel<float, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, em, n, scales + k, chk, tol2,
+                                                                                       k == 0);
             HNS_LAUNCHED();
             refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(
-                c.topo.view, div, p, nullptr, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
+                c.topo.view, div, p, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
             HNS_LAUNCHED();
             continue;
         }
@@ -639,14 +645,14 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         }
         c.phase_end();
         if (layout == HNS_INNER_PACKED)
-            refine_update_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+            refine_update_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         else if (layout == HNS_INNER_SPLIT)
-            refine_update_kernel<TI, HNS_INNER_SPLIT><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+            refine_update_kernel<TI, HNS_INNER_SPLIT><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         else
-            refine_update_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2);
+            refine_update_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         HNS_LAUNCHED();
         refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(
-            c.topo.view, div, p, nullptr, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
+            c.topo.view, div, p, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
         HNS_LAUNCHED();
     }
     return plan;
