@@ -196,6 +196,11 @@ double* Context::reduce_slots(int count) {
     return d_reduce.as<double>();
 }
 
+int Context::sm_count() const {
+    if (sms == 0) HNS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    return sms;
+}
+
 void Context::ensure_aux() {
     if (aux_stream == nullptr) HNS_CUDA(cudaStreamCreateWithFlags(&aux_stream, cudaStreamNonBlocking));
     if (aux_ready == nullptr) HNS_CUDA(cudaEventCreateWithFlags(&aux_ready, cudaEventDisableTiming));
@@ -371,6 +376,8 @@ HNS_API hns_status hns_destroy(hns_ctx* ctx) {
             (void)cudaStreamDestroy(c.aux_stream);
         }
         if (c.aux_ready) (void)cudaEventDestroy(c.aux_ready);
+        if (c.refine_echo_done) (void)cudaEventDestroy(c.refine_echo_done);
+        if (c.refine_echo) (void)cudaFreeHost(c.refine_echo);
         c.release_staging();
         for (auto& e : c.phase_events) {
             (void)cudaEventDestroy(e.start);

@@ -173,6 +173,20 @@ struct Context {
     Field* find_field(const std::string& name);
     Field& ensure_field(const std::string& name, int components, bool zero);
 
+    // Forecast of the refinement's outer iterations (hns_mixed.cu): each refined solve copies its
+    // residual checks to pinned memory behind an event; a later solve whose event has completed
+    // reads the count of outer iterations it needed. Outer iterations past the forecast launch
+    // their kernels on short grids, so that when they return at once they cost little.
+    double* refine_echo = nullptr;  // pinned, kEchoSlots doubles
+    cudaEvent_t refine_echo_done = nullptr;
+    bool refine_echo_pending = false;
+    int refine_echo_outer = 0;      // max_outer of the solve in refine_echo
+    double refine_echo_tol = 0.0;   // its tolerance
+    int refine_forecast = 0;        // outer iterations the last read-back solve needed; 0: unknown
+    static constexpr int kEchoSlots = 2 * (64 + 1);
+    mutable int sms = 0;
+    int sm_count() const;  // multiprocessors of the device (queried once)
+
     int64_t num_voxels() const { return topo.num_leaves * 512; }
     float* scratch_f32(const std::string& name, size_t count);
     double* reduce_slots(int count);
@@ -244,8 +258,10 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
 // launch, so the preceding kernel on the stream must be a half-sweep, and rhs, nb8 and check
 // must have been written by kernels that finished before that one started.
 void launch_split_face_table(const Context& c, int* nb8);
+// short_grid: one wave of CTAs looping over the leaves, for a launch expected to find the
+// refinement converged and return at once.
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
-                            float omega, const double* check, double tol2);
+                            float omega, const double* check, double tol2, bool short_grid = false);
 void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
                              void* e_out, void* faces_out, float omega, const double* check, double tol2);
 

@@ -465,9 +465,47 @@ unsigned row_blocks(const Context& c) { return (unsigned)((c.topo.num_leaves + k
 // 12 per SM 1.18, 4 per SM 1.15 ms.
 constexpr int kResidualCtasPerSm = 4;
 unsigned residual_blocks(const Context& c) {
-    int sms = 0;
-    HNS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
-    return std::max(1u, std::min(row_blocks(c), (unsigned)(sms * kResidualCtasPerSm)));
+    return std::max(1u, std::min(row_blocks(c), (unsigned)(c.sm_count() * kResidualCtasPerSm)));
+}
+
+// Outer iterations the most recent refined solve whose checks have reached the host needed
+// (0: unknown), read without waiting: the solve's checks were copied to pinned memory behind
+// an event, which is only queried.
+int refine_forecast(Context& c) {
+    if (!c.refine_echo_pending) return c.refine_forecast;
+    const cudaError_t q = cudaEventQuery(c.refine_echo_done);
+    if (q == cudaErrorNotReady) return c.refine_forecast;
+    HNS_CUDA(q);
+    c.refine_echo_pending = false;
+    c.refine_forecast = 0;
+    const double t2 = c.refine_echo_tol * c.refine_echo_tol;
+    for (int k = 1; k <= c.refine_echo_outer; ++k)
+        if (c.refine_echo[2 * k] <= t2 * c.refine_echo[2 * k + 1]) {
+            c.refine_forecast = k;
+            break;
+        }
+    return c.refine_forecast;
+}
+
+// Copies the solve's checks to pinned memory behind an event, for the forecast of later solves.
+void refine_echo(Context& c, const RefinePlan& plan) {
+    if (2 * (plan.max_outer + 1) > Context::kEchoSlots) return;
+    if (c.refine_echo == nullptr) {
+        HNS_CUDA(cudaMallocHost(&c.refine_echo, sizeof(double) * Context::kEchoSlots));
+        HNS_CUDA(cudaEventCreateWithFlags(&c.refine_echo_done, cudaEventDisableTiming));
+    }
+    HNS_CUDA(cudaMemcpyAsync(c.refine_echo, plan.slots, sizeof(double) * 2 * (size_t)(plan.max_outer + 1),
+                             cudaMemcpyDeviceToHost, c.stream));
+    HNS_CUDA(cudaEventRecord(c.refine_echo_done, c.stream));
+    c.refine_echo_pending = true;
+    c.refine_echo_outer = plan.max_outer;
+    c.refine_echo_tol = plan.tol;
+}
+
+bool capturing(const Context& c) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    HNS_CUDA(cudaStreamIsCapturing(c.stream, &st));
+    return st != cudaStreamCaptureStatusNone;
 }
 
 unsigned stream_blocks(const Context& c, int64_t n) {
@@ -596,8 +634,14 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, nullptr, r, h2, nullptr,
                                                                          tol2, plan.slots);
     HNS_LAUNCHED();
+    // Outer iterations past the forecast launch on short grids (one wave, looping): if the
+    // refinement has converged they return at once for the cost of the launch alone.
+    const bool echo = !capturing(c);
+    const int forecast = echo ? refine_forecast(c) : 0;
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
+        const bool spare = forecast > 0 && k >= forecast;
+        const unsigned gk = spare ? std::min(g, (unsigned)(c.sm_count() * 4)) : g;
         if (flags & HNS_SOLVE_MULTIGRID) {
             // One V-cycle on the scaled residual in FP32 (slot order), then p += s e.
             float* rm = c.scratch_f32("mg_rhat", (size_t)n);
@@ -616,11 +660,11 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
             continue;
         }
         if (layout == HNS_INNER_PACKED)
-            refine_scale_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+            refine_scale_kernel<TI, HNS_INNER_PACKED><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         else if (layout == HNS_INNER_SPLIT)
-            refine_scale_kernel<TI, HNS_INNER_SPLIT><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+            refine_scale_kernel<TI, HNS_INNER_SPLIT><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         else
-            refine_scale_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+            refine_scale_kernel<TI, HNS_INNER_ROWS><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         HNS_LAUNCHED();
         if (packed) launch_rhs_halo_pack(c, rhat, halo, chk, tol2);
         const TI* src = nullptr;
@@ -632,8 +676,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                 if (layout == HNS_INNER_SPLIT) {
                     // In place: red, then black.
                     dst = e_split;
-                    launch_rbgs_split_half(c, nb8, rhat, dst, 0, it == 0, omega, chk, tol2);
-                    launch_rbgs_split_half(c, nb8, rhat, dst, 1, false, omega, chk, tol2);
+                    launch_rbgs_split_half(c, nb8, rhat, dst, 0, it == 0, omega, chk, tol2, spare);
+                    launch_rbgs_split_half(c, nb8, rhat, dst, 1, false, omega, chk, tol2, spare);
                 } else if (packed) {
                     launch_rbgs_packed_half(c, rhat, halo, src, src_faces, dst, faces[it & 1], omega, chk, tol2);
                     src_faces = faces[it & 1];
@@ -646,16 +690,17 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         }
         c.phase_end();
         if (layout == HNS_INNER_PACKED)
-            refine_update_kernel<TI, HNS_INNER_PACKED><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
+            refine_update_kernel<TI, HNS_INNER_PACKED><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         else if (layout == HNS_INNER_SPLIT)
-            refine_update_kernel<TI, HNS_INNER_SPLIT><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
+            refine_update_kernel<TI, HNS_INNER_SPLIT><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         else
-            refine_update_kernel<TI, HNS_INNER_ROWS><<<g, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
+            refine_update_kernel<TI, HNS_INNER_ROWS><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         HNS_LAUNCHED();
         refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(
             c.topo.view, div, p, r, h2, chk, tol2, plan.slots + 2 * (k + 1));
         HNS_LAUNCHED();
     }
+    if (echo) refine_echo(c, plan);
     return plan;
 }
 

@@ -27,6 +27,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "hns_internal.cuh"
@@ -43,6 +44,7 @@ using namespace relax16;
 constexpr int kLeavesPerBlock = 2;   // leaves whose rows one block's threads cover
 constexpr int kLeavesPerThread = 4;  // leaves a thread relaxes its row in
 constexpr int kThreads = 64 * kLeavesPerBlock;
+constexpr int kShortGridCtasPerSm = 6;  // the register limit at 80 registers and 128 threads
 
 // nbr27 indices of the six face neighbours: (dx+1)*9 + (dy+1)*3 + (dz+1).
 constexpr int kNbXp = 22, kNbXm = 4, kNbYp = 16, kNbYm = 10, kNbZp = 14, kNbZm = 12;
@@ -104,7 +106,7 @@ __device__ __forceinline__ uint2 relax_row(uint2 XP, uint2 XM, uint2 YP, uint2 Y
 // unconditional: a row on a leaf face reads the neighbour leaf's row, a missing neighbour the
 // zero leaf. Offsets are 32-bit element counts (fewer than 2^22 leaves).
 template <bool kZero>
-__global__ void __launch_bounds__(kThreads) rbgs_split_half_kernel(const int* __restrict__ nb8,
+__global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half_kernel(const int* __restrict__ nb8,
                                                                     const __half* __restrict__ rhs, __half* e,
                                                                     int num_leaves, int colour, float omega,
                                                                     const double* __restrict__ check, double tol2,
@@ -118,8 +120,13 @@ __global__ void __launch_bounds__(kThreads) rbgs_split_half_kernel(const int* __
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
     const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
     const int p = (w + colour) & 1;  // z parity of this colour in the warp's rows
-    const int leaf0 = (int)blockIdx.x * (kLeavesPerBlock * kLeavesPerThread) + (int)(threadIdx.x >> 6);
     const uint32_t rowc = ((uint32_t)colour << 8) | (uint32_t)(4 * (32 * w + lane));  // own entries within a leaf
+    // Leaf groups (the leaves of one CTA pass): one per CTA in a full grid; a short grid loops.
+    // Within a launch a thread reads and writes only its own rows of the launch's colour and
+    // only reads the other colour, so the passes of a CTA are independent.
+    const int groups = (num_leaves + kLeavesPerBlock * kLeavesPerThread - 1) / (kLeavesPerBlock * kLeavesPerThread);
+    for (int g = blockIdx.x; g < groups; g += gridDim.x) {
+    const int leaf0 = g * (kLeavesPerBlock * kLeavesPerThread) + (int)(threadIdx.x >> 6);
     uint32_t own[kLeavesPerThread];
     bool live[kLeavesPerThread];
 #pragma unroll
@@ -182,6 +189,7 @@ __global__ void __launch_bounds__(kThreads) rbgs_split_half_kernel(const int* __
 #pragma unroll
     for (int k = 0; k < kLeavesPerThread; ++k)
         if (live[k]) *reinterpret_cast<uint2*>(e + own[k]) = out[k];
+    }
 }
 
 }  // namespace
@@ -194,12 +202,15 @@ void launch_split_face_table(const Context& c, int* nb8) {
 }
 
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
-                            float omega, const double* check, double tol2) {
+                            float omega, const double* check, double tol2, bool short_grid) {
     const int64_t L = c.topo.num_leaves;
     if (L == 0) return;
     if (L >= (int64_t(1) << 22)) fail(HNS_ERR_INVALID_ARG, "too many leaves for the colour-split inner solve");
     const int per_block = kLeavesPerBlock * kLeavesPerThread;
-    const unsigned blocks = (unsigned)((L + per_block - 1) / per_block);
+    unsigned blocks = (unsigned)((L + per_block - 1) / per_block);
+    // A launch that will most likely return at once (the refinement expected to have converged)
+    // uses one wave of CTAs: its cost is then the launch, not the scheduling of every CTA.
+    if (short_grid) blocks = std::min(blocks, (unsigned)(c.sm_count() * kShortGridCtasPerSm));
     const auto* r = static_cast<const __half*>(rhs);
     auto* x = static_cast<__half*>(e);
     if (e_zero) {

@@ -189,6 +189,41 @@ def test_inner_solve_layouts_bit_exact(dev, shell, grid):
         assert b[4] <= 1e-5
 
 
+def test_outer_forecast_short_grids_bit_exact(dev, shell):
+    """A context forecasts the refinement's outer iterations from the checks of its earlier
+    solves; the outer iterations past the forecast run their kernels on short grids (one wave,
+    looping over the leaves). Whether those iterations find the solve converged (a forecast at
+    or above the need) or still have work (a forecast below it), the step is the same to the bit
+    as on a fresh context, which has no forecast."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+
+    def solve(g, tol):
+        vb, dh, vo, do, info = _mixed(g, dev, dens, vel, tol=tol, inner=30, outer=12)
+        p = torch.empty(g.num_voxels, dtype=torch.float64, device=dev)
+        outer, res = g.refine_pressure(p)
+        torch.cuda.synchronize()
+        return vo.cpu(), do.cpu(), p.cpu(), outer, res
+
+    fresh = hl.Grid(origins, voxel_size=0.1)
+    ref = solve(fresh, 1e-6)
+    fresh.close()
+    assert ref[4] <= 1e-6
+
+    g = hl.Grid(origins, voxel_size=0.1)
+    loose = solve(g, 1e-3)  # forecast: the few outer iterations of a loose tolerance
+    assert loose[3] < ref[3]
+    under = solve(g, 1e-6)  # iterations past that forecast still have work on short grids
+    over = solve(g, 1e-6)   # forecast = the need: the iterations past it return at once
+    g.close()
+    for got in (under, over):
+        assert got[3] == ref[3]
+        assert got[4] == pytest.approx(ref[4], rel=1e-12)  # FP64 atomics: summation order varies
+        assert torch.equal(got[2], ref[2])
+        assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[1])
+
+
 @pytest.mark.parametrize("grid", ["spheres", "box"])
 def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
     """HNS_SOLVE_MULTIGRID: one V-cycle per outer step in place of the red-black iterations. The
