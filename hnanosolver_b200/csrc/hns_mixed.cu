@@ -436,6 +436,31 @@ __global__ void __launch_bounds__(kThreads) refine_scale_kernel(const float* __r
         sstore(rhat, inner_slot<kLayout>(q), __ldg(r + q) * inv);
 }
 
+// The same for FP16 r^ in the colour-split layout, four slots (half a z-row, z = 4h .. 4h + 3)
+// per thread: one 16-byte load and two 4-byte stores, z = 4h and 4h + 2 to entries 2h and 2h + 1
+// of the row in one colour, z = 4h + 1 and 4h + 3 to the same entries in the other. The values
+// are refine_scale_kernel's to the bit (FP32 product, one FP16 rounding).
+__global__ void __launch_bounds__(kThreads) refine_scale_split_kernel(const float* __restrict__ r,
+                                                                       __half* __restrict__ rhat, int64_t n,
+                                                                       const double* __restrict__ check, double tol2,
+                                                                       float* __restrict__ scale) {
+    if (converged(check, tol2)) return;
+    const double rms = sqrt(check[0] / (double)n);
+    const float sc = rms > 0.0 ? (float)rms : 1.0f;
+    const float inv = 1.0f / sc;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *scale = sc;
+    auto h16 = [](float v) { return (uint32_t)__half_as_ushort(__float2half_rn(v)); };
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < (n >> 2); u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = u << 2;
+        const float4 v = __ldg(reinterpret_cast<const float4*>(r + q));
+        const int loc = (int)(q & 511), a = loc >> 6, b = (loc >> 3) & 7, h = (loc >> 2) & 1;
+        const int p0 = (a + b) & 1;
+        const int64_t base = (q & ~int64_t(511)) + 4 * (32 * p0 + 4 * a + (b >> 1)) + 2 * h;
+        *reinterpret_cast<uint32_t*>(rhat + base + ((int64_t)p0 << 8)) = h16(v.x * inv) | (h16(v.z * inv) << 16);
+        *reinterpret_cast<uint32_t*>(rhat + base + ((int64_t)(p0 ^ 1) << 8)) = h16(v.y * inv) | (h16(v.w * inv) << 16);
+    }
+}
+
 // p += s e (FP64), pointwise; e in the inner solve's layout kLayout. first: the first outer
 // iteration, where p = 0 before it: p = 0 + s e without reading p (and p = 0 if the solve had
 // converged before any correction), so that p needs no clearing pass.
@@ -456,6 +481,47 @@ __global__ void __launch_bounds__(kThreads) refine_update_kernel(double* __restr
     else
         for (int64_t q = q0; q < n; q += dq) p[q] += sc * (double)sload(e, inner_slot<kLayout>(q));
 }
+
+// The same update from FP16 e in the colour-split layout, four slots per thread (as
+// refine_scale_split_kernel): two 4-byte loads of e and 16-byte accesses to p; the values are
+// refine_update_kernel's to the bit.
+__global__ void __launch_bounds__(kThreads) refine_update_split_kernel(double* __restrict__ p, const __half* __restrict__ e,
+                                                                        int64_t n, const float* __restrict__ scale,
+                                                                        const double* __restrict__ check, double tol2,
+                                                                        bool first) {
+    const int64_t u0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, du = (int64_t)gridDim.x * blockDim.x;
+    if (converged(check, tol2)) {
+        if (first)
+            for (int64_t u = u0; u < (n >> 2); u += du) {
+                double2* pp = reinterpret_cast<double2*>(p + (u << 2));
+                pp[0] = make_double2(0.0, 0.0);
+                pp[1] = make_double2(0.0, 0.0);
+            }
+        return;
+    }
+    const double sc = (double)*scale;
+    auto f = [](uint32_t bits) { return (double)__half2float(__ushort_as_half((unsigned short)bits)); };
+    for (int64_t u = u0; u < (n >> 2); u += du) {
+        const int64_t q = u << 2;
+        const int loc = (int)(q & 511), a = loc >> 6, b = (loc >> 3) & 7, h = (loc >> 2) & 1;
+        const int p0 = (a + b) & 1;
+        const int64_t base = (q & ~int64_t(511)) + 4 * (32 * p0 + 4 * a + (b >> 1)) + 2 * h;
+        const uint32_t w0 = __ldg(reinterpret_cast<const unsigned int*>(e + base + ((int64_t)p0 << 8)));
+        const uint32_t w1 = __ldg(reinterpret_cast<const unsigned int*>(e + base + ((int64_t)(p0 ^ 1) << 8)));
+        const double d0 = sc * f(w0 & 0xFFFFu), d1 = sc * f(w1 & 0xFFFFu), d2 = sc * f(w0 >> 16), d3 = sc * f(w1 >> 16);
+        double2* pp = reinterpret_cast<double2*>(p + q);
+        if (first) {
+            pp[0] = make_double2(0.0 + d0, 0.0 + d1);
+            pp[1] = make_double2(0.0 + d2, 0.0 + d3);
+        } else {
+            double2 x = pp[0], y = pp[1];
+            x.x += d0, x.y += d1, y.x += d2, y.y += d3;
+            pp[0] = x;
+            pp[1] = y;
+        }
+    }
+}
+
 
 unsigned row_blocks(const Context& c) { return (unsigned)((c.topo.num_leaves + kRowLeaves - 1) / kRowLeaves); }
 
@@ -661,9 +727,13 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         }
         if (layout == HNS_INNER_PACKED)
             refine_scale_kernel<TI, HNS_INNER_PACKED><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
-        else if (layout == HNS_INNER_SPLIT)
-            refine_scale_kernel<TI, HNS_INNER_SPLIT><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
-        else
+        else if (layout == HNS_INNER_SPLIT) {
+            if constexpr (sizeof(TI) == 2)
+                refine_scale_split_kernel<<<gk, kThreads, 0, c.stream>>>(r, reinterpret_cast<__half*>(rhat), n, chk, tol2,
+                                                                         scales + k);
+            else
+                refine_scale_kernel<TI, HNS_INNER_SPLIT><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
+        } else
             refine_scale_kernel<TI, HNS_INNER_ROWS><<<gk, kThreads, 0, c.stream>>>(r, rhat, n, chk, tol2, scales + k);
         HNS_LAUNCHED();
         if (packed) launch_rhs_halo_pack(c, rhat, halo, chk, tol2);
@@ -691,9 +761,14 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         c.phase_end();
         if (layout == HNS_INNER_PACKED)
             refine_update_kernel<TI, HNS_INNER_PACKED><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
-        else if (layout == HNS_INNER_SPLIT)
-            refine_update_kernel<TI, HNS_INNER_SPLIT><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
-        else
+        else if (layout == HNS_INNER_SPLIT) {
+            if constexpr (sizeof(TI) == 2)
+                refine_update_split_kernel<<<gk, kThreads, 0, c.stream>>>(p, reinterpret_cast<const __half*>(src), n,
+                                                                          scales + k, chk, tol2, k == 0);
+            else
+                refine_update_kernel<TI, HNS_INNER_SPLIT><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2,
+                                                                                          k == 0);
+        } else
             refine_update_kernel<TI, HNS_INNER_ROWS><<<gk, kThreads, 0, c.stream>>>(p, src, n, scales + k, chk, tol2, k == 0);
         HNS_LAUNCHED();
         refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(
