@@ -184,6 +184,8 @@ struct Context {
     double refine_echo_tol = 0.0;   // its tolerance
     int refine_forecast = 0;        // outer iterations the last read-back solve needed; 0: unknown
     static constexpr int kEchoSlots = 2 * (64 + 1);
+    // The colour-split inner solve's e and face-table buffers whose zero leaf and table are made.
+    const void* split_setup[2] = {nullptr, nullptr};
     mutable int sms = 0;
     int sm_count() const;  // multiprocessors of the device (queried once)
 

@@ -684,8 +684,13 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     if (layout == HNS_INNER_SPLIT) {
         e_split = reinterpret_cast<TI*>(c.scratch_f32("refine_e_split", ((size_t)(n + 512) * sizeof(TI) + 3) / 4));
         nb8 = reinterpret_cast<int*>(c.scratch_f32("refine_split_nb8", (size_t)c.topo.num_leaves * 8));
-        HNS_CUDA(cudaMemsetAsync(e_split + n, 0, 512 * sizeof(TI), c.stream));
-        launch_split_face_table(c, nb8);
+        // The zero leaf and the face table depend on the topology alone: made once per buffer.
+        if (c.split_setup[0] != e_split || c.split_setup[1] != nb8) {
+            HNS_CUDA(cudaMemsetAsync(e_split + n, 0, 512 * sizeof(TI), c.stream));
+            launch_split_face_table(c, nb8);
+            c.split_setup[0] = e_split;
+            c.split_setup[1] = nb8;
+        }
     }
     // Packed: the face buffers of e[0] and e[1] and the rhs halo records.
     void* faces[2] = {nullptr, nullptr};
