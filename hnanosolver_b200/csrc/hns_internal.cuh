@@ -289,7 +289,7 @@ template <typename TI>
 RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol,
                         unsigned flags = 0);
 void refine_result(Context& c, const RefinePlan& plan, int* outer, double* residual);
-void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
+void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
                          float dt);
 void launch_divergence_mixed(const Context& c, const void* vel, float* div);
 void launch_gradient_mixed(const Context& c, void* vel, const double* p);

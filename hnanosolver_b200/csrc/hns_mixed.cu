@@ -801,8 +801,138 @@ void refine_result(Context& c, const RefinePlan& plan, int* outer, double* resid
     }
 }
 
-void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
+namespace {
+
+// Voxel records for the mixed advection: a voxel's BF16 velocity and its first FP16 scalar as
+// one 8-byte record (u | v << 16, w | s << 16), so that each of the 2 x 8 trace taps and 6 clamp
+// neighbours is one load instead of four. Four voxels per thread: three 8-byte loads of
+// velocity, one of the scalar, two 16-byte stores.
+__global__ void __launch_bounds__(kThreads) pack_records_kernel(const __nv_bfloat16* __restrict__ vel,
+                                                                 const __half* __restrict__ s0, uint4* __restrict__ rec,
+                                                                 int64_t n) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < (n >> 2); u += (int64_t)gridDim.x * blockDim.x) {
+        const uint2* pv = reinterpret_cast<const uint2*>(vel + 12 * u);
+        const uint2 a = __ldg(pv), b = __ldg(pv + 1), c = __ldg(pv + 2);
+        const uint2 d = s0 != nullptr ? __ldg(reinterpret_cast<const uint2*>(s0 + 4 * u)) : make_uint2(0u, 0u);
+        rec[2 * u] = make_uint4(a.x, (a.y & 0xFFFFu) | (d.x << 16), (a.y >> 16) | (b.x << 16), (b.x >> 16) | (d.x & 0xFFFF0000u));
+        rec[2 * u + 1] = make_uint4(b.y, (c.x & 0xFFFFu) | (d.y << 16), (c.x >> 16) | (c.y << 16), (c.y >> 16) | (d.y & 0xFFFF0000u));
+    }
+}
+
+// The record at slot s (-1: outside the domain, all zero), as FP32 velocity and scalar.
+struct Rec {
+    float u, v, w, d;
+};
+__device__ __forceinline__ Rec rec_at(const uint2* __restrict__ rec, int32_t s) {
+    if (s < 0) return Rec{0.f, 0.f, 0.f, 0.f};
+    const uint2 r = __ldg(rec + (uint32_t)s);
+    return Rec{__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xFFFF0000u), __uint_as_float(r.y << 16),
+               __half2float(__ushort_as_half((unsigned short)(r.y >> 16)))};
+}
+
+// advect_mixed_kernel on voxel records: the same trace, taps, lerps and clamps in the same
+// order, so the same bits; the velocity and the first scalar come from the records, further
+// scalars (f) from their own arrays. 32-bit slots (fewer than 2^22 leaves).
+__global__ void __launch_bounds__(kThreads, 4) advect_records_kernel(TopoView t, const uint2* __restrict__ rec,
+                                                                      __nv_bfloat16* __restrict__ vel_out,
+                                                                      __half* __restrict__ s0_out, FieldSetT<__half> f,
+                                                                      float sdt) {
+    __shared__ LeafNbhd L;
+    const VoxelIdx v = voxel_of_block();
+    load_nbhd(L, t, v.leaf);
+    __syncthreads();
+    const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
+    const int32_t s = (int32_t(v.leaf) << 9) + int32_t(v.n);
+    const Rec o = rec_at(rec, s);
+    const float bx = (float)i - o.u * sdt, by = (float)j - o.v * sdt, bz = (float)k - o.w * sdt;
+    TapsT<int32_t> tb, tf;
+    taps_at(tb, t, L, bx, by, bz);
+    float x[8], y[8], z[8], d[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const Rec a = rec_at(rec, tb.s[q]);
+        x[q] = a.u, y[q] = a.v, z[q] = a.w, d[q] = a.d;
+    }
+    const float3 vf = make_float3(tri_lerp(tb, x), tri_lerp(tb, y), tri_lerp(tb, z));
+    const float pf = tri_lerp(tb, d);
+    taps_at(tf, t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const Rec a = rec_at(rec, tf.s[q]);
+        x[q] = a.u, y[q] = a.v, z[q] = a.w, d[q] = a.d;
+    }
+    const float3 vb = make_float3(tri_lerp(tf, x), tri_lerp(tf, y), tri_lerp(tf, z));
+    const float pb = tri_lerp(tf, d);
+    int32_t ns[6];
+    face_slots(L, s, v.n, ns);
+    float3 corr = make_float3(vf.x + 0.5f * (o.u - vb.x), vf.y + 0.5f * (o.v - vb.y), vf.z + 0.5f * (o.w - vb.z));
+    float3 mn = make_float3(o.u, o.v, o.w), mx = mn;
+    float dmn = o.d, dmx = o.d;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const Rec a = rec_at(rec, ns[q]);
+        mn.x = fminf(mn.x, a.u), mn.y = fminf(mn.y, a.v), mn.z = fminf(mn.z, a.w);
+        mx.x = fmaxf(mx.x, a.u), mx.y = fmaxf(mx.y, a.v), mx.z = fmaxf(mx.z, a.w);
+        dmn = fminf(dmn, a.d);
+        dmx = fmaxf(dmx, a.d);
+    }
+    mn.x = fminf(mn.x, vf.x), mn.y = fminf(mn.y, vf.y), mn.z = fminf(mn.z, vf.z);
+    mx.x = fmaxf(mx.x, vf.x), mx.y = fmaxf(mx.y, vf.y), mx.z = fmaxf(mx.z, vf.z);
+    corr.x = fmaxf(mn.x, fminf(corr.x, mx.x));
+    corr.y = fmaxf(mn.y, fminf(corr.y, mx.y));
+    corr.z = fmaxf(mn.z, fminf(corr.z, mx.z));
+    vstore(vel_out, wide(s), corr);
+    if (s0_out != nullptr) {
+        const float dcorr = pf + 0.5f * (o.d - pb);
+        dmn = fminf(dmn, pf);
+        dmx = fmaxf(dmx, pf);
+        sstore(s0_out, wide(s), fmaxf(dmn, fminf(dcorr, dmx)));
+    }
+    for (int c = 0; c < f.count; ++c) {
+        const __half* __restrict__ dd = f.in[c];
+        const float po = sload(dd, wide(s));
+        const float qf = tri1(tb, dd);
+        const float qb = tri1(tf, dd);
+        const float cc = qf + 0.5f * (po - qb);
+        float lo = po, hi = po;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const float a = tap1(dd, ns[q]);
+            lo = fminf(lo, a);
+            hi = fmaxf(hi, a);
+        }
+        lo = fminf(lo, qf);
+        hi = fmaxf(hi, qf);
+        sstore(f.out[c], wide(s), fmaxf(lo, fminf(cc, hi)));
+    }
+}
+
+}  // namespace
+
+void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
                          float dt) {
+    const int64_t n = c.num_voxels();
+    const float sdt = dt * (1.0f / c.dx);
+    auto aligned8 = [](const void* q) { return ((uintptr_t)q & 7u) == 0; };
+    if (n > 0 && c.topo.num_leaves < (int64_t(1) << 22) && aligned8(vel) && (ns == 0 || aligned8(sin[0])) &&
+        ns <= kMaxAdvectFields) {
+        // Voxel records: velocity and the first scalar interleaved, then one load per tap.
+        auto* rec = reinterpret_cast<uint4*>(c.scratch_f32("advect_records", (size_t)n * 2));
+        pack_records_kernel<<<stream_blocks(c, n), kThreads, 0, c.stream>>>(
+            static_cast<const __nv_bfloat16*>(vel), ns > 0 ? static_cast<const __half*>(sin[0]) : nullptr, rec, n);
+        HNS_LAUNCHED();
+        FieldSetT<__half> f{};
+        f.count = std::max(0, ns - 1);
+        for (int q = 0; q < f.count; ++q) {
+            f.in[q] = static_cast<const __half*>(sin[1 + q]);
+            f.out[q] = static_cast<__half*>(sout[1 + q]);
+        }
+        advect_records_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+            c.topo.view, reinterpret_cast<const uint2*>(rec), static_cast<__nv_bfloat16*>(vel_out),
+            ns > 0 ? static_cast<__half*>(sout[0]) : nullptr, f, sdt);
+        HNS_LAUNCHED();
+        return;
+    }
     int base = 0;
     do {
         FieldSetT<__half> f{};
@@ -815,10 +945,10 @@ void launch_advect_mixed(const Context& c, const void* vel, void* vel_out, const
         auto* vo = base == 0 ? static_cast<__nv_bfloat16*>(vel_out) : nullptr;
         if (c.topo.num_leaves < (int64_t(1) << 22))
             advect_mixed_kernel<__nv_bfloat16, __half, int32_t>
-                <<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vi, vo, f, dt * (1.0f / c.dx));
+                <<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vi, vo, f, sdt);
         else
             advect_mixed_kernel<__nv_bfloat16, __half, int64_t>
-                <<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vi, vo, f, dt * (1.0f / c.dx));
+                <<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vi, vo, f, sdt);
         HNS_LAUNCHED();
         base += f.count;
     } while (base < ns);

@@ -118,6 +118,36 @@ def test_mixed_step_against_fp64_oracle(dev, oracle, shell):
     g.close()
 
 
+@pytest.mark.parametrize("nscalars", [0, 3])
+def test_mixed_step_scalar_counts(dev, oracle, shell, nscalars):
+    """The mixed advection reads the velocity and the first scalar as interleaved voxel records
+    and further scalars from their own arrays: with no scalar the projected velocity is the one
+    of the single-scalar step, and with three each advected scalar is the oracle's FP32
+    MacCormack step of its FP16 input along the BF16 velocity, to the bit."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    vb = torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous()
+    rng = np.random.default_rng(3)
+    fields = [dens] + [rng.random(len(dens), dtype=np.float32) for _ in range(2)]
+    hs = [torch.from_numpy(f).to(dev).to(torch.float16).contiguous() for f in fields[:nscalars]]
+    outs = [torch.empty_like(h) for h in hs]
+    vo = torch.empty_like(vb)
+    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=8, inner_iterations=40, flags=0)
+    info = g.step_mixed(vb, vo, hs, outs, desc, info=True)
+    assert info.residual <= 1e-5
+    vb1, dh1, vo1, do1, _ = _mixed(g, dev, dens, vel)
+    torch.cuda.synchronize()
+    assert torch.equal(vo.cpu(), vo1.cpu())
+    t = oracle.topo(origins)
+    v_in = vb.float().cpu().numpy()
+    for h, o in zip(hs, outs):
+        expect = torch.from_numpy(t.advect_scalar(v_in, h.float().cpu().numpy(), 0.1, 10.0)).to(torch.float16)
+        assert torch.equal(o.cpu(), expect)
+    g.close()
+
+
 def test_mixed_host_equals_device(dev, shell):
     from hnanosolver_b200 import lib as hl
 
