@@ -274,6 +274,27 @@ __device__ __forceinline__ void store_vel_half_row(float* v, int64_t s, const fl
     q[2] = make_float4(u[2].z, u[3].x, u[3].y, u[3].z);
 }
 
+// Element-wise forms of the same, for velocity arrays that are not 8-byte (BF16) or 16-byte
+// (FP32) aligned; kVec selects the vector form.
+template <bool kVec, typename V>
+__device__ __forceinline__ void vel_row(const V* __restrict__ v, int64_t s, float3 u[4]) {
+    if constexpr (kVec) {
+        vel_half_row(v, s, u);
+    } else {
+#pragma unroll
+        for (int z = 0; z < 4; ++z) u[z] = vload(v, s + z);
+    }
+}
+template <bool kVec, typename V>
+__device__ __forceinline__ void store_vel_row(V* v, int64_t s, const float3 u[4]) {
+    if constexpr (kVec) {
+        store_vel_half_row(v, s, u);
+    } else {
+#pragma unroll
+        for (int z = 0; z < 4; ++z) vstore(v, s + z, u[z]);
+    }
+}
+
 __device__ __forceinline__ float vel_z(const __nv_bfloat16* __restrict__ v, int64_t s) {
     return __bfloat162float(__ldg(v + 3 * s + 2));
 }
@@ -281,18 +302,18 @@ __device__ __forceinline__ float vel_z(const __nv_bfloat16* __restrict__ v, int6
 // Divergence (divergence, src/Cuda/Kernel.cu:432-453) of a reduced-precision velocity into
 // FP32: per voxel the face velocities are the means of the centre and the neighbour (0 for a
 // missing neighbour), div = (xp - xm + yp - ym + zp - zm) / dx.
-template <typename V>
+template <typename V, bool kVec>
 __global__ void __launch_bounds__(kThreads) divergence_mixed_kernel(TopoView t, const V* __restrict__ vel,
                                                                      float* __restrict__ div, float inv_dx) {
     HalfRow r;
     if (!half_row(t, r, blockIdx.x)) return;
     const NbrRows q = nbr_rows(r);
     float3 c[4], xp[4], xm[4], yp[4], ym[4];
-    vel_half_row(vel, r.own, c);
-    vel_half_row(vel, q.xp, xp);
-    vel_half_row(vel, q.xm, xm);
-    vel_half_row(vel, q.yp, yp);
-    vel_half_row(vel, q.ym, ym);
+    vel_row<kVec>(vel, r.own, c);
+    vel_row<kVec>(vel, q.xp, xp);
+    vel_row<kVec>(vel, q.xm, xm);
+    vel_row<kVec>(vel, q.yp, yp);
+    vel_row<kVec>(vel, q.ym, ym);
     int64_t zin_s, zface_s;
     z_ends(r, zin_s, zface_s);
     const float zin = vel_z(vel, zin_s), zface = zface_s < 0 ? 0.f : vel_z(vel, zface_s);
@@ -314,7 +335,7 @@ __global__ void __launch_bounds__(kThreads) divergence_mixed_kernel(TopoView t, 
 // u -= grad p with p in FP64 (0 outside the domain), central differences
 // (subtractPressureGradient, src/Cuda/Kernel.cu:495-541), velocity in reduced precision or
 // FP32, in place.
-template <typename V>
+template <typename V, bool kVec>
 __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V* __restrict__ vel,
                                                                    const double* __restrict__ p, float inv_dx) {
     HalfRow r;
@@ -331,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
     const double zin = __ldg(p + zin_s), zface = zface_s < 0 ? 0.0 : __ldg(p + zface_s);
     const double zlo = r.h ? zin : zface, zhi = r.h ? zface : zin;
     float3 u[4];
-    vel_half_row(vel, r.own, u);
+    vel_row<kVec>(vel, r.own, u);
     const double hh = 0.5 * (double)inv_dx;
 #pragma unroll
     for (int z = 0; z < 4; ++z) {
@@ -340,7 +361,7 @@ __global__ void __launch_bounds__(kThreads) gradient_mixed_kernel(TopoView t, V*
         const float gz = (float)(((z < 3 ? c[z + 1] : zhi) - (z > 0 ? c[z - 1] : zlo)) * hh);
         u[z] = make_float3(u[z].x - gx, u[z].y - gy, u[z].z - gz);
     }
-    store_vel_half_row(vel, r.own, u);
+    store_vel_row<kVec>(vel, r.own, u);
 }
 
 // ---- refinement --------------------------------------------------------------------------
@@ -956,22 +977,33 @@ void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void*
 
 void launch_divergence_mixed(const Context& c, const void* vel, float* div) {
     if (c.topo.num_leaves == 0) return;
-    divergence_mixed_kernel<__nv_bfloat16><<<row_blocks(c), kThreads, 0, c.stream>>>(
-        c.topo.view, static_cast<const __nv_bfloat16*>(vel), div, 1.0f / c.dx);
+    const auto* v = static_cast<const __nv_bfloat16*>(vel);
+    if (((uintptr_t)vel & 1u) != 0) fail(HNS_ERR_INVALID_ARG, "BF16 velocity must be 2-byte aligned");
+    if (((uintptr_t)vel & 7u) == 0)
+        divergence_mixed_kernel<__nv_bfloat16, true><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, v, div, 1.0f / c.dx);
+    else
+        divergence_mixed_kernel<__nv_bfloat16, false><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, v, div, 1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
 void launch_gradient_mixed(const Context& c, void* vel, const double* p) {
     if (c.topo.num_leaves == 0) return;
-    gradient_mixed_kernel<__nv_bfloat16><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view,
-                                                                                     static_cast<__nv_bfloat16*>(vel), p,
-                                                                                     1.0f / c.dx);
+    auto* v = static_cast<__nv_bfloat16*>(vel);
+    if (((uintptr_t)vel & 1u) != 0) fail(HNS_ERR_INVALID_ARG, "BF16 velocity must be 2-byte aligned");
+    if (((uintptr_t)vel & 7u) == 0)
+        gradient_mixed_kernel<__nv_bfloat16, true><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, v, p, 1.0f / c.dx);
+    else
+        gradient_mixed_kernel<__nv_bfloat16, false><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, v, p, 1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
 void launch_gradient_f64(const Context& c, float* vel, const double* p) {
     if (c.topo.num_leaves == 0) return;
-    gradient_mixed_kernel<float><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, 1.0f / c.dx);
+    if (((uintptr_t)vel & 3u) != 0) fail(HNS_ERR_INVALID_ARG, "FP32 velocity must be 4-byte aligned");
+    if (((uintptr_t)vel & 15u) == 0)
+        gradient_mixed_kernel<float, true><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, 1.0f / c.dx);
+    else
+        gradient_mixed_kernel<float, false><<<row_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, 1.0f / c.dx);
     HNS_LAUNCHED();
 }
 
@@ -1049,9 +1081,14 @@ HNS_API hns_status hns_step_mixed(hns_ctx* ctx, const void* vel_in, void* vel_ou
         Context* c = check_ctx(ctx);
         check_mixed_desc(desc);
         if (!vel_in || !vel_out || vel_in == vel_out) fail(HNS_ERR_INVALID_ARG, "bad velocity arrays");
+        // 16-bit elements need 2-byte alignment; wider alignment only selects vector accesses.
+        auto odd = [](const void* q) { return ((uintptr_t)q & 1u) != 0; };
+        if (odd(vel_in) || odd(vel_out)) fail(HNS_ERR_INVALID_ARG, "BF16 velocity arrays must be 2-byte aligned");
         if (nscalars < 0 || (nscalars > 0 && (!scalars_in || !scalars_out))) fail(HNS_ERR_INVALID_ARG, "bad scalar arrays");
         for (int q = 0; q < nscalars; ++q)
             if (!scalars_in[q] || !scalars_out[q]) fail(HNS_ERR_INVALID_ARG, "null scalar field");
+            else if (odd(scalars_in[q]) || odd(scalars_out[q]))
+                fail(HNS_ERR_INVALID_ARG, "FP16 scalar arrays must be 2-byte aligned");
         DeviceGuard dg(c->device);
         const RefinePlan plan = mixed_step_device(*c, vel_in, vel_out, scalars_in, scalars_out, nscalars, *desc);
         st = mixed_info(*c, plan, *desc, info);

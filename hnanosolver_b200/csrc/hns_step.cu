@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -167,6 +168,8 @@ void set_fields(FieldSet& f, const float* const* in, float* const* out, int base
     f.count = count;
     for (int q = 0; q < count; ++q) {
         if (!in[base + q] || !out[base + q]) fail(HNS_ERR_INVALID_ARG, "null scalar field");
+        if (((uintptr_t)in[base + q] & 3u) != 0 || ((uintptr_t)out[base + q] & 3u) != 0)
+            fail(HNS_ERR_INVALID_ARG, "FP32 scalar arrays must be 4-byte aligned");
         f.in[q] = in[base + q];
         f.out[q] = out[base + q];
     }
@@ -204,6 +207,8 @@ HNS_API hns_status hns_step_plain(hns_ctx* ctx, const float* vel_in, float* vel_
         check_desc(desc);
         if (!vel_in || !vel_out) fail(HNS_ERR_INVALID_ARG, "null velocity");
         if (vel_in == vel_out) fail(HNS_ERR_INVALID_ARG, "vel_in and vel_out must differ");
+        if (((uintptr_t)vel_in & 3u) != 0 || ((uintptr_t)vel_out & 3u) != 0)
+            fail(HNS_ERR_INVALID_ARG, "FP32 velocity arrays must be 4-byte aligned");
         if (nscalars < 0 || (nscalars > 0 && (!scalars_in || !scalars_out))) fail(HNS_ERR_INVALID_ARG, "bad scalar arrays");
         DeviceGuard dg(c->device);
         advect_chain(*c, vel_in, vel_out, scalars_in, scalars_out, nscalars, desc->dt);
