@@ -454,9 +454,10 @@ def ours(args, wl):
             g.step_mixed(vb[s0], vb[1 - s0], [dh[s0]], [dh[1 - s0]], st)
             ms_state[0] = 1 - s0
 
-        # advection, divergence, first residual, gradient; per outer iteration scale, 2 inner
-        # half-sweeps per iteration, update, residual (the face table is made once per context).
-        launches_per_step = 4 + outer * (3 + 2 * wl["inner"])
+        # record packing, advection, divergence, first residual, gradient; per outer iteration
+        # scale, 2 half-sweeps per inner iteration, update, residual (the face table is made once
+        # per context).
+        launches_per_step = 5 + outer * (3 + 2 * wl["inner"])
         # One launch is a half-sweep: half of an iteration's pass-model bytes (read e, read r,
         # write e at 2 bytes each).
         kernel_bytes, kernel_name, phase = 3, "rbgs_split_half_kernel (FP16 inner solve, colour-split, one colour per launch)", "inner"
