@@ -189,7 +189,10 @@ class ClockSampler:
 
 
 def dist_info():
-    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    from hnanosolver_b200 import replicas
+
+    r = replicas.ranks_from_env()
+    return r.rank, r.world, r.local
 
 
 def reference_arm(args, wl):
@@ -359,19 +362,16 @@ def ours(args, wl):
     from hnanosolver_b200 import lib as hl
     from hnanosolver_b200 import synth
 
-    rank, world, local = dist_info()
-    dist = world > 1
-    if dist:
-        import datetime
+    from hnanosolver_b200 import replicas
 
-        import torch.distributed as td
-
-        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    R = replicas.ranks_from_env()
+    rank, world, local = R.rank, R.world, R.local
+    replicas.start(R, "nccl")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
     origins = synth.topology(args.workload)
-    dens, vel = synth.noise_fields(origins, seed=rank)
+    dens, vel = synth.noise_fields(origins, seed=replicas.seed_of(R))
     n = len(dens)
     g = hl.Grid(origins, voxel_size=wl["dx"], device=local)
     stream = torch.cuda.Stream(device=dev)
@@ -471,25 +471,20 @@ def ours(args, wl):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    if dist:
-        td.barrier()
+    replicas.barrier(R)
     clocks = ClockSampler(local)
     clocks.start()
     g.profile_read()
     g.profile_enable(True)
     ms = _timed_steps(torch, stream, step, args.steps)
-    if dist:
-        td.barrier()
+    replicas.barrier(R)
     clk = clocks.stop()
     g.profile_enable(False)
     prof = g.profile_read()
     last = g.last_refine() if mixed else g.last_solve()
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = replicas.max_over_ranks(R, ms, dev)
     ms_step = ms / args.steps
-    value = world * n * args.steps / (ms / 1e3)
+    value = replicas.aggregate_rate(R, n, args.steps, ms)
 
     # Dominant kernel: average duration of its launches inside the timed region (phase
     # events around them / device counter of launches that ran).
@@ -514,10 +509,7 @@ def ours(args, wl):
     for _ in range(e2e_steps):
         run_host()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        td.all_reduce(t, op=td.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(R, e2e_s, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -561,8 +553,7 @@ def ours(args, wl):
         }
         print(json.dumps(line), flush=True)
     g.close()
-    if dist:
-        td.destroy_process_group()
+    replicas.finish(R)
 
 
 def main():
