@@ -360,9 +360,7 @@ def ours(args, wl):
     import torch
 
     from hnanosolver_b200 import lib as hl
-    from hnanosolver_b200 import synth
-
-    from hnanosolver_b200 import replicas
+    from hnanosolver_b200 import replicas, synth
 
     R = replicas.ranks_from_env()
     rank, world, local = R.rank, R.world, R.local
