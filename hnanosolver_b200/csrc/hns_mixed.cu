@@ -595,9 +595,10 @@ bool capturing(const Context& c) {
     return st != cudaStreamCaptureStatusNone;
 }
 
+// Grid of the grid-stride passes: four values per thread, at most 32 CTAs per SM.
 unsigned stream_blocks(const Context& c, int64_t n) {
     const int64_t b = (n + kThreads * 4 - 1) / (kThreads * 4);
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 32));
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)c.sm_count() * 32));
 }
 
 // ---- conversions -------------------------------------------------------------------------
