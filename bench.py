@@ -43,8 +43,10 @@ WORKLOADS = {
                      # omega_refined / inner: the refinement's inner SOR factor and iterations per outer step,
                      # the fastest to 1e-5 in a sweep of 1.85-1.96 x 16-90 (they also serve the FP32 refinement).
                      # omega: plain FP32 SOR, the fastest that reaches 1e-5 (1.84 and above stall near 1.2e-5).
+                     # fp32_iterations: red-black iterations the plain FP32 GPU solve takes to 1e-5 on this grid
+                     # (measured on the B200 with checks every 10); both CPU legs run exactly this count.
                      dx=0.1, dt=0.1, omega=1.82, omega_refined=1.92, inner=36, tolerance=1e-5, cap=3000, check_every=10,
-                     fp32_iterations=620),
+                     fp32_iterations=470),
     "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60",
                      dx=0.1, dt=1.0 / 24.0, omega=1.8, omega_refined=1.9, inner=30, tolerance=1e-5, cap=3000,
                      check_every=10, fp32_iterations=None),
@@ -195,6 +197,16 @@ def dist_info():
     return r.rank, r.world, r.local
 
 
+def workload_config(args, wl, origins):
+    """The workload-defining `config`, printed identically by both arms."""
+    n = 512 * len(origins)
+    return {"workload": args.workload, "description": wl["desc"], "voxels": n, "leaves": len(origins),
+            "dt": wl["dt"], "dx": wl["dx"], "tolerance": wl["tolerance"],
+            "residual": "relative FP64 Poisson residual ||b - L p|| / ||b||, b = div dx^2",
+            "fp32_red_black_iterations": wl["fp32_iterations"],
+            "l2": "inputs larger than L2 (%.0f MB of fields and solver state per GPU)" % (((12 + 4) * 2 + 8 + 16) * n / 1e6)}
+
+
 def reference_arm(args, wl):
     """Reference CPU implementation of the step on a bounded sample (rank 0 only)."""
     rank, world, _ = dist_info()
@@ -208,7 +220,7 @@ def reference_arm(args, wl):
     origins = synth.topology(args.workload)
     dens, vel = synth.noise_fields(origins, seed=0)
     g = ref.grid(synth.leaf_dense_coords(origins))
-    iters = wl["fp32_iterations"] or 200
+    iters = wl["fp32_iterations"]
     n = len(dens)
     blocks = (n + 255) // 256
     stride = max(1, blocks // 2048)
@@ -231,7 +243,9 @@ def reference_arm(args, wl):
         "impl": "reference", "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "voxels": n, "leaves": len(origins), "red_black_iterations": iters},
+        "config": workload_config(args, wl, origins),
+        "details": {"step": "the plain step in FP32 (advect velocity and density, divergence, red-black SOR from p = 0, "
+                            "gradient subtraction)", "red_black_iterations": iters, "omega": wl["omega"]},
         "cpu_baseline": {"value": value, "unit": "voxel-steps/s", "cores": cores, "kind": "reference",
                          "sample": sample, "cpu": binding.cpu_model(), "library": os.path.basename(ref.path)},
         "e2e": {"value": value, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -452,10 +466,10 @@ def ours(args, wl):
             g.step_mixed(vb[s0], vb[1 - s0], [dh[s0]], [dh[1 - s0]], st)
             ms_state[0] = 1 - s0
 
-        # record packing, advection, divergence, first residual, gradient; per outer iteration
-        # scale, 2 half-sweeps per inner iteration, update, residual (the face table is made once
-        # per context).
-        launches_per_step = 5 + outer * (3 + 2 * wl["inner"])
+        # record packing, advection, divergence, first residual, convergence log, gradient; per
+        # outer iteration scale, 2 half-sweeps per inner iteration, update, residual (the face
+        # table is made once per context).
+        launches_per_step = 6 + outer * (3 + 2 * wl["inner"])
         # One launch is a half-sweep: half of an iteration's pass-model bytes (read e, read r,
         # write e at 2 bytes each).
         kernel_bytes, kernel_name, phase = 3, "rbgs_split_half_kernel (FP16 inner solve, colour-split, one colour per launch)", "inner"
@@ -463,7 +477,7 @@ def ours(args, wl):
         info, outer = info32, None
         st = plain_desc(cap32)
         step = step32(st)
-        launches_per_step = 3 + cap32
+        launches_per_step = 4 + cap32
         kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_stream_kernel<float>", "solve"
 
     for _ in range(args.warmup):
@@ -474,12 +488,17 @@ def ours(args, wl):
     clocks.start()
     g.profile_read()
     g.profile_enable(True)
+    g.solve_log(capacity=0, reset=True)
     ms = _timed_steps(torch, stream, step, args.steps)
     replicas.barrier(R)
     clk = clocks.stop()
     g.profile_enable(False)
     prof = g.profile_read()
     last = g.last_refine() if mixed else g.last_solve()
+    # Every timed step's solve, from the device-side convergence log.
+    logged, entries = g.solve_log(capacity=args.steps, reset=True)
+    worst = max((e.residual for e in entries), default=float("nan"))
+    not_converged = sum(1 for e in entries if e.residual > tol)
     ms = replicas.max_over_ranks(R, ms, dev)
     ms_step = ms / args.steps
     value = replicas.aggregate_rate(R, n, args.steps, ms)
@@ -511,32 +530,33 @@ def ours(args, wl):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, wl, info32.iterations)
+        cpu = cpu_baseline(args, wl, wl["fp32_iterations"])
     adjoint = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adjoint = adjoint_rollout(torch, hl, synth, dev)
 
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
-        cfg = {"workload": args.workload, "description": wl["desc"], "voxels": n, "leaves": len(origins),
-               "precision": args.precision, "dt": wl["dt"], "dx": wl["dx"], "tolerance": tol,
-               "residual": "relative FP64 Poisson residual ||b - L p|| / ||b||, b = div dx^2",
-               "l2": "inputs larger than L2 (%.0f MB of fields and solver state per GPU)" % (((12 + 4) * 2 + 8 + 16) * n / 1e6),
-               "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+        cfg = workload_config(args, wl, origins)
+        det = {"precision": args.precision, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
                "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
-               "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None}
+               "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
+               "timed_solves_logged": logged, "worst_residual_timed_steps": worst,
+               "timed_steps_above_tolerance": not_converged}
         if mixed:
-            cfg.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+            det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
                         "omega_inner": wl["omega_refined"], "inner_iterations": wl["inner"], "outer_cap": outer,
                         "red_black_iterations": last.iterations, "residual_reached": last.residual})
         else:
-            cfg.update({"omega": wl["omega"], "red_black_iterations": last.iterations, "iteration_cap": cap32,
+            det.update({"omega": wl["omega"], "red_black_iterations": last.iterations, "iteration_cap": cap32,
                         "residual_checked": last.residual})
         line = {
             "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 arithmetic; bf16/f16 storage, f64 refinement" if mixed else "f32", "data": "synthetic",
+            "config": cfg, "details": det,
             "roofline": {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": kernel_bytes * n, "launch_ms": k_ms,

@@ -8,8 +8,9 @@
 //   confine_sources       adv -> adv2, + sources, gravity       (vorticityConfinement out of
 //                                                                place, add_velocity_source(_xyz),
 //                                                                add_scalar_source, add_gravity)
-//   div_combust_buoy      adv2 -> div, fields, adv3             (divergence, combustion_oxygen,
-//                                                                temperature_buoyancy)
+//   div_combust_buoy      adv2 -> div, fields, adv3             (divergence, combustion_oxygen or
+//                                                                the force model's burn,
+//                                                                temperature_buoyancy [+ density])
 //   rbgs x iterations     div -> p                              (redBlackGaussSeidelUpdate)
 //   [divergence, rbgs x max(2, iterations/2)]  when disturbanceEnable > 0
 //   subtract_gradient     adv3, p -> velocity
@@ -92,16 +93,29 @@ __global__ void __launch_bounds__(kThreads) confine_sources_kernel(TopoView t, c
     for (int q = 0; q < ss.count; ++q) ss.dst[q][s] += dt * __ldg(ss.src[q] + s);
 }
 
-// divergence (Kernel.cu:432-453) of the forced velocity, combustion_oxygen
-// (Kernel.cu:641-677) in place on fuel/waste/temperature/flame with the expansion added to
-// that divergence, then temperature_buoyancy (Kernel.cu:546-563) from the burned temperature
-// into a separate velocity buffer (neighbouring threads still read `vel`).
+// The burn model and the buoyancy's density term of one step (hns_force_model), with the
+// reference's parameters.
+struct Burn {
+    float gain, expansion;           // combustion_oxygen: temperatureRelease, expansionRate
+    float rate, heat, ignition;      // combustion: burn rate, heat release, ignition temperature
+    float alpha;                     // density buoyancy; 0: the reference's temperature_buoyancy
+};
+
+// divergence (Kernel.cu:432-453) of the forced velocity, the combustion model in place on its
+// fields (kModel: HNS_COMBUSTION_OXYGEN, combustion_oxygen (Kernel.cu:641-677) on fuel, waste,
+// temperature and flame, the expansion added to that divergence; HNS_COMBUSTION_RATE,
+// combustion (Kernel.cu:568-588) on fuel and temperature; HNS_COMBUSTION_NONE), then
+// temperature_buoyancy (Kernel.cu:546-563) from the burned temperature, with the density term
+// v.y -= alpha density dt when alpha != 0, into a separate velocity buffer (neighbouring
+// threads still read `vel`).
+template <int kModel>
 __global__ void __launch_bounds__(kThreads) div_combust_buoy_kernel(TopoView t, const float* __restrict__ vel,
                                                                      float* __restrict__ vel_out, float* __restrict__ div,
                                                                      float inv_dx, float* __restrict__ fuel,
                                                                      float* __restrict__ waste, float* __restrict__ temp,
-                                                                     float* __restrict__ flame, float gain, float expansion,
-                                                                     float dt, float ambient, float strength) {
+                                                                     float* __restrict__ flame,
+                                                                     const float* __restrict__ density, Burn B, float dt,
+                                                                     float ambient, float strength) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
     load_nbhd(L, t, v.leaf);
@@ -117,24 +131,38 @@ __global__ void __launch_bounds__(kThreads) div_combust_buoy_kernel(TopoView t, 
     const float zm = (c.z + near_v(t, L, vel, i, j, k - 1).z) * 0.5f;
     float dv = (xp - xm + yp - ym + zp - zm) * inv_dx;
 
-    float f = fuel[s];
-    const float w = waste[s], T = temp[s], fl = flame[s];
-    if (f < 0.001f) f = 0.0f;
-    const float oxy = 1.0f - f - w;
-    float Tn = T;
-    if (oxy < 0.0f) {
-        fuel[s] = f;
-    } else {
-        const float burn = fminf(oxy, f);
-        fuel[s] = f - burn;
-        waste[s] = w + burn * 2.0f;
-        Tn = T + burn * gain;
-        temp[s] = Tn;
-        dv += burn * expansion;
-        flame[s] = fmaxf(fl, fminf(1.0f, burn * 10.0f));
+    float Tn = temp[s];
+    if constexpr (kModel == HNS_COMBUSTION_OXYGEN) {
+        float f = fuel[s];
+        const float w = waste[s], T = Tn, fl = flame[s];
+        if (f < 0.001f) f = 0.0f;
+        const float oxy = 1.0f - f - w;
+        if (oxy < 0.0f) {
+            fuel[s] = f;
+        } else {
+            const float burn = fminf(oxy, f);
+            fuel[s] = f - burn;
+            waste[s] = w + burn * 2.0f;
+            Tn = T + burn * B.gain;
+            temp[s] = Tn;
+            dv += burn * B.expansion;
+            flame[s] = fmaxf(fl, fminf(1.0f, burn * 10.0f));
+        }
+    } else if constexpr (kModel == HNS_COMBUSTION_RATE) {
+        const float f = fuel[s];
+        if (f > 0.0f && Tn >= B.ignition) {
+            const float burned = fminf(f, B.rate * dt);
+            fuel[s] = f - burned;
+            Tn = Tn + burned * B.heat;
+            temp[s] = Tn;
+        }
     }
     div[s] = dv;
-    if (Tn <= ambient) {
+    if (B.alpha != 0.0f) {
+        const float bt = Tn > ambient ? fmaxf(0.0f, (Tn - ambient) * strength) : 0.0f;
+        const float fy = bt - B.alpha * (density != nullptr ? __ldg(density + s) : 0.0f);
+        st3(vel_out, s, make_float3(c.x, c.y + fy * dt, c.z));
+    } else if (Tn <= ambient) {
         st3(vel_out, s, c);
     } else {
         const float by = fmaxf(0.0f, (Tn - ambient) * strength);
@@ -143,6 +171,18 @@ __global__ void __launch_bounds__(kThreads) div_combust_buoy_kernel(TopoView t, 
 }
 
 unsigned leaf_blocks(const Context& c) { return (unsigned)(c.topo.num_leaves * 2); }
+
+}  // namespace
+
+void check_force_model(const hns_force_model& m) {
+    if (m.combustion != HNS_COMBUSTION_OXYGEN && m.combustion != HNS_COMBUSTION_RATE && m.combustion != HNS_COMBUSTION_NONE)
+        fail(HNS_ERR_INVALID_ARG, "unknown combustion model " + std::to_string(m.combustion));
+    if (!std::isfinite(m.burn_rate) || !std::isfinite(m.heat_release) || !std::isfinite(m.ignition_temp) ||
+        !std::isfinite(m.density_buoyancy))
+        fail(HNS_ERR_INVALID_ARG, "force model parameters must be finite");
+}
+
+namespace {
 
 bool is_source(const std::string& n) { return n.rfind("src_", 0) == 0; }
 
@@ -168,7 +208,7 @@ Field& Context::ensure_field(const std::string& name, int components, bool zero)
     return *f;
 }
 
-void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& P) {
+void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& P, const hns_force_model& M) {
     const size_t n = (size_t)c.num_voxels();
     const float dx = c.dx;
     const float inv_dx = 1.0f / dx;
@@ -234,14 +274,29 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
             (sz && sz->components == 1) ? sz->buf.as<float>() : nullptr, P.gravity, ss);
         HNS_LAUNCHED();
 
-        // fuel/waste/temperature/flame are created zero-filled on first use (:326-338).
-        float* fuel = c.ensure_field("fuel", 1, true).buf.as<float>();
-        float* waste = c.ensure_field("waste", 1, true).buf.as<float>();
+        // The combustion model's fields are created zero-filled on first use (:326-338 for
+        // the reference's fuel/waste/temperature/flame; fuel and temperature for the rate model,
+        // temperature alone without combustion); density when the buoyancy has a density term.
+        const bool oxygen = M.combustion == HNS_COMBUSTION_OXYGEN;
+        float* fuel = M.combustion != HNS_COMBUSTION_NONE ? c.ensure_field("fuel", 1, true).buf.as<float>() : nullptr;
+        float* waste = oxygen ? c.ensure_field("waste", 1, true).buf.as<float>() : nullptr;
         float* temp = c.ensure_field("temperature", 1, true).buf.as<float>();
-        float* flame = c.ensure_field("flame", 1, true).buf.as<float>();
-        div_combust_buoy_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-            c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, P.temperatureRelease, P.expansionRate, dt_sub,
-            P.ambientTemp, P.buoyancyStrength);
+        float* flame = oxygen ? c.ensure_field("flame", 1, true).buf.as<float>() : nullptr;
+        const float* dens = M.density_buoyancy != 0.0f ? c.ensure_field("density", 1, true).buf.as<float>() : nullptr;
+        const Burn B{P.temperatureRelease, P.expansionRate, M.burn_rate, M.heat_release, M.ignition_temp,
+                     M.density_buoyancy};
+        if (M.combustion == HNS_COMBUSTION_OXYGEN)
+            div_combust_buoy_kernel<HNS_COMBUSTION_OXYGEN><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+                c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, dens, B, dt_sub, P.ambientTemp,
+                P.buoyancyStrength);
+        else if (M.combustion == HNS_COMBUSTION_RATE)
+            div_combust_buoy_kernel<HNS_COMBUSTION_RATE><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+                c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, dens, B, dt_sub, P.ambientTemp,
+                P.buoyancyStrength);
+        else
+            div_combust_buoy_kernel<HNS_COMBUSTION_NONE><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+                c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, dens, B, dt_sub, P.ambientTemp,
+                P.buoyancyStrength);
         HNS_LAUNCHED();
         c.phase_end();
 
@@ -360,12 +415,19 @@ HNS_API hns_status hns_field_info(const hns_ctx* ctx, int index, char* name, siz
 }
 
 HNS_API hns_status hns_advance(hns_ctx* ctx, int iterations, float dt, const hns_combustion_params* params) {
+    return hns_advance_model(ctx, iterations, dt, params, nullptr);
+}
+
+HNS_API hns_status hns_advance_model(hns_ctx* ctx, int iterations, float dt, const hns_combustion_params* params,
+                                     const hns_force_model* model) {
     return guarded([&] {
         Context* c = check_ctx(ctx);
         if (!params) fail(HNS_ERR_INVALID_ARG, "null params");
         if (iterations < 0) fail(HNS_ERR_INVALID_ARG, "negative iteration count");
+        const hns_force_model M = model ? *model : hns_force_model{};
+        check_force_model(M);
         DeviceGuard g(c->device);
-        run_advance(*c, iterations, dt, *params);
+        run_advance(*c, iterations, dt, *params, M);
     });
 }
 

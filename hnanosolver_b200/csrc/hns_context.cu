@@ -294,6 +294,8 @@ hns_status create_impl(hns_ctx** out, float voxel_size, int device, const std::f
             c.counters = c.d_counters.as<unsigned long long>();
             HNS_CUDA(cudaMemsetAsync(c.counters, 0, c.d_counters.bytes, c.stream));
             c.reduce_slots(1);
+            c.d_solve_log.alloc(sizeof(double) * (2 * Context::kSolveLogCap + 1));
+            HNS_CUDA(cudaMemsetAsync(c.d_solve_log.ptr, 0, c.d_solve_log.bytes, c.stream));
         } catch (...) {
             (void)cudaStreamDestroy(c.own_stream);
             c.own_stream = nullptr;
@@ -619,6 +621,7 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
     return guarded([&] {
         Context* c = check_ctx(ctx);
         check_ptr(vel, "velocity");
+        if (((uintptr_t)vel & 3u) != 0) fail(HNS_ERR_INVALID_ARG, "velocity must be 4-byte aligned");
         if (iterations < 0) fail(HNS_ERR_INVALID_ARG, "negative iteration count");
         DeviceGuard g(c->device);
         const size_t n = (size_t)c->num_voxels();

@@ -152,6 +152,11 @@ struct Context {
     // Scratch owned by the context, grown on demand and reused across calls.
     std::map<std::string, DeviceBuffer> scratch;
     DeviceBuffer d_reduce;  // FP64 reduction accumulators, allocated once (kReduceSlots doubles)
+    // Convergence log (hns_solve_log): kSolveLogCap entries of (iterations, residual) written on
+    // the device by every checked or refined solve, then the count of entries appended (as a
+    // 64-bit integer in the last slot). Allocated with the context.
+    static constexpr int kSolveLogCap = 4096;
+    DeviceBuffer d_solve_log;
     SolvePlan last_solve;   // schedule of the most recent checked solve (hns_last_solve)
     RefinePlan last_refine; // schedule of the most recent refined solve (hns_last_refine)
     // Profiling (hns_profile_*): device counters and per-phase events on the stream.
@@ -296,8 +301,9 @@ void launch_gradient_mixed(const Context& c, void* vel, const double* p);
 // u -= grad p for an FP32 velocity and an FP64 pressure, in place.
 void launch_gradient_f64(const Context& c, float* vel, const double* p);
 
-// HNS_Advance over the context's fields (hns_advance.cu).
-void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& params);
+// HNS_Advance over the context's fields with a force model (hns_advance.cu).
+void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& params, const hns_force_model& model);
+void check_force_model(const hns_force_model& m);
 
 // Runs `iterations` fused RBGS iterations from `p` (or zero) and leaves the result in `p`.
 void rbgs_solve(Context& c, const float* div, float* p, int iterations, float omega, unsigned flags);
@@ -311,6 +317,11 @@ SolvePlan rbgs_solve_checked(Context& c, const float* div, float* p, int max_ite
                              double tol, int check_every);
 // Host readback (synchronizes): iterations run and the last evaluated relative residual.
 void solve_result(Context& c, const SolvePlan& plan, int* iterations, double* residual);
+// Appends a solve's result to the context's convergence log on the device (no host wait). The
+// solve's checks are nchecks pairs {sum r^2, sum b^2}; the first passing check q (r^2 <= tol^2
+// b^2) stands for (q + offset) * per iterations; when none passes, the entry has cap_iterations
+// and the last check's residual.
+void log_solve(Context& c, const double* checks, int nchecks, double tol, int per, int offset, int cap_iterations);
 
 }  // namespace hns
 

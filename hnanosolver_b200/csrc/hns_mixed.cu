@@ -803,6 +803,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         HNS_LAUNCHED();
     }
     if (echo) refine_echo(c, plan);
+    log_solve(c, plan.slots, plan.max_outer + 1, tol, plan.inner, 0, plan.max_outer * plan.inner);
     return plan;
 }
 

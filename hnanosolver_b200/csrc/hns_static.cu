@@ -5,6 +5,7 @@
 //
 // The array lives in this translation unit only, so under CUDA's lazy module loading it
 // occupies device memory only in processes that call hns_project_static.
+#include <cstdint>
 #include <mutex>
 
 #include "hns_internal.cuh"
@@ -22,13 +23,18 @@ static __device__ __align__(256) float g_static_scratch[3 * kStaticMaxVoxels];
 std::mutex g_static_mu;
 float* g_static_ptr[kStaticMaxDevices] = {};
 
-// Address of g_static_scratch on `device`, looked up once per device with that device current
-// (the caller holds a DeviceGuard for it). The first lookup also loads this file's module.
-float* static_scratch(int device) {
+// Address of g_static_scratch on `device`, with that device current (the caller holds a
+// DeviceGuard for it). The first lookup also loads this file's module. Outside stream capture
+// the address is looked up again on every call (cheap), so a primary context that was reset and
+// re-created in between gets the array's new address; while the stream is being captured the
+// address cached by an earlier call is used, so that the first call must come before capture.
+float* static_scratch(int device, cudaStream_t stream) {
     if (device < 0 || device >= kStaticMaxDevices)
         fail(HNS_ERR_UNSUPPORTED, "hns_project_static supports device ordinals below " + std::to_string(kStaticMaxDevices));
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    HNS_CUDA(cudaStreamIsCapturing(stream, &cap));
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[device]) {
+    if (cap == cudaStreamCaptureStatusNone || !g_static_ptr[device]) {
         float* ptr = nullptr;
         HNS_CUDA(cudaGetSymbolAddress((void**)&ptr, g_static_scratch));
         g_static_ptr[device] = ptr;
@@ -48,6 +54,7 @@ HNS_API hns_status hns_project_static(hns_ctx* ctx, float* vel, int iterations, 
     return guarded([&] {
         Context* c = check_ctx(ctx);
         if (!vel) fail(HNS_ERR_INVALID_ARG, "null velocity");
+        if (((uintptr_t)vel & 3u) != 0) fail(HNS_ERR_INVALID_ARG, "velocity must be 4-byte aligned");
         if (iterations < 0) fail(HNS_ERR_INVALID_ARG, "negative iteration count");
         const size_t n = (size_t)c->num_voxels();
         if (n > kStaticMaxVoxels)
@@ -55,7 +62,7 @@ HNS_API hns_status hns_project_static(hns_ctx* ctx, float* vel, int iterations, 
                                           " active voxels, above the fixed scratch's maximum of " +
                                           std::to_string(kStaticMaxVoxels) + " (2048 leaves); use hns_project");
         DeviceGuard g(c->device);
-        float* base = static_scratch(c->device);
+        float* base = static_scratch(c->device, c->stream);
         float* div = base;
         float* p = base + kStaticMaxVoxels;
         float* tmp = base + 2 * kStaticMaxVoxels;

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -48,6 +49,7 @@ SolvePlan rbgs_solve_checked(Context& c, const float* div, float* p, int max_ite
         launch_rbgs_iteration(c, div, src, dst, omega, flags, chk, tol2, out);
         src = dst;
     }
+    log_solve(c, plan.slots, plan.num_checks, tol, E, 1, K);
     return plan;
 }
 
@@ -71,6 +73,35 @@ void solve_result(Context& c, const SolvePlan& plan, int* iterations, double* re
     const int q = plan.num_checks - 1;
     *iterations = plan.max_iterations;
     *residual = h[2 * q + 1] > 0 ? std::sqrt(h[2 * q] / h[2 * q + 1]) : 0.0;
+}
+
+namespace {
+
+__global__ void solve_log_kernel(const double* __restrict__ chk, int nchecks, double tol2, int per, int offset,
+                                 int cap_iterations, double* __restrict__ log, int cap) {
+    int q = nchecks - 1;
+    bool hit = false;
+    for (int i = 0; i < nchecks; ++i)
+        if (chk[2 * i] <= tol2 * chk[2 * i + 1]) {
+            q = i;
+            hit = true;
+            break;
+        }
+    unsigned long long* count = reinterpret_cast<unsigned long long*>(log + 2 * cap);
+    const unsigned long long m = *count;
+    double* e = log + 2 * (m % (unsigned long long)cap);
+    e[0] = hit ? (double)((q + offset) * per) : (double)cap_iterations;
+    e[1] = chk[2 * q + 1] > 0.0 ? sqrt(chk[2 * q] / chk[2 * q + 1]) : 0.0;
+    *count = m + 1;
+}
+
+}  // namespace
+
+void log_solve(Context& c, const double* checks, int nchecks, double tol, int per, int offset, int cap_iterations) {
+    if (nchecks <= 0 || c.d_solve_log.ptr == nullptr) return;
+    solve_log_kernel<<<1, 1, 0, c.stream>>>(checks, nchecks, tol * tol, per, offset, cap_iterations,
+                                            c.d_solve_log.as<double>(), Context::kSolveLogCap);
+    HNS_LAUNCHED();
 }
 
 namespace {
@@ -249,6 +280,30 @@ HNS_API hns_status hns_step_plain_host(hns_ctx* ctx, float* vel, float* const* s
         st = finish_info(*c, o, *desc, info);
     });
     return g != HNS_OK ? g : st;
+}
+
+HNS_API hns_status hns_solve_log(hns_ctx* ctx, hns_solve_info* out, int capacity, int* count, int reset) {
+    return guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!count || capacity < 0 || (capacity > 0 && !out)) fail(HNS_ERR_INVALID_ARG, "bad log arguments");
+        DeviceGuard dg(c->device);
+        const int cap = Context::kSolveLogCap;
+        std::vector<double> h(2 * (size_t)cap + 1);
+        HNS_CUDA(cudaMemcpyAsync(h.data(), c->d_solve_log.ptr, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        HNS_CUDA(cudaStreamSynchronize(c->stream));
+        unsigned long long m = 0;
+        std::memcpy(&m, &h[2 * (size_t)cap], sizeof(m));
+        *count = (int)std::min<unsigned long long>(m, 0x7fffffffull);
+        // The most recent min(m, cap, capacity) entries, oldest first.
+        const unsigned long long k = std::min<unsigned long long>({m, (unsigned long long)cap, (unsigned long long)capacity});
+        for (unsigned long long q = 0; q < k; ++q) {
+            const unsigned long long idx = (m - k + q) % (unsigned long long)cap;
+            out[q].iterations = (int)h[2 * idx];
+            out[q].residual = h[2 * idx + 1];
+            out[q].initial_residual = 1.0;
+        }
+        if (reset) HNS_CUDA(cudaMemsetAsync(c->d_solve_log.as<double>() + 2 * cap, 0, sizeof(double), c->stream));
+    });
 }
 
 HNS_API hns_status hns_last_solve(hns_ctx* ctx, hns_solve_info* info) {

@@ -58,6 +58,31 @@ SOLVE_REFINE = 4
 SOLVE_MULTIGRID = 8
 
 
+COMBUSTION_OXYGEN, COMBUSTION_RATE, COMBUSTION_NONE = 0, 1, 2
+
+
+class ForceModel(ctypes.Structure):
+    """hns_force_model: the burn (COMBUSTION_*) and the buoyancy's density term; the zero value
+    is the reference's HNS_Advance."""
+
+    _fields_ = [("combustion", _i), ("burn_rate", _f), ("heat_release", _f), ("ignition_temp", _f),
+                ("density_buoyancy", _f)]
+
+
+FIRE_FIELDS = ("velocity", "density", "temperature", "fuel", "waste", "flame")
+FIRE_SOURCES = ("velocity", "temperature", "density", "fuel")
+
+
+class FireFields(ctypes.Structure):
+    """hns_fire_fields: BF16 velocity and FP16 scalars (device pointers, None: absent)."""
+
+    _fields_ = [(k, _p) for k in FIRE_FIELDS]
+
+
+class FireSources(ctypes.Structure):
+    _fields_ = [(k, _p) for k in FIRE_SOURCES]
+
+
 class CombustionParams(ctypes.Structure):
     """hns_combustion_params: the layout of the reference's CombustionParams."""
 
@@ -118,6 +143,7 @@ def _load():
     _sig(lib, "hns_step_plain", _i, _p, _p, _p, _p, _p, _i, ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_step_plain_host", _i, _p, _p, _p, _i, ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_last_solve", _i, _p, ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_solve_log", _i, _p, ctypes.POINTER(SolveInfo), _i, ctypes.POINTER(_i), _i)
     _sig(lib, "hns_field_set", _i, _p, ctypes.c_char_p, _i, _p, _i)
     _sig(lib, "hns_field_get", _i, _p, ctypes.c_char_p, _p, _i)
     _sig(lib, "hns_field_ptr", _i, _p, ctypes.c_char_p, ctypes.POINTER(_p), ctypes.POINTER(_i))
@@ -125,7 +151,11 @@ def _load():
     _sig(lib, "hns_field_count", _i, _p)
     _sig(lib, "hns_field_info", _i, _p, _i, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(_i))
     _sig(lib, "hns_advance", _i, _p, _i, _f, ctypes.POINTER(CombustionParams))
+    _sig(lib, "hns_advance_model", _i, _p, _i, _f, ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel))
     _sig(lib, "hns_active_mask", _i, _p, _p)
+    _sig(lib, "hns_advance_mixed", _i, _p, ctypes.POINTER(FireFields), ctypes.POINTER(FireFields),
+         ctypes.POINTER(FireSources), _f, ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel),
+         ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_convert", _i, _p, _p, _i, _p, _i, _i64)
     _sig(lib, "hns_step_mixed", _i, _p, _p, _p, _p, _p, _i, ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_step_mixed_host", _i, _p, _p, _p, _i, ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
@@ -329,8 +359,24 @@ class Grid:
     def field_remove(self, name: str):
         check(lib.hns_field_remove(self._h, name.encode()))
 
-    def advance(self, iterations: int, dt: float, params: CombustionParams):
-        check(lib.hns_advance(self._h, iterations, dt, ctypes.byref(params)))
+    def advance(self, iterations: int, dt: float, params: CombustionParams, model: ForceModel | None = None):
+        if model is None:
+            check(lib.hns_advance(self._h, iterations, dt, ctypes.byref(params)))
+        else:
+            check(lib.hns_advance_model(self._h, iterations, dt, ctypes.byref(params), ctypes.byref(model)))
+
+    def advance_mixed(self, fields_in: dict, fields_out: dict, sources: dict | None, dt: float,
+                      params: CombustionParams, model: ForceModel | None, desc: MixedDesc, info: bool = False):
+        """hns_advance_mixed on torch tensors: fields_in / fields_out map names of FIRE_FIELDS to
+        BF16 (velocity) or FP16 device tensors; sources maps names of FIRE_SOURCES."""
+        fi = FireFields(*[_dptr(fields_in.get(k)) for k in FIRE_FIELDS])
+        fo = FireFields(*[_dptr(fields_out.get(k)) for k in FIRE_FIELDS])
+        src = FireSources(*[_dptr((sources or {}).get(k)) for k in FIRE_SOURCES])
+        si = SolveInfo()
+        check(lib.hns_advance_mixed(self._h, ctypes.byref(fi), ctypes.byref(fo), ctypes.byref(src), dt,
+                                    ctypes.byref(params), ctypes.byref(model) if model is not None else None,
+                                    ctypes.byref(desc), ctypes.byref(si) if info else None))
+        return si if info else None
 
     def active_mask(self) -> np.ndarray:
         out = np.zeros(self.num_voxels, np.uint8)
@@ -397,6 +443,15 @@ class Grid:
         check(lib.hns_step_mixed_host(self._h, vel.ctypes.data, ptrs, len(scalars), ctypes.byref(desc),
                                       ctypes.byref(si) if info else None))
         return si if info else None
+
+    def solve_log(self, capacity: int = 4096, reset: bool = True):
+        """(count, entries): solves logged since the last reset, and the most recent
+        min(count, 4096, capacity) of them, oldest first (hns_solve_log)."""
+        arr = (SolveInfo * max(1, capacity))()
+        count = _i()
+        check(lib.hns_solve_log(self._h, arr, capacity, ctypes.byref(count), 1 if reset else 0))
+        k = min(count.value, 4096, capacity)
+        return count.value, [arr[q] for q in range(k)]
 
     def last_refine(self) -> SolveInfo:
         si = SolveInfo()

@@ -13,6 +13,8 @@ Workloads (seed 0 unless stated):
              radius-200 sphere: about 23M voxels
   box128     128^3 box, 4096 leaves, 2,097,152 voxels (the differentiable rollout)
   fire1024   1024^3 box, leaves inside 32 seeded spheres of radius 30-120
+
+fire_state() adds the fire workloads' fields and their sphere source (fuel and heat).
 """
 from __future__ import annotations
 
@@ -60,12 +62,19 @@ def _leaf_centers(extent: int) -> np.ndarray:
     return _box_leaves(extent).astype(np.float64) + 3.5
 
 
-def spheres_topology(extent: int, count: int, rmin: float, rmax: float, seed: int) -> np.ndarray:
-    """Leaves of an extent^3 box whose centre lies within r + half-diagonal of one of
-    `count` seeded spheres (radius U(rmin, rmax), centre U(r, extent - r))."""
+def spheres(extent: int, count: int, rmin: float, rmax: float, seed: int):
+    """The seeded spheres of spheres_topology: (centres (count, 3), radii (count,)), radius
+    U(rmin, rmax), centre U(r, extent - r) per axis."""
     rng = np.random.default_rng(seed)
     radii = rng.uniform(rmin, rmax, size=count)
     centers = np.stack([rng.uniform(r, extent - r, size=3) for r in radii])
+    return centers, radii
+
+
+def spheres_topology(extent: int, count: int, rmin: float, rmax: float, seed: int) -> np.ndarray:
+    """Leaves of an extent^3 box whose centre lies within r + half-diagonal of one of
+    `count` seeded spheres (radius U(rmin, rmax), centre U(r, extent - r))."""
+    centers, radii = spheres(extent, count, rmin, rmax, seed)
     leaves = _box_leaves(extent)
     lc = leaves.astype(np.float64) + 3.5
     keep = np.zeros(len(leaves), dtype=bool)
@@ -83,6 +92,10 @@ def shell_topology(extent: int = 512, radius: float = 200.0, band: float = 16.0,
     d = np.linalg.norm(leaves.astype(np.float64) + 3.5 - center, axis=1)
     keep = np.abs(d - radius) <= band + LEAF_HALF_DIAGONAL
     return sort_leaves_nanovdb(leaves[keep])
+
+
+# The sphere sets of the fire workloads: (extent, count, rmin, rmax).
+SPHERE_WORKLOADS = {"plume256": (256, 8, 20.0, 60.0), "fire1024": (1024, 32, 30.0, 120.0)}
 
 
 def topology(name: str, seed: int = 0) -> np.ndarray:
@@ -194,3 +207,29 @@ def noise_fields(origins: np.ndarray, seed: int = 0):
     dens = value_noise_leaves(origins, seed)
     vel = np.stack([2.0 * value_noise_leaves(origins, seed + 1 + k) - 1.0 for k in range(3)], axis=1)
     return np.ascontiguousarray(dens, dtype=np.float32), np.ascontiguousarray(vel, dtype=np.float32)
+
+
+def sphere_mask(origins: np.ndarray, centre, radius: float) -> np.ndarray:
+    """float32 per slot: 1 where the voxel lies within `radius` voxels of `centre`, else 0."""
+    c = leaf_dense_coords(origins).astype(np.float64)
+    return (np.linalg.norm(c - np.asarray(centre, dtype=np.float64), axis=1) <= radius).astype(np.float32)
+
+
+def fire_state(name: str, seed: int = 0, source_radius: float = 10.0, fuel_rate: float = 1.0,
+               temperature_rate: float = 2.0):
+    """Initial state and sources of a fire workload (plume256, fire1024): velocity and density
+    as noise_fields; temperature, fuel and flame zero; the sources src_fuel = fuel_rate and
+    src_temperature = temperature_rate inside a sphere of source_radius voxels at the centre of
+    the workload's first sphere, zero elsewhere. Returns (origins, fields, sources): fields
+    maps velocity (N, 3) and density, temperature, fuel, flame (N,); sources maps src_fuel and
+    src_temperature (N,). All float32."""
+    extent, count, rmin, rmax = SPHERE_WORKLOADS[name]
+    origins = topology(name, seed)
+    centers, _ = spheres(extent, count, rmin, rmax, seed)
+    dens, vel = noise_fields(origins, seed)
+    n = len(dens)
+    mask = sphere_mask(origins, centers[0], source_radius)
+    fields = {"velocity": vel, "density": dens, "temperature": np.zeros(n, np.float32),
+              "fuel": np.zeros(n, np.float32), "flame": np.zeros(n, np.float32)}
+    sources = {"src_fuel": mask * np.float32(fuel_rate), "src_temperature": mask * np.float32(temperature_rate)}
+    return origins, fields, sources

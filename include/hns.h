@@ -151,7 +151,10 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
  * allocator) holds the free memory.
  * - At most 1,048,576 active voxels (2048 leaves); larger grids return HNS_ERR_UNSUPPORTED.
  * - The first call on each device looks the array's address up (cudaGetSymbolAddress, which
- *   also loads its module); make that first call before any stream capture begins.
+ *   also loads its module); make that first call before any stream capture begins. Calls made
+ *   outside capture look it up again; calls made during capture use the address found by the
+ *   last call outside it, so the device must not be reset between that call and the capture.
+ * - vel must be 4-byte aligned (HNS_ERR_INVALID_ARG otherwise).
  * - The array is shared by every context on a device: calls that overlap in time on one
  *   device (different streams or threads) race on it. Serialise them.
  * - The pressure scratch is cleared to zero on every call. */
@@ -201,6 +204,15 @@ HNS_API hns_status hns_step_plain_host(hns_ctx* ctx, float* vel, float* const* s
 /* Iterations and last checked residual of the most recent convergence-checked solve
  * (synchronizes). residual is -1 when that solve ran without a tolerance. */
 HNS_API hns_status hns_last_solve(hns_ctx* ctx, hns_solve_info* info);
+/* Convergence log. Every convergence-checked solve (a tolerance > 0) and every refined solve
+ * appends one entry on the device, in stream order and without a host wait: the iterations
+ * its result took (red-black iterations; outer x inner for a refined solve; the cap when the
+ * tolerance was not reached) and the relative FP64 residual of its last check. The context
+ * keeps the last 4096 entries. hns_solve_log (synchronizes) sets *count to the entries
+ * appended since the last reset, copies the most recent min(*count, 4096, capacity) of them
+ * to out (oldest first; initial_residual 1) and, when reset is nonzero, starts a new count.
+ * No counterpart in the reference, whose solves have no tolerance. */
+HNS_API hns_status hns_solve_log(hns_ctx* ctx, hns_solve_info* out, int capacity, int* count, int reset);
 
 /* ---- mixed precision -------------------------------------------------------------------
  * Fields stored as BF16 velocity (3 x bf16 interleaved per slot) and FP16 scalars, FP32
@@ -290,6 +302,69 @@ typedef struct hns_combustion_params {
  * scalars present at the call's start with the projected velocity. fuel, waste, temperature
  * and flame are created zero-filled when missing. */
 HNS_API hns_status hns_advance(hns_ctx* ctx, int iterations, float dt, const hns_combustion_params* params);
+/* Force models of the all-in-one step. The reference's HNS_Advance burns with
+ * combustion_oxygen and has a temperature-only buoyancy; its `combustion` kernel (rate and heat,
+ * src/Cuda/Kernel.cu:568-588) is called by no step. hns_force_model selects the burn and adds a
+ * density term to the buoyancy; its zero value is the reference's step. */
+#define HNS_COMBUSTION_OXYGEN 0 /* combustion_oxygen (Kernel.cu:641-677): fuel, waste, temperature, flame;
+                                   adds expansionRate x burn to the divergence */
+#define HNS_COMBUSTION_RATE 1   /* combustion (Kernel.cu:568-588): where fuel > 0 and T >= ignition_temp,
+                                   burn min(fuel, burn_rate dt); T += burned x heat_release */
+#define HNS_COMBUSTION_NONE 2   /* no burn */
+
+typedef struct hns_force_model {
+    int combustion;         /* HNS_COMBUSTION_* */
+    float burn_rate;        /* HNS_COMBUSTION_RATE */
+    float heat_release;     /* HNS_COMBUSTION_RATE */
+    float ignition_temp;    /* HNS_COMBUSTION_RATE */
+    float density_buoyancy; /* alpha: v.y += (b_T - alpha density) dt, b_T the reference's temperature
+                               buoyancy (max(0, (T - ambientTemp) buoyancyStrength) where
+                               T > ambientTemp, else 0); 0 is the reference's buoyancy */
+} hns_force_model;
+
+/* hns_advance with a force model (NULL: the reference's). The fields the combustion model uses
+ * are created zero-filled when missing (oxygen: fuel, waste, temperature, flame; rate: fuel,
+ * temperature; none: temperature), and "density" when density_buoyancy != 0. */
+HNS_API hns_status hns_advance_model(hns_ctx* ctx, int iterations, float dt, const hns_combustion_params* params,
+                                     const hns_force_model* model);
+/* ---- the all-in-one step on reduced-precision storage --------------------------------------
+ * HNS_Advance's sequence (hns_advance_model) on caller-owned device arrays stored as BF16
+ * velocity (3 per slot, interleaved) and FP16 scalars, with FP32 arithmetic and each pressure
+ * solve the FP64 iterative refinement of hns_step_mixed, run to solve->tolerance instead of a
+ * fixed iteration count. A field is given in both `in` and `out` or in neither; in and out must
+ * not alias. temperature is required; fuel unless the model burns nothing; waste and flame for
+ * the oxygen burn; density for a density buoyancy. Every field given is advected (the
+ * reference's advect_scalars, along the projected velocity); the step creates no field. */
+typedef struct hns_fire_fields {
+    void* velocity;    /* BF16 [3N] */
+    void* density;     /* FP16 [N] or NULL */
+    void* temperature; /* FP16 [N] */
+    void* fuel;        /* FP16 [N] or NULL */
+    void* waste;       /* FP16 [N] or NULL */
+    void* flame;       /* FP16 [N] or NULL */
+} hns_fire_fields;
+
+/* Sources added each substep, f += dt src (add_velocity_source / add_scalar_source,
+ * src/Cuda/Kernel.cu:732-745); NULL entries (or a NULL struct) add nothing. */
+typedef struct hns_fire_sources {
+    const void* velocity;    /* BF16 [3N] */
+    const void* temperature; /* FP16 [N] */
+    const void* density;     /* FP16 [N] */
+    const void* fuel;        /* FP16 [N] */
+} hns_fire_sources;
+
+/* One HNS_Advance call from `in` to `out` (params->substeps substeps of dt / substeps; the
+ * intermediate states live in solver-owned arrays). solve: omega (inner SOR factor, <= 0:
+ * 1.9), tolerance, max_outer, inner_iterations and flags as in hns_step_mixed; its dt is
+ * ignored. With the disturbance branch (params->disturbanceEnable > 0) the velocity is solved
+ * again after the buoyancy, as HNS_Advance does. With info the call synchronizes, reports the
+ * last solve's inner iterations (outer x inner) and FP64 residual, and returns
+ * HNS_ERR_NOT_CONVERGED when it is above the tolerance; every solve is also appended to the
+ * convergence log (hns_solve_log). */
+HNS_API hns_status hns_advance_mixed(hns_ctx* ctx, const hns_fire_fields* in, const hns_fire_fields* out,
+                                     const hns_fire_sources* sources, float dt, const hns_combustion_params* params,
+                                     const hns_force_model* model, const hns_mixed_desc* solve, hns_solve_info* info);
+
 /* host uint8[num_voxels]: the activity mask of the last step (the reference's
  * build_activity_mask marks every slot active, src/Cuda/Kernel.cu:75). */
 HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out);

@@ -28,11 +28,13 @@ _i = ctypes.c_int
 
 
 def build(ref: bool | None = None) -> None:
-    """Compile the oracle (and, where the reference checkout exists, oracle/_ref)."""
+    """Compile the oracle and oracle/_ref: always with ref=True, never with ref=False, and with
+    ref=None only where the reference checkout exists (oracle/Makefile's ref-if-present: the
+    HNS_REFERENCE environment variable or the recipe's default path)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     if ref is None:
-        ref = os.path.isdir("/root/reference/src/Cuda")
-    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref-if-present"], check=True)
+    elif ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
 
 
@@ -65,6 +67,18 @@ class AdvanceFields(ctypes.Structure):
         ("src_vel_y", _p), ("src_vel_z", _p), ("src_temperature", _p), ("src_density", _p), ("src_fuel", _p),
         ("collision_sdf", _p),
     ]
+
+
+class ForceModel(ctypes.Structure):
+    """hnso_force_model: combustion 0 oxygen (the reference's step), 1 rate/heat, 2 none; the
+    buoyancy's density term alpha; omega > 0 replaces the solves' SOR factor."""
+
+    _fields_ = [("combustion", _i), ("burn_rate", _d), ("heat_release", _d), ("ignition_temp", _d),
+                ("density_buoyancy", _d), ("omega", _d)]
+
+
+# Fields each combustion model uses, created zero-filled when absent (fuel, waste, temperature, flame).
+MODEL_FIELDS = {0: ("fuel", "waste", "temperature", "flame"), 1: ("fuel", "temperature"), 2: ("temperature",)}
 
 
 def make_advance_fields(n, velocity, scalars: dict, created: dict, sources: dict):
@@ -127,6 +141,9 @@ class Oracle:
             _sig(lib, "hnso_add_velocity_source_xyz" + s, None, _i64, _p, _p, _p, _p, r)
             _sig(lib, "hnso_add_gravity" + s, None, _i64, _p, r, r)
             _sig(lib, "hnso_project" + s, None, _p, _p, _p, _p, r, _i, r)
+        for suf, real in (("_f32", _f), ("_f64", _d)):
+            _sig(lib, "hnso_hns_advance_model" + suf, None, _p, ctypes.POINTER(AdvanceFields), real, _i, real,
+                 ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel))
         _sig(lib, "hnso_hns_advance_f32", None, _p, ctypes.POINTER(AdvanceFields), _f, _i, _f,
              ctypes.POINTER(CombustionParams))
 
@@ -253,6 +270,23 @@ class OracleTopo:
         return vel, sc, created
 
 
+    def hns_advance_model(self, velocity, scalars: dict, sources: dict, dx, iteration, dt, params: CombustionParams,
+                          model: ForceModel | None = None, dtype=np.float32):
+        """hns_advance with a force model, in float32 or float64. Returns (velocity, scalars,
+        created), copies of the inputs; `created` holds the fields the model made."""
+        model = model or ForceModel()
+        vel = np.ascontiguousarray(velocity, dtype=dtype).copy()
+        sc = {k: np.ascontiguousarray(v, dtype=dtype).copy() for k, v in scalars.items()}
+        created = {k: np.zeros(self.n, dtype) for k in MODEL_FIELDS[model.combustion] if k not in sc}
+        src = {k: np.ascontiguousarray(v, dtype=dtype) for k, v in sources.items()}
+        f, keep = make_advance_fields(self.n, vel, sc, created, src)
+        suf = "_f64" if np.dtype(dtype) == np.float64 else "_f32"
+        getattr(self.o.lib, "hnso_hns_advance_model" + suf)(self.h, ctypes.byref(f), dx, iteration, dt,
+                                                            ctypes.byref(params), ctypes.byref(model))
+        del keep
+        return vel, sc, created
+
+
 class RefOracle:
     """The reference's own kernels (host-compiled). Takes the leaf-dense coordinates and
     builds the reference's NanoVDB ValueOnIndex grid from them."""
@@ -291,6 +325,9 @@ class RefOracle:
         _sig(lib, "ref_hns_advance", None, _p, _p, ctypes.POINTER(AdvanceFields), _f, _i, _f,
              ctypes.POINTER(CombustionParams))
         _sig(lib, "ref_plain_step", None, _p, _p, _i64, _p, _p, _i, _f, _f, _i, _f, _p)
+
+        _sig(lib, "ref_hns_advance_model", None, _p, _p, ctypes.POINTER(AdvanceFields), _f, _i, _f,
+             ctypes.POINTER(CombustionParams), _i, _f, _f, _f)
 
     def grid(self, coords) -> "RefGrid":
         return RefGrid(self, coords)
@@ -410,6 +447,21 @@ class RefGrid:
         src = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in sources.items()}
         f, keep = make_advance_fields(self.n, vel, sc, created, src)
         self.lib.ref_hns_advance(self.h, ptr(self.coords), ctypes.byref(f), dx, iteration, dt, ctypes.byref(params))
+        del keep
+        return vel, sc, created
+
+
+    def hns_advance_model(self, velocity, scalars: dict, sources: dict, dx, iteration, dt, params: CombustionParams,
+                          combustion: int = 0, burn_rate=0.0, heat_release=0.0, ignition_temp=0.0):
+        """The reference's HNS_Advance sequence with its `combustion` kernel in place of
+        combustion_oxygen when combustion == 1 (the reference has no density buoyancy term)."""
+        vel = np.ascontiguousarray(velocity, dtype=np.float32).copy()
+        sc = {k: np.ascontiguousarray(v, dtype=np.float32).copy() for k, v in scalars.items()}
+        created = {k: np.zeros(self.n, np.float32) for k in MODEL_FIELDS[combustion] if k not in sc}
+        src = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in sources.items()}
+        f, keep = make_advance_fields(self.n, vel, sc, created, src)
+        self.lib.ref_hns_advance_model(self.h, ptr(self.coords), ctypes.byref(f), dx, iteration, dt, ctypes.byref(params),
+                                       combustion, burn_rate, heat_release, ignition_temp)
         del keep
         return vel, sc, created
 

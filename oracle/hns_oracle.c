@@ -125,18 +125,21 @@ void hnso_sort_leaves_nanovdb(int32_t* leaf_origins, int64_t num_leaves) {
 #define FMA fmaf
 #define SQRT sqrtf
 #define INV6 0.166666667f
+#define OMEGA_OF_DX(dx) (2.0f / (1.0f + sinf(3.14159f * (dx))))
 #include "hns_oracle_impl.h"
 #undef R
 #undef S
 #undef FMA
 #undef SQRT
 #undef INV6
+#undef OMEGA_OF_DX
 
 #define R double
 #define S _f64
 #define FMA fma
 #define SQRT sqrt
 #define INV6 (1.0 / 6.0)
+#define OMEGA_OF_DX(dx) (2.0 / (1.0 + sin(3.14159 * (dx))))
 #include "hns_oracle_impl.h"
 #undef R
 #undef S
@@ -145,103 +148,9 @@ void hnso_sort_leaves_nanovdb(int32_t* leaf_origins, int64_t num_leaves) {
 #undef INV6
 
 /* ---- HNS_Advance ------------------------------------------------------------------------
- * The kernel sequence of one HNS_Advance call (src/Cuda/HNanoSolver.cu:223-456): with a
- * collision SDF, enforceCollisionBoundaries on the velocity first (:241-244); per substep advect velocity, confinement (run out of place; the reference's
- * in-place launch at :279-281 races), velocity and scalar sources, gravity, divergence,
- * oxygen combustion (adds expansion to the divergence), buoyancy from the burned
- * temperature, iteration x (red, black) from p = 0 with omega = 2/(1+sin(3.14159 dx)), the
- * disturbance re-solve (divergence again, p = 0, max(2, iteration/2) sweeps) when enabled,
- * gradient subtraction into the velocity (with the SDF, then enforceCollisionBoundaries again,
- * :411-414), then advection of the persistent scalars with the projected velocity; the SDF
- * also enters the velocity and scalar advection and the gradient subtraction. */
-static float* find_scalar(const hnso_advance_fields* f, const char* name) {
-    for (int i = 0; i < f->nscalars; ++i)
-        if (strcmp(f->names[i], name) == 0) return f->scalars[i];
-    return NULL;
-}
-
+ * The reference's step is the force model's zero value (hns_oracle_impl.h,
+ * hnso_hns_advance_model). */
 void hnso_hns_advance_f32(const hnso_topo* t, const hnso_advance_fields* F, float dx, int iteration, float dt,
                           const hnso_combustion_params* P) {
-    const int64_t N = F->n;
-    const float inv_dx = 1.0f / dx;
-    const int SUBS = P->substeps > 1 ? P->substeps : 1;
-    const float dt_sub = dt / (float)SUBS;
-    static const char* special[4] = {"fuel", "waste", "temperature", "flame"};
-    int made[4] = {0, 0, 0, 0};
-    float* adv = (float*)calloc((size_t)(3 * N), sizeof(float));
-    float* adv2 = (float*)calloc((size_t)(3 * N), sizeof(float));
-    float* div = (float*)calloc((size_t)N, sizeof(float));
-    float* p = (float*)calloc((size_t)N, sizeof(float));
-    float* o[4];
-    for (int q = 0; q < 4; ++q) o[q] = (float*)calloc((size_t)N, sizeof(float));
-
-    const float* sdf = F->collision_sdf;
-    if (sdf) hnso_enforce_collision_f32(t, F->velocity, sdf, inv_dx);
-    for (int s = 0; s < SUBS; ++s) {
-        advect_vector_impl_f32(t, F->velocity, adv, dt_sub, inv_dx, sdf);
-        hnso_vorticity_confinement_f32(t, adv, adv2, dt_sub, inv_dx, P->vorticityScale, P->factorScale);
-        float* sw = adv;
-        adv = adv2;
-        adv2 = sw;
-        if (F->src_vel) {
-            hnso_add_velocity_source_f32(N, adv, F->src_vel, dt_sub);
-        } else if (F->src_vel_x && F->src_vel_y && F->src_vel_z) {
-            hnso_add_velocity_source_xyz_f32(N, adv, F->src_vel_x, F->src_vel_y, F->src_vel_z, dt_sub);
-        }
-        const float* srcs[3] = {F->src_temperature, F->src_density, F->src_fuel};
-        const char* dsts[3] = {"temperature", "density", "fuel"};
-        for (int q = 0; q < 3; ++q) {
-            float* dst = find_scalar(F, dsts[q]);
-            if (!dst)
-                for (int k = 0; k < 4; ++k)
-                    if (made[k] && strcmp(special[k], dsts[q]) == 0) dst = F->created[k];
-            if (srcs[q] && dst) hnso_add_scalar_source_f32(N, dst, srcs[q], dt_sub);
-        }
-        if (P->gravity != 0.0f) hnso_add_gravity_f32(N, adv, P->gravity, dt_sub);
-        hnso_divergence_f32(t, adv, div, inv_dx);
-
-        float* fld[4];
-        for (int k = 0; k < 4; ++k) {
-            fld[k] = find_scalar(F, special[k]);
-            if (!fld[k]) {
-                fld[k] = F->created[k];
-                if (!made[k]) {
-                    memset(fld[k], 0, sizeof(float) * (size_t)N);
-                    made[k] = 1;
-                }
-            }
-        }
-        for (int q = 0; q < 4; ++q) memset(o[q], 0, sizeof(float) * (size_t)N);
-        hnso_combustion_oxygen_f32(N, fld[0], fld[1], fld[2], div, fld[3], o[0], o[1], o[2], o[3], P->temperatureRelease,
-                                   P->expansionRate);
-        hnso_temperature_buoyancy_f32(N, adv, o[2], adv, dt_sub, P->ambientTemp, P->buoyancyStrength);
-        for (int k = 0; k < 4; ++k) memcpy(fld[k], o[k], sizeof(float) * (size_t)N);
-
-        memset(p, 0, sizeof(float) * (size_t)N);
-        const float omega = 2.0f / (1.0f + sinf(3.14159f * dx));
-        hnso_rbgs_f32(t, div, p, dx, iteration, omega);
-        if (P->disturbanceEnable > 0.0f) {
-            hnso_divergence_f32(t, adv, div, inv_dx);
-            memset(p, 0, sizeof(float) * (size_t)N);
-            hnso_rbgs_f32(t, div, p, dx, iteration / 2 > 2 ? iteration / 2 : 2, omega);
-        }
-        subtract_gradient_impl_f32(t, adv, p, F->velocity, inv_dx, sdf);
-        if (sdf) hnso_enforce_collision_f32(t, F->velocity, sdf, inv_dx);
-
-        if (F->nscalars > 0) {
-            float** outs = (float**)malloc(sizeof(float*) * (size_t)F->nscalars);
-            for (int k = 0; k < F->nscalars; ++k) outs[k] = (float*)calloc((size_t)N, sizeof(float));
-            advect_scalars_impl_f32(t, F->velocity, (const float* const*)F->scalars, outs, F->nscalars, dt_sub, inv_dx, sdf);
-            for (int k = 0; k < F->nscalars; ++k) {
-                memcpy(F->scalars[k], outs[k], sizeof(float) * (size_t)N);
-                free(outs[k]);
-            }
-            free(outs);
-        }
-    }
-    free(adv);
-    free(adv2);
-    free(div);
-    free(p);
-    for (int q = 0; q < 4; ++q) free(o[q]);
+    hnso_hns_advance_model_f32(t, F, dx, iteration, dt, P, NULL);
 }

@@ -79,6 +79,8 @@ typedef struct {
                                       R strength);                                                                 \
     void hnso_combustion##S(int64_t n, const R* fuel, const R* temp, R* out_fuel, R* out_temp, R dt, R ignition,   \
                             R rate, R heat);                                                                       \
+    void hnso_buoyancy_density##S(int64_t n, const R* vel, const R* temp, const R* density, R* out, R dt,        \
+                                  R ambient, R strength, R alpha);                                               \
     void hnso_combustion_oxygen##S(int64_t n, const R* fuel, const R* waste, const R* temp, R* div, const R* flame, \
                                    R* o_fuel, R* o_waste, R* o_temp, R* o_flame, R gain, R expansion);             \
     void hnso_add_scalar_source##S(int64_t n, R* field, const R* src, R dt);                                       \
@@ -91,29 +93,54 @@ typedef struct {
 HNSO_DECLARE(float, _f32)
 HNSO_DECLARE(double, _f64)
 
-/* Fields of one HNS_Advance call (src/Cuda/HNanoSolver.cu:223-456). `names`/`scalars` are
- * the persistent scalar fields present when the call starts; exactly these are advected.
- * fuel/waste/temperature/flame absent from that list are created zero-filled on first use
- * in `created` (n floats each) and are not advected during this call. */
+/* Fields of one HNS_Advance call (src/Cuda/HNanoSolver.cu:223-456), in float (_f32) or double
+ * (_f64). `names`/`scalars` are the persistent scalar fields present when the call starts;
+ * exactly these are advected. fuel/waste/temperature/flame absent from that list are created
+ * zero-filled on first use in `created` (n values each, in that order) and are not advected
+ * during this call. */
+#define HNSO_ADVANCE_FIELDS(R, S)                                                                                  \
+    typedef struct {                                                                                               \
+        int64_t n;                                                                                                 \
+        R* velocity;                                                                                               \
+        int nscalars;                                                                                              \
+        const char* const* names;                                                                                  \
+        R* const* scalars;                                                                                         \
+        R* created[4];                                                                                             \
+        const R* src_vel;                                                                                          \
+        const R* src_vel_x;                                                                                        \
+        const R* src_vel_y;                                                                                        \
+        const R* src_vel_z;                                                                                        \
+        const R* src_temperature;                                                                                  \
+        const R* src_density;                                                                                      \
+        const R* src_fuel;                                                                                         \
+        const R* collision_sdf; /* n, or NULL: no collider */                                                      \
+    } hnso_advance_fields##S;
+HNSO_ADVANCE_FIELDS(float, _f32)
+HNSO_ADVANCE_FIELDS(double, _f64)
+typedef hnso_advance_fields_f32 hnso_advance_fields;
+
+/* Force model of the step. The zero value is the reference's HNS_Advance.
+ * combustion: 0 combustion_oxygen (src/Cuda/Kernel.cu:641-677, the reference's step),
+ *             1 combustion (Kernel.cu:568-588: burn min(fuel, burn_rate dt) where fuel > 0
+ *               and T >= ignition_temp, T += burned heat_release), 2 none.
+ * density_buoyancy: alpha of the buoyancy's density term v.y -= alpha density dt (an
+ *             extension; the reference has none).
+ * omega:      > 0 replaces the solves' SOR factor 2/(1+sin(3.14159 dx)). */
 typedef struct {
-    int64_t n;
-    float* velocity;
-    int nscalars;
-    const char* const* names;
-    float* const* scalars;
-    float* created[4];
-    const float* src_vel;
-    const float* src_vel_x;
-    const float* src_vel_y;
-    const float* src_vel_z;
-    const float* src_temperature;
-    const float* src_density;
-    const float* src_fuel;
-    const float* collision_sdf; /* n, or NULL: no collider */
-} hnso_advance_fields;
+    int combustion;
+    double burn_rate;
+    double heat_release;
+    double ignition_temp;
+    double density_buoyancy;
+    double omega;
+} hnso_force_model;
 
 void hnso_hns_advance_f32(const hnso_topo* t, const hnso_advance_fields* f, float dx, int iteration, float dt,
                           const hnso_combustion_params* params);
+void hnso_hns_advance_model_f32(const hnso_topo* t, const hnso_advance_fields_f32* f, float dx, int iteration, float dt,
+                                const hnso_combustion_params* params, const hnso_force_model* model);
+void hnso_hns_advance_model_f64(const hnso_topo* t, const hnso_advance_fields_f64* f, double dx, int iteration,
+                                double dt, const hnso_combustion_params* params, const hnso_force_model* model);
 
 #ifdef __cplusplus
 }

@@ -467,6 +467,26 @@ void FN(hnso_temperature_buoyancy)(int64_t n, const R* vel, const R* temp, R* ou
     }
 }
 
+/* temperature_buoyancy with a density term, the extension the configurations' buoyancy needs
+ * (the reference has no density term): v.y += (b_T - alpha * density) dt, with b_T the
+ * reference's max(0, (T - Tamb) beta) where T > Tamb and 0 elsewhere. alpha = 0 is exactly
+ * hnso_temperature_buoyancy. density may be NULL (taken as 0). */
+void FN(hnso_buoyancy_density)(int64_t n, const R* vel, const R* temp, const R* density, R* out, R dt, R ambient,
+                               R strength, R alpha) {
+    if (alpha == (R)0) {
+        FN(hnso_temperature_buoyancy)(n, vel, temp, out, dt, ambient, strength);
+        return;
+    }
+    for (int64_t s = 0; s < n; ++s) {
+        const R T = temp[s];
+        const R bt = T > ambient ? FN(fmax_)((R)0, (T - ambient) * strength) : (R)0;
+        const R f = bt - alpha * (density ? density[s] : (R)0);
+        out[3 * s] = vel[3 * s];
+        out[3 * s + 1] = vel[3 * s + 1] + f * dt;
+        out[3 * s + 2] = vel[3 * s + 2];
+    }
+}
+
 /* combustion (src/Cuda/Kernel.cu:568-588): burn min(fuel, rate*dt) where fuel > 0 and
  * T >= ignition; heat release raises T. */
 void FN(hnso_combustion)(int64_t n, const R* fuel, const R* temp, R* out_fuel, R* out_temp, R dt, R ignition, R rate,
@@ -545,6 +565,130 @@ void FN(hnso_project)(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterat
     memcpy(tmp, vel, sizeof(R) * 3 * (size_t)N);
     FN(hnso_subtract_gradient)(t, tmp, p, vel, inv_dx);
     free(tmp);
+}
+
+/* ---- HNS_Advance with a force model ----------------------------------------------------
+ * The kernel sequence of one HNS_Advance call (src/Cuda/HNanoSolver.cu:223-456): with a
+ * collision SDF, enforceCollisionBoundaries on the velocity first (:241-244); per substep
+ * advect velocity, confinement (run out of place; the reference's in-place launch at
+ * :279-281 races), velocity and scalar sources, gravity, divergence, the combustion model,
+ * buoyancy from the burned temperature, iteration x (red, black) from p = 0 with omega =
+ * 2/(1+sin(3.14159 dx)), the disturbance re-solve (divergence again, p = 0,
+ * max(2, iteration/2) sweeps) when enabled, gradient subtraction into the velocity (with the
+ * SDF, then enforceCollisionBoundaries again, :411-414), then advection of the persistent
+ * scalars with the projected velocity; the SDF also enters the velocity and scalar advection
+ * and the gradient subtraction.
+ * The model (NULL: the reference) chooses the combustion: combustion_oxygen (Kernel.cu:641-677,
+ * the reference's step; adds expansion to the divergence), combustion (Kernel.cu:568-588,
+ * rate/heat; no step of the reference calls it) or none; adds the density term of the
+ * buoyancy (hnso_buoyancy_density); and may replace the SOR factor (FP64 solves run to
+ * convergence). Fields the combustion model uses (oxygen: fuel, waste, temperature, flame;
+ * rate: fuel, temperature; none: temperature) that are absent from F->scalars are created
+ * zero-filled in F->created on first use and not advected during this call. */
+static R* FN(find_scalar)(const FN(hnso_advance_fields)* f, const char* name) {
+    for (int i = 0; i < f->nscalars; ++i)
+        if (strcmp(f->names[i], name) == 0) return f->scalars[i];
+    return NULL;
+}
+
+void FN(hnso_hns_advance_model)(const hnso_topo* t, const FN(hnso_advance_fields)* F, R dx, int iteration, R dt,
+                                const hnso_combustion_params* P, const hnso_force_model* M) {
+    const hnso_force_model reference_model = {0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!M) M = &reference_model;
+    const int64_t N = F->n;
+    const R inv_dx = (R)1 / dx;
+    const int SUBS = P->substeps > 1 ? P->substeps : 1;
+    const R dt_sub = dt / (R)SUBS;
+    static const char* special[4] = {"fuel", "waste", "temperature", "flame"};
+    int uses[4] = {1, 1, 1, 1};
+    if (M->combustion == 1) uses[1] = uses[3] = 0;
+    if (M->combustion == 2) uses[0] = uses[1] = uses[3] = 0;
+    int made[4] = {0, 0, 0, 0};
+    R* adv = (R*)calloc((size_t)(3 * N), sizeof(R));
+    R* adv2 = (R*)calloc((size_t)(3 * N), sizeof(R));
+    R* div = (R*)calloc((size_t)N, sizeof(R));
+    R* p = (R*)calloc((size_t)N, sizeof(R));
+    R* o[4];
+    for (int q = 0; q < 4; ++q) o[q] = (R*)calloc((size_t)N, sizeof(R));
+
+    const R* sdf = F->collision_sdf;
+    if (sdf) FN(hnso_enforce_collision)(t, F->velocity, sdf, inv_dx);
+    for (int s = 0; s < SUBS; ++s) {
+        FN(advect_vector_impl)(t, F->velocity, adv, dt_sub, inv_dx, sdf);
+        FN(hnso_vorticity_confinement)(t, adv, adv2, dt_sub, inv_dx, P->vorticityScale, P->factorScale);
+        R* sw = adv;
+        adv = adv2;
+        adv2 = sw;
+        if (F->src_vel) {
+            FN(hnso_add_velocity_source)(N, adv, F->src_vel, dt_sub);
+        } else if (F->src_vel_x && F->src_vel_y && F->src_vel_z) {
+            FN(hnso_add_velocity_source_xyz)(N, adv, F->src_vel_x, F->src_vel_y, F->src_vel_z, dt_sub);
+        }
+        const R* srcs[3] = {F->src_temperature, F->src_density, F->src_fuel};
+        const char* dsts[3] = {"temperature", "density", "fuel"};
+        for (int q = 0; q < 3; ++q) {
+            R* dst = FN(find_scalar)(F, dsts[q]);
+            if (!dst)
+                for (int k = 0; k < 4; ++k)
+                    if (made[k] && strcmp(special[k], dsts[q]) == 0) dst = F->created[k];
+            if (srcs[q] && dst) FN(hnso_add_scalar_source)(N, dst, srcs[q], dt_sub);
+        }
+        if (P->gravity != 0.0f) FN(hnso_add_gravity)(N, adv, P->gravity, dt_sub);
+        FN(hnso_divergence)(t, adv, div, inv_dx);
+
+        R* fld[4] = {NULL, NULL, NULL, NULL};
+        for (int k = 0; k < 4; ++k) {
+            if (!uses[k]) continue;
+            fld[k] = FN(find_scalar)(F, special[k]);
+            if (!fld[k]) {
+                fld[k] = F->created[k];
+                if (!made[k]) {
+                    memset(fld[k], 0, sizeof(R) * (size_t)N);
+                    made[k] = 1;
+                }
+            }
+        }
+        if (M->combustion == 0) {
+            for (int q = 0; q < 4; ++q) memset(o[q], 0, sizeof(R) * (size_t)N);
+            FN(hnso_combustion_oxygen)(N, fld[0], fld[1], fld[2], div, fld[3], o[0], o[1], o[2], o[3],
+                                       P->temperatureRelease, P->expansionRate);
+            for (int k = 0; k < 4; ++k) memcpy(fld[k], o[k], sizeof(R) * (size_t)N);
+        } else if (M->combustion == 1) {
+            FN(hnso_combustion)(N, fld[0], fld[2], o[0], o[2], dt_sub, (R)M->ignition_temp, (R)M->burn_rate,
+                                (R)M->heat_release);
+            memcpy(fld[0], o[0], sizeof(R) * (size_t)N);
+            memcpy(fld[2], o[2], sizeof(R) * (size_t)N);
+        }
+        FN(hnso_buoyancy_density)(N, adv, fld[2], FN(find_scalar)(F, "density"), adv, dt_sub, P->ambientTemp,
+                                  P->buoyancyStrength, (R)M->density_buoyancy);
+
+        memset(p, 0, sizeof(R) * (size_t)N);
+        const R omega = M->omega > 0.0 ? (R)M->omega : OMEGA_OF_DX(dx);
+        FN(hnso_rbgs)(t, div, p, dx, iteration, omega);
+        if (P->disturbanceEnable > 0.0f) {
+            FN(hnso_divergence)(t, adv, div, inv_dx);
+            memset(p, 0, sizeof(R) * (size_t)N);
+            FN(hnso_rbgs)(t, div, p, dx, iteration / 2 > 2 ? iteration / 2 : 2, omega);
+        }
+        FN(subtract_gradient_impl)(t, adv, p, F->velocity, inv_dx, sdf);
+        if (sdf) FN(hnso_enforce_collision)(t, F->velocity, sdf, inv_dx);
+
+        if (F->nscalars > 0) {
+            R** outs = (R**)malloc(sizeof(R*) * (size_t)F->nscalars);
+            for (int k = 0; k < F->nscalars; ++k) outs[k] = (R*)calloc((size_t)N, sizeof(R));
+            FN(advect_scalars_impl)(t, F->velocity, (const R* const*)F->scalars, outs, F->nscalars, dt_sub, inv_dx, sdf);
+            for (int k = 0; k < F->nscalars; ++k) {
+                memcpy(F->scalars[k], outs[k], sizeof(R) * (size_t)N);
+                free(outs[k]);
+            }
+            free(outs);
+        }
+    }
+    free(adv);
+    free(adv2);
+    free(div);
+    free(p);
+    for (int q = 0; q < 4; ++q) free(o[q]);
 }
 
 #undef FN

@@ -310,8 +310,12 @@ static float* find_scalar(const RefAdvanceFields* f, const char* name) {
 
 // Restates HNS_Advance (src/Cuda/HNanoSolver.cu:223-456), with the reference's collision
 // kernels and branches when F->collision_sdf is set (:241-244, :273-275, :406-414, :438-441).
-void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, float dx, int iteration, float dt,
-                     const CombustionParams* params) {
+// combustion: 0 runs combustion_oxygen (the reference's step); 1 runs the reference's
+// `combustion` kernel (Kernel.cu:568-588) with burn_rate, heat_release and ignition_temp in its
+// place, creating only fuel and temperature when absent, the sequence otherwise unchanged.
+void ref_hns_advance_model(void* g, const int32_t* coords, const RefAdvanceFields* F, float dx, int iteration, float dt,
+                           const CombustionParams* params, int combustion_model, float burn_rate, float heat_release,
+                           float ignition_temp) {
     const IndexGrid* grid = static_cast<RefGrid*>(g)->grid;
     const int64_t N = F->n;
     const float inv_dx = 1.0f / dx;
@@ -351,8 +355,9 @@ void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, 
         if (params->gravity != 0.0f) launch(N, [&] { add_gravity(V(adv.data()), params->gravity, dt_sub, nullptr, (int)N); });
         launch(N, [&] { divergence(grid, cc, V(adv.data()), div.data(), inv_dx, nullptr, (size_t)N); });
 
-        float* fld[4];
+        float* fld[4] = {nullptr, nullptr, nullptr, nullptr};
         for (int k = 0; k < 4; ++k) {
+            if (combustion_model == 1 && (k == 1 || k == 3)) continue;
             fld[k] = find_scalar(F, special[k]);
             if (!fld[k]) {
                 fld[k] = F->created[k];
@@ -366,18 +371,27 @@ void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, 
         std::fill(o_waste.begin(), o_waste.end(), 0.0f);
         std::fill(o_temp.begin(), o_temp.end(), 0.0f);
         std::fill(o_flame.begin(), o_flame.end(), 0.0f);
-        launch(N, [&] {
-            combustion_oxygen(fld[0], fld[1], fld[2], div.data(), fld[3], o_fuel.data(), o_waste.data(), o_temp.data(),
-                              o_flame.data(), params->temperatureRelease, params->expansionRate, nullptr, (int)N);
-        });
+        if (combustion_model == 1) {
+            launch(N, [&] {
+                combustion(grid, cc, fld[0], fld[2], o_fuel.data(), o_temp.data(), dt_sub, ignition_temp, burn_rate,
+                           heat_release, (size_t)N);
+            });
+        } else {
+            launch(N, [&] {
+                combustion_oxygen(fld[0], fld[1], fld[2], div.data(), fld[3], o_fuel.data(), o_waste.data(), o_temp.data(),
+                                  o_flame.data(), params->temperatureRelease, params->expansionRate, nullptr, (int)N);
+            });
+        }
         launch(N, [&] {
             temperature_buoyancy(V(adv.data()), o_temp.data(), V(adv.data()), dt_sub, params->ambientTemp, params->buoyancyStrength,
                                  nullptr, (size_t)N);
         });
         std::copy(o_fuel.begin(), o_fuel.end(), fld[0]);
-        std::copy(o_waste.begin(), o_waste.end(), fld[1]);
         std::copy(o_temp.begin(), o_temp.end(), fld[2]);
-        std::copy(o_flame.begin(), o_flame.end(), fld[3]);
+        if (combustion_model != 1) {
+            std::copy(o_waste.begin(), o_waste.end(), fld[1]);
+            std::copy(o_flame.begin(), o_flame.end(), fld[3]);
+        }
 
         std::fill(p.begin(), p.end(), 0.0f);
         const float omega = 2.0f / (1.0f + sinf(3.14159f * dx));
@@ -404,6 +418,11 @@ void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, 
             for (int k = 0; k < F->nscalars; ++k) std::copy(outs[k].begin(), outs[k].end(), F->scalars[k]);
         }
     }
+}
+
+void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, float dx, int iteration, float dt,
+                     const CombustionParams* params) {
+    ref_hns_advance_model(g, coords, F, dx, iteration, dt, params, 0, 0.0f, 0.0f, 0.0f);
 }
 
 }  // extern "C"

@@ -1,0 +1,140 @@
+"""The all-in-one step with force models (hns_advance_model) against the oracle's restatement
+(hnso_hns_advance_model, pinned to the reference's own `combustion`, `combustion_oxygen` and
+`temperature_buoyancy` kernels by tests/test_oracle_forces.py and tests/test_oracle.py):
+max |gpu - oracle| / max |oracle| <= 1e-5 for every field after every call.
+
+Covered: the rate/heat burn (the reference's `combustion` kernel), the oxygen burn of the
+reference's step and no burn, each with the buoyancy's density term; the fields each model
+creates; and the sparse-plume configuration at full size (256^3 box, 8 seeded spheres of
+radius 20-60, a radius-10 source of fuel 1.0 and heat 2.0 at the first sphere's centre,
+alpha 0.1, beta 0.5, confinement 0.3, burn rate 0.5 and heat 1.0, 100 red-black iterations,
+dt 1/24) for two steps."""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from hnanosolver_b200 import synth
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def _params(**kw):
+    from oracle.binding import CombustionParams as OP
+
+    from hnanosolver_b200.lib import CombustionParams
+
+    p = OP.houdini_defaults()
+    p.buoyancyStrength = 0.5
+    p.ambientTemp = 0.0
+    p.vorticityScale = 0.3
+    p.factorScale = 1.0
+    p.disturbanceEnable = 0.0
+    p.gravity = 0.0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p, CombustionParams.from_buffer_copy(bytes(p))
+
+
+def _models(combustion, alpha, rate=0.5, heat=1.0, ignition=0.0):
+    from oracle.binding import ForceModel as OM
+
+    from hnanosolver_b200.lib import ForceModel
+
+    return (OM(combustion=combustion, burn_rate=rate, heat_release=heat, ignition_temp=ignition, density_buoyancy=alpha),
+            ForceModel(combustion=combustion, burn_rate=rate, heat_release=heat, ignition_temp=ignition,
+                       density_buoyancy=alpha))
+
+
+def _run_both(grid, t, vel, state, sources, calls, iterations, dt, op, params, om, gm):
+    """`calls` steps on the device and in the oracle, compared after each."""
+    ov = vel
+    for call in range(calls):
+        grid.advance(iterations, dt, params, gm)
+        ov, sc, cr = t.hns_advance_model(ov, state, sources, 0.1, iterations, dt, op, om)
+        state = {**sc, **cr}  # created fields persist and are advected from the next call on
+        assert rel_err(grid.field_get("velocity"), ov) <= TOL, call
+        for name, ref in state.items():
+            assert rel_err(grid.field_get(name), ref) <= TOL, (call, name)
+    return ov, state
+
+
+@pytest.mark.parametrize("combustion,alpha,substeps", [(1, 0.1, 1), (1, 0.0, 2), (0, 0.1, 1), (2, 0.1, 1)])
+def test_force_models_three_calls(dev, oracle, combustion, alpha, substeps):
+    from hnanosolver_b200 import lib as hl
+
+    origins = synth.spheres_topology(80, 3, 8.0, 18.0, seed=6)
+    dens, vel = synth.smoothed_fields(origins, seed=11, box_passes=2)
+    vel = (vel * 5.0).astype(np.float32)
+    n = len(dens)
+    rng = np.random.default_rng(5)
+    centres, _ = synth.spheres(80, 3, 8.0, 18.0, 6)
+    mask = synth.sphere_mask(origins, centres[0], 6.0)
+    sources = {"src_fuel": mask, "src_temperature": mask * np.float32(2.0)}
+    state = {"density": dens, "temperature": (rng.random(n, dtype=np.float32) * 1.5).astype(np.float32),
+             "fuel": (rng.random(n, dtype=np.float32) * (rng.random(n) < 0.5)).astype(np.float32),
+             "flame": np.zeros(n, np.float32)}
+    op, params = _params(substeps=substeps)
+    om, gm = _models(combustion, alpha)
+    grid = hl.Grid(origins, voxel_size=0.1)
+    grid.field_set("velocity", vel)
+    for k, a in {**state, **sources}.items():
+        grid.field_set(k, a)
+    _run_both(grid, oracle.topo(origins), vel, state, sources, 3, 15, 1.0 / 24.0, op, params, om, gm)
+    names = set(grid.field_names())
+    assert ("waste" in names) == (combustion == 0)
+    grid.close()
+
+
+@pytest.mark.parametrize("combustion,made", [(1, {"fuel", "temperature"}), (2, {"temperature"}),
+                                             (0, {"fuel", "waste", "temperature", "flame"})])
+def test_force_models_create_their_fields(dev, oracle, combustion, made):
+    from hnanosolver_b200 import lib as hl
+
+    origins = synth.spheres_topology(64, 2, 8.0, 14.0, seed=8)
+    dens, vel = synth.smoothed_fields(origins, seed=3, box_passes=1)
+    centres, _ = synth.spheres(64, 2, 8.0, 14.0, 8)
+    mask = synth.sphere_mask(origins, centres[0], 5.0)
+    sources = {"src_fuel": mask, "src_temperature": mask * np.float32(2.0)}
+    op, params = _params()
+    om, gm = _models(combustion, 0.1)
+    grid = hl.Grid(origins, voxel_size=0.1)
+    grid.field_set("velocity", vel)
+    grid.field_set("density", dens)
+    for k, a in sources.items():
+        grid.field_set(k, a)
+    _, state = _run_both(grid, oracle.topo(origins), vel, {"density": dens}, sources, 2, 10, 0.1, op, params, om, gm)
+    assert set(grid.field_names()) - {"velocity", "density", "src_fuel", "src_temperature"} == made
+    assert set(state) - {"density"} == made
+    grid.close()
+
+
+def test_plume256_configuration(dev, oracle):
+    """The sparse-plume configuration at full size, two steps, every field against the oracle."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, fields, sources = synth.fire_state("plume256")
+    assert 3_000_000 < 512 * len(origins) < 4_000_000
+    op, params = _params()
+    om, gm = _models(1, 0.1)
+    grid = hl.Grid(origins, voxel_size=0.1)
+    for k, a in {**fields, **sources}.items():
+        grid.field_set(k, a)
+    state = {k: v for k, v in fields.items() if k != "velocity"}
+    ov, state = _run_both(grid, oracle.topo(origins), fields["velocity"], state, sources, 2, 100, 1.0 / 24.0, op,
+                          params, om, gm)
+    # Fuel and heat entered at the source and burned there.
+    inside = sources["src_fuel"] > 0
+    assert state["temperature"][inside].min() > 0.0
+    assert state["fuel"][inside].max() > 0.0
+    assert float(np.abs(ov - fields["velocity"]).max()) > 1e-3
+    grid.close()
