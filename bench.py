@@ -2,7 +2,7 @@
 """Throughput of one solver step on a seeded synthetic sparse grid, on 1..N GPUs.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload shell512] [--precision fp32]
+                    [--workload shell512|plume256|fire1024] [--forces] [--precision mixed|fp32]
 
 A step is one pass of the hot path over the grid: the SOP operator chain
 HNanoAdvect + HNanoAdvectVelocity + HNanoProjectNonDivergent (scalars and velocity advected
@@ -52,6 +52,24 @@ WORKLOADS = {
                      check_every=10, fp32_iterations=None),
 }
 RBGS_BYTES_PER_VOXEL = 12  # one fused red+black iteration: read p, read div, write p (FP32)
+
+# The fire step (HNS_Advance with the configurations' forces): the sparse plume runs it in FP32
+# with a fixed 100 red-black iterations per step, the large sparse fire on BF16/FP16 storage with
+# the refined solve to 1e-5. Forces: buoyancy alpha 0.1 (density) and beta 0.5 (temperature,
+# ambient 0), vorticity confinement 0.3 with a one-voxel offset, the rate/heat burn (rate 0.5,
+# heat 1.0, ignition 0), no gravity, no disturbance re-solve; sources of fuel 1.0 and heat 2.0 in
+# a radius-10 sphere at the first sphere's centre (synth.fire_state).
+FIRE = dict(alpha=0.1, beta=0.5, ambient=0.0, confinement=0.3, factor_scale=1.0, burn_rate=0.5, heat_release=1.0,
+            ignition=0.0, source_radius=10.0, source_fuel=1.0, source_temperature=2.0)
+FIRE_WORKLOADS = {
+    "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60; fields density, temperature, "
+                          "fuel, flame and velocity (FP32); fire forces and sources; 100 red-black iterations per step",
+                     dx=0.1, dt=1.0 / 24.0, iterations=100, precision="fp32", fp32_iterations=100),
+    "fire1024": dict(desc="1024^3 box, leaves inside 32 seeded spheres of radius 30-120; fields density, temperature, "
+                          "fuel, flame (FP16) and velocity (BF16); fire forces and sources; refined solve to 1e-5",
+                     dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.94, inner=40, cap=8000,
+                     check_every=20, precision="mixed", fp32_iterations=None),
+}
 
 
 def measured_peak_gbs():
@@ -574,14 +592,312 @@ def ours(args, wl):
     replicas.finish(R)
 
 
+def fire_params(mod):
+    """(CombustionParams, ForceModel) of the fire step, from the module `mod` (the library's
+    lib or the oracle's binding)."""
+    p = mod.CombustionParams()
+    p.expansionRate, p.temperatureRelease = 0.1, 0.5  # the oxygen burn's; unused by the rate burn
+    p.buoyancyStrength, p.ambientTemp = FIRE["beta"], FIRE["ambient"]
+    p.vorticityScale, p.factorScale = FIRE["confinement"], FIRE["factor_scale"]
+    p.disturbanceEnable, p.substeps, p.gravity = 0.0, 1, 0.0
+    m = mod.ForceModel(combustion=1, burn_rate=FIRE["burn_rate"], heat_release=FIRE["heat_release"],
+                       ignition_temp=FIRE["ignition"], density_buoyancy=FIRE["alpha"])
+    return p, m
+
+
+def fire_config(args, wl, origins):
+    n = 512 * len(origins)
+    cfg = {"workload": args.workload, "step": "fire", "description": wl["desc"], "voxels": n, "leaves": len(origins),
+           "dt": wl["dt"], "dx": wl["dx"], "forces": FIRE, "fp32_red_black_iterations": wl["fp32_iterations"],
+           "l2": "inputs larger than L2 (%.0f MB of fields and solver state per GPU)" % (80 * n / 1e6)}
+    if "tolerance" in wl:
+        cfg["tolerance"] = wl["tolerance"]
+        cfg["residual"] = "relative FP64 Poisson residual ||b - L p|| / ||b||, b = div dx^2"
+    return cfg
+
+
+def fire_cpu_sample(args, wl, iters, omega, steps, warmup, budget_s=None):
+    """The reference's HNS_Advance with its `combustion` kernel (oracle/_ref, all host threads)
+    on a bounded sample: every launch over 1/S of its 256-voxel blocks. Returns (rate, sample
+    description, threads)."""
+    from hnanosolver_b200 import synth
+    from oracle import binding
+
+    ref = binding.RefOracle()
+    origins, fields, sources = synth.fire_state(args.workload)
+    g = ref.grid(synth.leaf_dense_coords(origins))
+    n = 512 * len(origins)
+    blocks = (n + 255) // 256
+    stride = max(1, blocks // 2048)
+    params, model = fire_params(binding)
+    state = {k: v for k, v in fields.items() if k != "velocity"}
+    ref.lib.ref_set_block_stride(stride)
+
+    def one():
+        return g.hns_advance_model(fields["velocity"], state, sources, wl["dx"], iters, wl["dt"], params,
+                                   combustion=1, burn_rate=model.burn_rate, heat_release=model.heat_release,
+                                   ignition_temp=model.ignition_temp, omega=omega)
+
+    for _ in range(warmup):
+        one()
+    times, t_start = [], time.perf_counter()
+    while len(times) < steps and (budget_s is None or not times or time.perf_counter() - t_start < budget_s):
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+    ref.lib.ref_set_block_stride(1)
+    sampled = (blocks + stride - 1) // stride * 256
+    t = sum(times) / len(times)
+    sample = (f"{len(times)} steps of the reference's HNS_Advance kernels with its combustion kernel (no density "
+              f"buoyancy term: the reference has none), every launch over 1/{stride} of its 256-voxel blocks "
+              f"({sampled} of {n} voxels), {iters} red-black iterations at omega {omega or 'from dx'}")
+    return sampled / t, sample, ref.lib.ref_num_threads(), binding.cpu_model(), os.path.basename(ref.path)
+
+
+def reference_arm_fire(args, wl):
+    rank, world, _ = dist_info()
+    if rank != 0:
+        return
+    from hnanosolver_b200 import synth
+
+    origins = synth.topology(args.workload)
+    iters = wl["fp32_iterations"] or 1000
+    value, sample, cores, cpu, library = fire_cpu_sample(args, wl, iters, wl.get("omega", 0.0), args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 512 * len(origins) / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": fire_config(args, wl, origins),
+        "cpu_baseline": {"value": value, "unit": "voxel-steps/s", "cores": cores, "kind": "reference", "sample": sample,
+                         "cpu": cpu, "library": library},
+        "e2e": {"value": value, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def ours_fire(args, wl):
+    import torch
+
+    from hnanosolver_b200 import lib as hl
+    from hnanosolver_b200 import replicas, synth
+
+    R = replicas.ranks_from_env()
+    rank, world, local = R.rank, R.world, R.local
+    replicas.start(R, "nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    origins, fields, sources = synth.fire_state(args.workload, seed=replicas.seed_of(R))
+    n = 512 * len(origins)
+    g = hl.Grid(origins, voxel_size=wl["dx"], device=local)
+    stream = torch.cuda.Stream(device=dev)
+    g.set_stream(stream.cuda_stream)
+    params, model = fire_params(hl)
+    mixed = args.precision == "mixed"
+    dt = wl["dt"]
+    tol = wl.get("tolerance")
+
+    def load_fp32():
+        for k, a in {**fields, **sources}.items():
+            g.field_set(k, a)
+
+    # ---- FP32 forms of the fire step at the same residual (the solve-to-tolerance workloads) ----
+    fp32 = None
+    cap32 = None
+    if tol is not None:
+        def pdesc(cap):
+            return hl.StepDesc(dt=0.0, max_iterations=cap, omega=wl["omega"], tolerance=tol,
+                               check_every=wl["check_every"], flags=0)
+
+        def rdesc(outer):
+            return hl.StepDesc(dt=0.0, max_iterations=0, omega=wl["omega_refined"], tolerance=tol, check_every=10,
+                               flags=hl.SOLVE_REFINE, max_outer=outer, inner_iterations=wl["inner"])
+
+        def tolerant(fn):
+            try:
+                return fn()
+            except hl.HnsError as e:
+                if e.status != 6:
+                    raise
+                return None
+
+        load_fp32()
+        i32 = tolerant(lambda: g.advance_solve(dt, params, model, pdesc(wl["cap"]), info=True)) or g.last_solve()
+        cap32 = i32.iterations + 2 * wl["check_every"]
+        load_fp32()
+        ir = tolerant(lambda: g.advance_solve(dt, params, model, rdesc(60), info=True)) or g.last_refine()
+        outer_r = max(1, ir.iterations // wl["inner"]) + 2
+        cmp_steps = 0 if args.no_fp32_comparison else max(1, min(args.steps, 3))
+        if cmp_steps:
+            load_fp32()
+            g.advance_solve(dt, params, model, pdesc(cap32))
+            ms_plain = _timed_steps(torch, stream, lambda: g.advance_solve(dt, params, model, pdesc(cap32)),
+                                    cmp_steps) / cmp_steps
+            lp = g.last_solve()
+            load_fp32()
+            g.advance_solve(dt, params, model, rdesc(outer_r))
+            ms_ref = _timed_steps(torch, stream, lambda: g.advance_solve(dt, params, model, rdesc(outer_r)),
+                                  cmp_steps) / cmp_steps
+            lr = g.last_refine()
+            fp32 = {"plain": {"value": n / (ms_plain / 1e3), "ms_per_step": ms_plain, "omega": wl["omega"],
+                              "red_black_iterations": lp.iterations, "residual_checked": lp.residual},
+                    "refined": {"value": n / (ms_ref / 1e3), "ms_per_step": ms_ref, "omega": wl["omega_refined"],
+                                "inner_iterations": wl["inner"], "red_black_iterations": lr.iterations,
+                                "residual": lr.residual}}
+
+    # ---- the timed form ----
+    if mixed:
+        def to_dev(d):
+            out = {}
+            for k, a in d.items():
+                t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+                out[k] = (t.to(torch.bfloat16) if k == "velocity" else t.to(torch.float16)).reshape(-1).contiguous()
+            return out
+
+        cur = to_dev(fields)
+        bufs = [cur, {k: torch.empty_like(v) for k, v in cur.items()}]
+        src = to_dev({"fuel": sources["src_fuel"], "temperature": sources["src_temperature"]})
+
+        def mdesc(outer):
+            return hl.MixedDesc(dt=0.0, omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
+                                inner_iterations=wl["inner"], flags=0)
+
+        torch.cuda.synchronize()
+        try:
+            info = g.advance_mixed(bufs[0], bufs[1], src, dt, params, model, mdesc(60), info=True)
+        except hl.HnsError as e:
+            if e.status != 6:
+                raise
+            info = g.last_refine()
+        outer = max(1, info.iterations // wl["inner"]) + 2
+        st = mdesc(outer)
+        ms_state = [0]
+
+        def step():
+            s0 = ms_state[0]
+            g.advance_mixed(bufs[s0], bufs[1 - s0], src, dt, params, model, st)
+            ms_state[0] = 1 - s0
+
+        # record packing, velocity advection, confinement, divergence/burn/buoyancy, first residual,
+        # convergence log, gradient, scalar advection; per outer iteration scale, 2 half-sweeps per
+        # inner iteration, update, residual.
+        launches_per_step = 8 + outer * (3 + 2 * wl["inner"])
+        kernel_bytes, kernel_name, phase = 3, "rbgs_split_half_kernel (FP16 inner solve, colour-split, one colour per launch)", "inner"
+    else:
+        load_fp32()
+        iters = wl["iterations"]
+        outer = None
+
+        def step():
+            g.advance(iters, dt, params, model)
+
+        # velocity advection, confinement and sources, divergence/burn/buoyancy, the red-black
+        # iterations, gradient, scalar advection.
+        launches_per_step = 5 + iters
+        kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_stream_kernel<float>", "solve"
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    replicas.barrier(R)
+    clocks = ClockSampler(local)
+    clocks.start()
+    g.profile_read()
+    g.profile_enable(True)
+    g.solve_log(capacity=0, reset=True)
+    ms = _timed_steps(torch, stream, step, args.steps)
+    replicas.barrier(R)
+    clk = clocks.stop()
+    g.profile_enable(False)
+    prof = g.profile_read()
+    logged, entries = g.solve_log(capacity=args.steps, reset=True)
+    worst = max((e.residual for e in entries), default=None)
+    ms = replicas.max_over_ranks(R, ms, dev)
+    value = replicas.aggregate_rate(R, n, args.steps, ms)
+    k_ms = prof.phase_ms[hl.PHASES[phase]] / max(1, prof.solver_launches)
+    peak, peak_kind = measured_peak_gbs()
+    achieved = kernel_bytes * n / (k_ms / 1e3) / 1e9
+
+    # End to end through the C ABI with FP32 host buffers (pinned).
+    e2e_steps = max(1, min(args.steps, 3))
+    hf = {k: torch.from_numpy(np.ascontiguousarray(v.reshape(-1))).pin_memory().numpy() for k, v in fields.items()}
+    hs = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy() for k, v in sources.items()}
+    if mixed:
+        hsrc = {"fuel": hs["src_fuel"], "temperature": hs["src_temperature"]}
+        run_host = lambda: g.advance_mixed_host(hf, hsrc, dt, params, model, st)  # noqa: E731
+        h2d = (12 + 4 * 4 + 2 * 4) * n
+        d2h = (12 + 4 * 4) * n
+        path = "hns_advance_mixed_host (C ABI, pinned FP32 host buffers: fields and sources up, fields down)"
+    else:
+        def run_host():
+            for k, a in hs.items():
+                g.field_set(k, a)
+            g.advance(wl["iterations"], dt, params, model)
+            for k in fields:
+                g.field_get(k, out=hf[k])
+        h2d = 2 * 4 * n
+        d2h = (12 + 4 * 4) * n
+        path = ("hns_field_set of the sources, hns_advance_model, hns_field_get of every field (the reference's "
+                "per-cook HNS_UploadSources / HNS_Advance / HNS_DownloadForOutput crossing)")
+    run_host()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        run_host()
+    e2e_s = replicas.max_over_ranks(R, (time.perf_counter() - t0) / e2e_steps, dev)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        iters_cpu = wl["iterations"] if not mixed else (fp32["plain"]["red_black_iterations"] if fp32 else cap32)
+        v, sample, cores, cpu_name, library = fire_cpu_sample(args, wl, iters_cpu, wl.get("omega", 0.0), 3, 0,
+                                                              budget_s=20.0)
+        cpu = {"value": v, "unit": "voxel-steps/s", "cores": cores, "kind": "reference", "sample": sample,
+               "cpu": cpu_name}
+
+    if rank == 0:
+        phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
+        det = {"precision": args.precision, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+               "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
+               "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
+               "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
+               "timed_solves_logged": logged, "worst_residual_timed_steps": worst,
+               "timed_steps_above_tolerance": (sum(1 for e in entries if e.residual > tol) if tol else None)}
+        if mixed:
+            det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+                        "omega_inner": wl["omega_refined"], "inner_iterations": wl["inner"], "outer_cap": outer})
+        else:
+            det.update({"red_black_iterations": wl["iterations"], "omega": "2/(1+sin(3.14159 dx)) (the reference's)"})
+        line = {
+            "metric": "active voxel-steps/s", "value": value, "unit": "voxel-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 arithmetic; bf16/f16 storage, f64 refinement" if mixed else "f32", "data": "synthetic",
+            "config": fire_config(args, wl, origins), "details": det,
+            "roofline": {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes_per_launch": kernel_bytes * n, "launch_ms": k_ms,
+                         "launches_timed": int(prof.solver_launches)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps, "path": path},
+            "gpu_launches": args.steps * launches_per_step,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    replicas.finish(R)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="shell512")
-    ap.add_argument("--precision", choices=["mixed", "fp32"], default="mixed")
+    ap.add_argument("--workload", choices=sorted(set(WORKLOADS) | set(FIRE_WORKLOADS)), default="shell512")
+    ap.add_argument("--forces", action="store_true",
+                    help="the fire step (HNS_Advance with the configurations' forces) instead of the SOP chain; "
+                         "implied by fire1024")
+    ap.add_argument("--precision", choices=["mixed", "fp32"], default=None,
+                    help="mixed (default for the SOP chain and fire1024) or fp32 (default for plume256 --forces)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout measured beside the step")
     ap.add_argument("--no-fp32-comparison", action="store_true",
@@ -589,6 +905,17 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
+    fire = args.forces or args.workload not in WORKLOADS
+    if fire:
+        if args.workload not in FIRE_WORKLOADS:
+            ap.error(f"--forces has no fire workload {args.workload!r}")
+        wl = FIRE_WORKLOADS[args.workload]
+        args.precision = args.precision or wl["precision"]
+        if args.precision == "mixed" and "tolerance" not in wl:
+            ap.error("the mixed fire step solves to a tolerance; this workload runs a fixed iteration count")
+        (reference_arm_fire if args.impl == "reference" else ours_fire)(args, wl)
+        return
+    args.precision = args.precision or "mixed"
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         reference_arm(args, wl)

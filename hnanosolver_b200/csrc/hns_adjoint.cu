@@ -565,7 +565,6 @@ void launch_adj_confinement(const Context& c, const float* vel, const float* out
 // ---- C ABI -----------------------------------------------------------------------------------
 
 namespace hns {
-namespace {
 
 // The adjoint of `iterations` red-black iterations from p = 0 (the forward's
 // HNS_SOLVE_ZERO_INIT): the half-sweeps' transposes in reverse order, black first, in place on
@@ -587,6 +586,8 @@ void adj_rbgs(Context& c, const float* p_bar, float* div_bar, int iterations, fl
             scale[colour] *= 1.f - omega;
         }
 }
+
+namespace {
 
 // vel_bar (the adjoint of the projected velocity) -> the adjoint of the velocity before the
 // projection: vel_bar - D^T M^T G^T vel_bar, accumulated in place.

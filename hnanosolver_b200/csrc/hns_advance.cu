@@ -174,6 +174,34 @@ unsigned leaf_blocks(const Context& c) { return (unsigned)(c.topo.num_leaves * 2
 
 }  // namespace
 
+void launch_div_combust_buoy(const Context& c, const float* vel, float* vel_out, float* div, float* fuel, float* waste,
+                             float* temp, float* flame, const float* density, const hns_combustion_params& P,
+                             const hns_force_model& M, float dt) {
+    const Burn B{P.temperatureRelease, P.expansionRate, M.burn_rate, M.heat_release, M.ignition_temp, M.density_buoyancy};
+    const float inv_dx = 1.0f / c.dx;
+    if (M.combustion == HNS_COMBUSTION_OXYGEN)
+        div_combust_buoy_kernel<HNS_COMBUSTION_OXYGEN><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+            c.topo.view, vel, vel_out, div, inv_dx, fuel, waste, temp, flame, density, B, dt, P.ambientTemp,
+            P.buoyancyStrength);
+    else if (M.combustion == HNS_COMBUSTION_RATE)
+        div_combust_buoy_kernel<HNS_COMBUSTION_RATE><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+            c.topo.view, vel, vel_out, div, inv_dx, fuel, waste, temp, flame, density, B, dt, P.ambientTemp,
+            P.buoyancyStrength);
+    else
+        div_combust_buoy_kernel<HNS_COMBUSTION_NONE><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+            c.topo.view, vel, vel_out, div, inv_dx, fuel, waste, temp, flame, density, B, dt, P.ambientTemp,
+            P.buoyancyStrength);
+    HNS_LAUNCHED();
+}
+
+void launch_confine_sources(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale,
+                            const float* src_v3, float gravity) {
+    confine_sources_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, out, dt, 1.0f / c.dx, scale,
+                                                                       (int)factor_scale, src_v3, nullptr, nullptr,
+                                                                       nullptr, gravity, ScalarSources{});
+    HNS_LAUNCHED();
+}
+
 void check_force_model(const hns_force_model& m) {
     if (m.combustion != HNS_COMBUSTION_OXYGEN && m.combustion != HNS_COMBUSTION_RATE && m.combustion != HNS_COMBUSTION_NONE)
         fail(HNS_ERR_INVALID_ARG, "unknown combustion model " + std::to_string(m.combustion));
@@ -208,7 +236,8 @@ Field& Context::ensure_field(const std::string& name, int components, bool zero)
     return *f;
 }
 
-void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& P, const hns_force_model& M) {
+void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& P, const hns_force_model& M,
+                 const hns_step_desc* solve, hns_solve_info* info) {
     const size_t n = (size_t)c.num_voxels();
     const float dx = c.dx;
     const float inv_dx = 1.0f / dx;
@@ -238,10 +267,13 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
     float* div = c.scratch_f32("advance_div", n);
     float* p = c.scratch_f32("advance_p", n);
     const float omega = 2.0f / (1.0f + sinf(3.14159f * dx));  // host sinf, as :365
+    const float solve_omega = (solve != nullptr && solve->omega > 0.f) ? solve->omega : omega;
     // A collider: the "collision_sdf" field (HNS_EnsureContext stores it when the SOP has one,
     // :121-133), enforced on the velocity before the substeps (:241-244).
     Field* sdff = c.find_field("collision_sdf");
     const float* sdf = (sdff && sdff->components == 1) ? sdff->buf.as<float>() : nullptr;
+    if (sdf && solve != nullptr && (solve->flags & HNS_SOLVE_REFINE))
+        fail(HNS_ERR_UNSUPPORTED, "the refined solve of the step does not take a collider");
     if (sdf) launch_collision_enforce(c, c.find_field(vel_name)->buf.as<float>(), sdf);
 
     for (int s = 0; s < subs; ++s) {
@@ -283,36 +315,50 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
         float* temp = c.ensure_field("temperature", 1, true).buf.as<float>();
         float* flame = oxygen ? c.ensure_field("flame", 1, true).buf.as<float>() : nullptr;
         const float* dens = M.density_buoyancy != 0.0f ? c.ensure_field("density", 1, true).buf.as<float>() : nullptr;
-        const Burn B{P.temperatureRelease, P.expansionRate, M.burn_rate, M.heat_release, M.ignition_temp,
-                     M.density_buoyancy};
-        if (M.combustion == HNS_COMBUSTION_OXYGEN)
-            div_combust_buoy_kernel<HNS_COMBUSTION_OXYGEN><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-                c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, dens, B, dt_sub, P.ambientTemp,
-                P.buoyancyStrength);
-        else if (M.combustion == HNS_COMBUSTION_RATE)
-            div_combust_buoy_kernel<HNS_COMBUSTION_RATE><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-                c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, dens, B, dt_sub, P.ambientTemp,
-                P.buoyancyStrength);
-        else
-            div_combust_buoy_kernel<HNS_COMBUSTION_NONE><<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-                c.topo.view, adv2, adv3, div, inv_dx, fuel, waste, temp, flame, dens, B, dt_sub, P.ambientTemp,
-                P.buoyancyStrength);
-        HNS_LAUNCHED();
+        launch_div_combust_buoy(c, adv2, adv3, div, fuel, waste, temp, flame, dens, P, M, dt_sub);
         c.phase_end();
 
         c.phase_begin(HNS_PHASE_SOLVE);
-        rbgs_solve(c, div, p, iterations, omega, HNS_SOLVE_ZERO_INIT);
+        const bool refined = solve != nullptr && (solve->flags & HNS_SOLVE_REFINE);
+        double* p64 = refined ? reinterpret_cast<double*>(c.scratch_f32("refine_p", 2 * n)) : nullptr;
+        // The solve: `iterations` red-black iterations (the reference), or the step
+        // description's solve to its tolerance (checked red-black SOR, or the FP32 refinement).
+        auto pressure_solve = [&](int its) {
+            if (solve == nullptr) {
+                rbgs_solve(c, div, p, its, omega, HNS_SOLVE_ZERO_INIT);
+            } else if (refined) {
+                c.last_refine = refine_solve<float>(c, div, p64, solve->max_outer > 0 ? solve->max_outer : 8,
+                                                    solve->inner_iterations > 0 ? solve->inner_iterations : 60,
+                                                    solve_omega, solve->tolerance, solve->flags);
+            } else {
+                c.last_solve = rbgs_solve_checked(c, div, p, solve->max_iterations, solve_omega, HNS_SOLVE_ZERO_INIT,
+                                                  solve->tolerance, solve->check_every);
+            }
+        };
+        pressure_solve(iterations);
         if (P.disturbanceEnable > 0.0f) {
             // The disturbance injection is commented out in the reference; what remains is a
             // second, shorter solve of the divergence without the expansion (:377-403).
             launch_divergence(c, adv3, div);
-            rbgs_solve(c, div, p, std::max(2, iterations / 2), omega, HNS_SOLVE_ZERO_INIT);
+            pressure_solve(std::max(2, iterations / 2));
         }
         c.phase_end();
         c.phase_begin(HNS_PHASE_GRADIENT);
-        vel = c.find_field(vel_name)->buf.as<float>();
-        launch_subtract_gradient(c, adv3, p, vel, sdf);
-        if (sdf) launch_collision_enforce(c, vel, sdf);  // :411-414
+        if (refined) {
+            // u = adv3 - grad p with the FP64 pressure, in place on adv3, whose buffer then
+            // becomes the velocity field's (the old velocity buffer is the next adv3).
+            DeviceBuffer& a3 = c.scratch["advance_adv3"];
+            Field* vf = c.find_field(vel_name);
+            if (a3.bytes != vf->buf.bytes) fail(HNS_ERR_CUDA, "velocity and step buffers differ in size");
+            launch_gradient_f64(c, adv3, p64);
+            std::swap(vf->buf, a3);
+            adv3 = a3.as<float>();
+            vel = vf->buf.as<float>();
+        } else {
+            vel = c.find_field(vel_name)->buf.as<float>();
+            launch_subtract_gradient(c, adv3, p, vel, sdf);
+            if (sdf) launch_collision_enforce(c, vel, sdf);  // :411-414
+        }
         c.phase_end();
 
         if (!adv_names.empty()) {
@@ -331,6 +377,20 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
             for (const auto& name : adv_names) std::swap(c.find_field(name)->buf, c.scratch["advance_twin:" + name]);
             c.phase_end();
         }
+    }
+    if (info && solve != nullptr) {
+        // The last solve of the call (the one whose pressure made the velocity).
+        int its = 0;
+        double res = 0.0;
+        if (solve->flags & HNS_SOLVE_REFINE) {
+            refine_result(c, c.last_refine, &its, &res);
+            its *= c.last_refine.inner;
+        } else {
+            solve_result(c, c.last_solve, &its, &res);
+        }
+        info->iterations = its;
+        info->residual = res;
+        info->initial_residual = 1.0;
     }
 }
 
@@ -427,8 +487,31 @@ HNS_API hns_status hns_advance_model(hns_ctx* ctx, int iterations, float dt, con
         const hns_force_model M = model ? *model : hns_force_model{};
         check_force_model(M);
         DeviceGuard g(c->device);
-        run_advance(*c, iterations, dt, *params, M);
+        run_advance(*c, iterations, dt, *params, M, nullptr, nullptr);
     });
+}
+
+HNS_API hns_status hns_advance_solve(hns_ctx* ctx, float dt, const hns_combustion_params* params,
+                                     const hns_force_model* model, const hns_step_desc* solve, hns_solve_info* info) {
+    hns_status st = HNS_OK;
+    const hns_status g = guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!params || !solve) fail(HNS_ERR_INVALID_ARG, "null params or solve description");
+        if (!(solve->tolerance > 0.0) || !std::isfinite(solve->tolerance))
+            fail(HNS_ERR_INVALID_ARG, "the solve needs a positive tolerance");
+        if (!(solve->flags & HNS_SOLVE_REFINE) && solve->max_iterations <= 0)
+            fail(HNS_ERR_INVALID_ARG, "the solve needs a positive iteration cap");
+        if (solve->flags & ~(unsigned)(HNS_SOLVE_REFINE | HNS_SOLVE_ZERO_INIT))
+            fail(HNS_ERR_UNSUPPORTED, "solve flags other than HNS_SOLVE_REFINE are not supported by this step");
+        const hns_force_model M = model ? *model : hns_force_model{};
+        check_force_model(M);
+        DeviceGuard dg(c->device);
+        run_advance(*c, 0, dt, *params, M, solve, info);
+        if (info && info->residual > solve->tolerance)
+            st = record_error(HNS_ERR_NOT_CONVERGED, "pressure solve stopped after " + std::to_string(info->iterations) +
+                                                         " iterations with residual " + std::to_string(info->residual));
+    });
+    return g != HNS_OK ? g : st;
 }
 
 HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out) {

@@ -459,4 +459,59 @@ HNS_API hns_status hns_advance_mixed(hns_ctx* ctx, const hns_fire_fields* in, co
     return g != HNS_OK ? g : st;
 }
 
+HNS_API hns_status hns_advance_mixed_host(hns_ctx* ctx, const hns_fire_f32* fields, const hns_fire_sources_f32* sources,
+                                          float dt, const hns_combustion_params* params, const hns_force_model* model,
+                                          const hns_mixed_desc* solve, hns_solve_info* info) {
+    hns_status st = HNS_OK;
+    const hns_status g = guarded([&] {
+        Context* c = check_ctx(ctx);
+        if (!fields || !fields->velocity) fail(HNS_ERR_INVALID_ARG, "null host fields");
+        DeviceGuard dg(c->device);
+        const size_t n = (size_t)c->num_voxels();
+        float* host[6] = {fields->velocity, fields->density, fields->temperature, fields->fuel, fields->waste, fields->flame};
+        static const char* names[6] = {"velocity", "density", "temperature", "fuel", "waste", "flame"};
+        float* stage = c->scratch_f32("fire_host_stage", 3 * n);
+        hns_fire_fields in{}, out{};
+        void** pin[6] = {&in.velocity, &in.density, &in.temperature, &in.fuel, &in.waste, &in.flame};
+        void** pout[6] = {&out.velocity, &out.density, &out.temperature, &out.fuel, &out.waste, &out.flame};
+        // Upload each host field in FP32 and convert it to its storage type (BF16 velocity,
+        // FP16 scalars) in solver-owned arrays.
+        for (int q = 0; q < 6; ++q) {
+            if (!host[q]) continue;
+            const size_t cnt = q == 0 ? 3 * n : n;
+            const int dt_store = q == 0 ? HNS_DTYPE_BF16 : HNS_DTYPE_F16;
+            *pin[q] = c->scratch_f32(std::string("fire_host_in_") + names[q], (cnt + 1) / 2);
+            *pout[q] = c->scratch_f32(std::string("fire_host_out_") + names[q], (cnt + 1) / 2);
+            HNS_CUDA(cudaMemcpyAsync(stage, host[q], cnt * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+            convert_array(*c, stage, HNS_DTYPE_F32, *pin[q], dt_store, (int64_t)cnt);
+        }
+        hns_fire_sources src{};
+        if (sources) {
+            const float* hs[4] = {sources->velocity, sources->temperature, sources->density, sources->fuel};
+            const void** ps[4] = {&src.velocity, &src.temperature, &src.density, &src.fuel};
+            static const char* sn[4] = {"velocity", "temperature", "density", "fuel"};
+            for (int q = 0; q < 4; ++q) {
+                if (!hs[q]) continue;
+                const size_t cnt = q == 0 ? 3 * n : n;
+                void* dst = c->scratch_f32(std::string("fire_host_src_") + sn[q], (cnt + 1) / 2);
+                HNS_CUDA(cudaMemcpyAsync(stage, hs[q], cnt * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+                convert_array(*c, stage, HNS_DTYPE_F32, dst, q == 0 ? HNS_DTYPE_BF16 : HNS_DTYPE_F16, (int64_t)cnt);
+                *ps[q] = dst;
+            }
+        }
+        st = hns_advance_mixed(ctx, &in, &out, &src, dt, params, model, solve, info);
+        if (st != HNS_OK && st != HNS_ERR_NOT_CONVERGED) fail(st, hns_last_error());
+        // Convert back to FP32 and download in place.
+        for (int q = 0; q < 6; ++q) {
+            if (!host[q]) continue;
+            const size_t cnt = q == 0 ? 3 * n : n;
+            convert_array(*c, *pout[q], q == 0 ? HNS_DTYPE_BF16 : HNS_DTYPE_F16, stage, HNS_DTYPE_F32, (int64_t)cnt);
+            HNS_CUDA(cudaMemcpyAsync(host[q], stage, cnt * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+        }
+        HNS_CUDA(cudaStreamSynchronize(c->stream));
+        if (st == HNS_ERR_NOT_CONVERGED) fail(st, "refined solve above the tolerance");
+    });
+    return g != HNS_OK ? g : st;
+}
+
 }  // extern "C"

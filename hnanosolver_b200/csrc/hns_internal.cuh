@@ -165,6 +165,9 @@ struct Context {
     bool profiling = false;
     int rbgs_kernel = HNS_RBGS_BULK;      // hns_set_option(HNS_OPT_RBGS_KERNEL)
     int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
+    int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
+    bool l2_resident = false;            // hns_set_option(HNS_OPT_L2_RESIDENT)
+    size_t l2_setaside = 0;              // persisting L2 bytes set aside for this context's device
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -267,8 +270,10 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
 void launch_split_face_table(const Context& c, int* nb8);
 // short_grid: one wave of CTAs looping over the leaves, for a launch expected to find the
 // refinement converged and return at once.
+// window: an L2 access-policy window for the launch (HNS_OPT_L2_RESIDENT), or null.
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
-                            float omega, const double* check, double tol2, bool short_grid = false);
+                            float omega, const double* check, double tol2, bool short_grid = false,
+                            const cudaAccessPolicyWindow* window = nullptr);
 void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
                              void* e_out, void* faces_out, float omega, const double* check, double tol2);
 
@@ -286,6 +291,8 @@ void launch_adj_rbgs_colour(const Context& c, float* lam, float* div_bar, int co
 void launch_adj_confinement(const Context& c, const float* vel, const float* out_bar, float* vel_bar, float dt,
                             float scale, float factor_scale);
 void launch_adj_accumulate(const Context& c, const float* src, float* dst, int64_t n);
+// div_bar += M^T p_bar for `iterations` red-black iterations from p = 0 (p = M div).
+void adj_rbgs(Context& c, const float* p_bar, float* div_bar, int iterations, float omega);
 
 // ---- mixed precision and refinement (hns_mixed.cu) ----
 void convert_array(const Context& c, const void* src, int src_dt, void* dst, int dst_dt, int64_t n);
@@ -302,8 +309,19 @@ void launch_gradient_mixed(const Context& c, void* vel, const double* p);
 void launch_gradient_f64(const Context& c, float* vel, const double* p);
 
 // HNS_Advance over the context's fields with a force model (hns_advance.cu).
-void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& params, const hns_force_model& model);
+// solve: null runs `iterations` red-black iterations per solve (the reference); otherwise each
+// solve runs to solve->tolerance (checked SOR, or the FP32 refinement with HNS_SOLVE_REFINE) and,
+// with info, the last solve's result is reported (synchronizes).
+void run_advance(Context& c, int iterations, float dt, const hns_combustion_params& params, const hns_force_model& model,
+                 const hns_step_desc* solve, hns_solve_info* info);
 void check_force_model(const hns_force_model& m);
+// The step's force kernels (hns_advance.cu): confinement + velocity source + gravity, vel -> out;
+// divergence + burn (in place on its fields) + buoyancy, vel -> vel_out.
+void launch_confine_sources(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale,
+                            const float* src_v3, float gravity);
+void launch_div_combust_buoy(const Context& c, const float* vel, float* vel_out, float* div, float* fuel, float* waste,
+                             float* temp, float* flame, const float* density, const hns_combustion_params& P,
+                             const hns_force_model& M, float dt);
 
 // Runs `iterations` fused RBGS iterations from `p` (or zero) and leaves the result in `p`.
 void rbgs_solve(Context& c, const float* div, float* p, int iterations, float omega, unsigned flags);

@@ -279,7 +279,8 @@ template <typename T>
 __global__ void __launch_bounds__(NT, kMinBlocksPerSM)
     rbgs_stream_kernel(TopoView t, const T* __restrict__ rhs, const T* __restrict__ p_in, T* __restrict__ p_out,
                        float dx2, float omega, const double* __restrict__ check, double tol2,
-                       double* __restrict__ resid_out, unsigned long long* __restrict__ counters) {
+                       double* __restrict__ resid_out, unsigned long long* __restrict__ counters,
+                       uint32_t first_polls) {
     __shared__ Stage<T> st[2];
     __shared__ double red[2][NT / 32];
     __shared__ int ok;
@@ -349,10 +350,11 @@ __global__ void __launch_bounds__(NT, kMinBlocksPerSM)
         __syncthreads();
         if (next < L) stage_issue(nxt, cp, tid);
         // One thread waits for the current stage (sleeping between polls); the others wait at
-        // the CTA barrier.
+        // the CTA barrier. first_polls bounds this first wait (kMaxPolls unless a test lowers it
+        // to make the wait give up); the drain waits below keep kMaxPolls.
         if (tid == 0) {
             const uint32_t parity = (i >> 1) & 1;
-            if (!ptx::mbar_wait_bounded_sleep(&cur.bar, parity, kMaxPolls, kSuspendNs)) {
+            if (!ptx::mbar_wait_bounded_sleep(&cur.bar, parity, first_polls, kSuspendNs)) {
                 // The copies did not land in time: flag it, and give them and the next stage's
                 // copies a second bounded wait so that no copy is still writing when the CTA's
                 // shared memory is released. p_out keeps its old values for the leaves left.
@@ -457,8 +459,9 @@ template <typename T>
 void launch_stream(const Context& c, const T* rhs, const T* p_in, T* p_out, float dx2, float omega,
                    const double* check, double tol2, double* resid_out) {
     if (c.topo.num_leaves <= 0) return;
+    const uint32_t first_polls = c.first_wait_polls < 0 ? kMaxPolls : (uint32_t)c.first_wait_polls;
     rbgs_stream_kernel<T><<<stream_grid<T>(c), NT, 0, c.stream>>>(c.topo.view, rhs, p_in, p_out, dx2, omega, check, tol2,
-                                                                 resid_out, c.counters);
+                                                                 resid_out, c.counters, first_polls);
     HNS_LAUNCHED();
 }
 

@@ -202,7 +202,8 @@ void launch_split_face_table(const Context& c, int* nb8) {
 }
 
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
-                            float omega, const double* check, double tol2, bool short_grid) {
+                            float omega, const double* check, double tol2, bool short_grid,
+                            const cudaAccessPolicyWindow* window) {
     const int64_t L = c.topo.num_leaves;
     if (L == 0) return;
     if (L >= (int64_t(1) << 22)) fail(HNS_ERR_INVALID_ARG, "too many leaves for the colour-split inner solve");
@@ -213,9 +214,24 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     if (short_grid) blocks = std::min(blocks, (unsigned)(c.sm_count() * kShortGridCtasPerSm));
     const auto* r = static_cast<const __half*>(rhs);
     auto* x = static_cast<__half*>(e);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[2];
+    unsigned na = 0;
+    if (window != nullptr) {
+        // The inner solve's arrays kept in the L2 set-aside across half-sweeps.
+        attr[na].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[na].val.accessPolicyWindow = *window;
+        ++na;
+    }
     if (e_zero) {
-        rbgs_split_half_kernel<true><<<blocks, kThreads, 0, c.stream>>>(nb8, r, x, (int)L, colour, omega, check, tol2,
-                                                                         c.counters);
+        cfg.attrs = attr;
+        cfg.numAttrs = na;
+        HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<true>, nb8, r, x, (int)L, colour, omega, check, tol2,
+                                    c.counters));
         HNS_LAUNCHED();
         return;
     }
@@ -223,16 +239,11 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     // and the right-hand side) overlaps the tail of the preceding half-sweep, and e is read after
     // griddepcontrol.wait. The caller guarantees that the preceding kernel on the stream is a
     // half-sweep and that rhs, nb8 and check were written before it started.
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = c.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[na].val.programmaticStreamSerializationAllowed = 1;
+    ++na;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = na;
     HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<false>, nb8, r, x, (int)L, colour, omega, check, tol2,
                                 c.counters));
     HNS_LAUNCHED();

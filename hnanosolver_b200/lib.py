@@ -23,6 +23,8 @@ OPT_RBGS_KERNEL = 1
 RBGS_PLAIN, RBGS_BULK = 0, 1
 OPT_INNER_LAYOUT = 2
 INNER_ROWS, INNER_PACKED, INNER_SPLIT = 0, 1, 2
+OPT_WAIT_POLLS = 3
+OPT_L2_RESIDENT = 4
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 
@@ -80,6 +82,16 @@ class FireFields(ctypes.Structure):
 
 
 class FireSources(ctypes.Structure):
+    _fields_ = [(k, _p) for k in FIRE_SOURCES]
+
+
+class FireF32(ctypes.Structure):
+    """hns_fire_f32: FP32 arrays (host or device pointers by use; None: absent)."""
+
+    _fields_ = [(k, _p) for k in FIRE_FIELDS]
+
+
+class FireSourcesF32(ctypes.Structure):
     _fields_ = [(k, _p) for k in FIRE_SOURCES]
 
 
@@ -153,6 +165,17 @@ def _load():
     _sig(lib, "hns_advance", _i, _p, _i, _f, ctypes.POINTER(CombustionParams))
     _sig(lib, "hns_advance_model", _i, _p, _i, _f, ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel))
     _sig(lib, "hns_active_mask", _i, _p, _p)
+    _sig(lib, "hns_adjoint_advance", _i, _p, ctypes.POINTER(FireF32), ctypes.POINTER(FireSourcesF32),
+         ctypes.POINTER(FireF32), ctypes.POINTER(FireF32), _f, _i, ctypes.POINTER(CombustionParams),
+         ctypes.POINTER(ForceModel))
+    _sig(lib, "hns_adjoint_advance_mixed", _i, _p, ctypes.POINTER(FireFields), ctypes.POINTER(FireSources),
+         ctypes.POINTER(FireF32), ctypes.POINTER(FireF32), _f, ctypes.POINTER(CombustionParams),
+         ctypes.POINTER(ForceModel), ctypes.POINTER(MixedDesc))
+    _sig(lib, "hns_advance_solve", _i, _p, _f, ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel),
+         ctypes.POINTER(StepDesc), ctypes.POINTER(SolveInfo))
+    _sig(lib, "hns_advance_mixed_host", _i, _p, ctypes.POINTER(FireF32), ctypes.POINTER(FireSourcesF32), _f,
+         ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel), ctypes.POINTER(MixedDesc),
+         ctypes.POINTER(SolveInfo))
     _sig(lib, "hns_advance_mixed", _i, _p, ctypes.POINTER(FireFields), ctypes.POINTER(FireFields),
          ctypes.POINTER(FireSources), _f, ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel),
          ctypes.POINTER(MixedDesc), ctypes.POINTER(SolveInfo))
@@ -340,10 +363,16 @@ class Grid:
         check(lib.hns_field_set(self._h, name.encode(), components or 1,
                                 None if data is None else data.ctypes.data, 0))
 
-    def field_get(self, name: str) -> np.ndarray:
+    def field_get(self, name: str, out: np.ndarray | None = None) -> np.ndarray:
+        """Copy of a field into a new host array, or into `out` (contiguous float32 of the
+        field's size)."""
         ptr, comps = _p(), _i()
         check(lib.hns_field_ptr(self._h, name.encode(), ctypes.byref(ptr), ctypes.byref(comps)))
-        out = np.zeros((self.num_voxels, 3) if comps.value == 3 else self.num_voxels, np.float32)
+        size = self.num_voxels * comps.value
+        if out is None:
+            out = np.zeros((self.num_voxels, 3) if comps.value == 3 else self.num_voxels, np.float32)
+        elif out.dtype != np.float32 or not out.flags.c_contiguous or out.size != size:
+            raise ValueError(f"out must be contiguous float32 with {size} values")
         check(lib.hns_field_get(self._h, name.encode(), out.ctypes.data, 0))
         return out
 
@@ -377,6 +406,50 @@ class Grid:
                                     ctypes.byref(params), ctypes.byref(model) if model is not None else None,
                                     ctypes.byref(desc), ctypes.byref(si) if info else None))
         return si if info else None
+
+    def advance_solve(self, dt: float, params: CombustionParams, model: ForceModel | None, desc: StepDesc,
+                      info: bool = False):
+        """hns_advance_solve: the all-in-one step with each solve run to desc.tolerance."""
+        si = SolveInfo()
+        check(lib.hns_advance_solve(self._h, dt, ctypes.byref(params),
+                                    ctypes.byref(model) if model is not None else None, ctypes.byref(desc),
+                                    ctypes.byref(si) if info else None))
+        return si if info else None
+
+    def advance_mixed_host(self, fields: dict, sources: dict | None, dt: float, params: CombustionParams,
+                           model: ForceModel | None, desc: MixedDesc, info: bool = False):
+        """hns_advance_mixed_host: `fields` maps FIRE_FIELDS names to contiguous float32 host
+        arrays, updated in place; `sources` maps FIRE_SOURCES names to float32 host arrays."""
+        for a in list(fields.values()) + list((sources or {}).values()):
+            if a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("host fields must be contiguous float32")
+        fh = FireF32(*[fields[k].ctypes.data if k in fields else None for k in FIRE_FIELDS])
+        src = FireSourcesF32(*[(sources or {})[k].ctypes.data if k in (sources or {}) else None for k in FIRE_SOURCES])
+        si = SolveInfo()
+        check(lib.hns_advance_mixed_host(self._h, ctypes.byref(fh), ctypes.byref(src), dt, ctypes.byref(params),
+                                         ctypes.byref(model) if model is not None else None, ctypes.byref(desc),
+                                         ctypes.byref(si) if info else None))
+        return si if info else None
+
+    def adjoint_advance(self, fields_in: dict, sources: dict | None, out_bar: dict, in_bar: dict, dt: float,
+                        iterations: int, params: CombustionParams, model: ForceModel | None):
+        """hns_adjoint_advance on FP32 device tensors (dicts keyed by FIRE_FIELDS / FIRE_SOURCES)."""
+        f = lambda d, cls, keys: cls(*[_dptr((d or {}).get(k)) for k in keys])  # noqa: E731
+        check(lib.hns_adjoint_advance(self._h, ctypes.byref(f(fields_in, FireF32, FIRE_FIELDS)),
+                                      ctypes.byref(f(sources, FireSourcesF32, FIRE_SOURCES)),
+                                      ctypes.byref(f(out_bar, FireF32, FIRE_FIELDS)),
+                                      ctypes.byref(f(in_bar, FireF32, FIRE_FIELDS)), dt, iterations,
+                                      ctypes.byref(params), ctypes.byref(model) if model is not None else None))
+
+    def adjoint_advance_mixed(self, fields_in: dict, sources: dict | None, out_bar: dict, in_bar: dict, dt: float,
+                              params: CombustionParams, model: ForceModel | None, desc: MixedDesc):
+        """hns_adjoint_advance_mixed: BF16/FP16 inputs and sources, FP32 adjoints."""
+        f = lambda d, cls, keys: cls(*[_dptr((d or {}).get(k)) for k in keys])  # noqa: E731
+        check(lib.hns_adjoint_advance_mixed(self._h, ctypes.byref(f(fields_in, FireFields, FIRE_FIELDS)),
+                                            ctypes.byref(f(sources, FireSources, FIRE_SOURCES)),
+                                            ctypes.byref(f(out_bar, FireF32, FIRE_FIELDS)),
+                                            ctypes.byref(f(in_bar, FireF32, FIRE_FIELDS)), dt, ctypes.byref(params),
+                                            ctypes.byref(model) if model is not None else None, ctypes.byref(desc)))
 
     def active_mask(self) -> np.ndarray:
         out = np.zeros(self.num_voxels, np.uint8)

@@ -365,6 +365,42 @@ HNS_API hns_status hns_advance_mixed(hns_ctx* ctx, const hns_fire_fields* in, co
                                      const hns_fire_sources* sources, float dt, const hns_combustion_params* params,
                                      const hns_force_model* model, const hns_mixed_desc* solve, hns_solve_info* info);
 
+/* hns_advance_model with each pressure solve run to a tolerance instead of a fixed iteration
+ * count: solve->tolerance (> 0), and either plain red-black SOR checked every check_every
+ * iterations up to max_iterations, or (flags HNS_SOLVE_REFINE) the FP64 iterative refinement
+ * around FP32 red-black inner solves (max_outer x inner_iterations); omega <= 0 selects
+ * 2/(1+sin(3.14159 dx)). The FP32 step the mixed-precision hns_advance_mixed is compared with
+ * at an equal residual. A collider ("collision_sdf") is supported by the plain solve only.
+ * With info the call synchronizes and reports the last solve (HNS_ERR_NOT_CONVERGED above
+ * the tolerance); every solve is appended to the convergence log. */
+HNS_API hns_status hns_advance_solve(hns_ctx* ctx, float dt, const hns_combustion_params* params,
+                                     const hns_force_model* model, const hns_step_desc* solve, hns_solve_info* info);
+
+/* The fire step's fields and sources as FP32 arrays (the reference's GridIndexedData blocks):
+ * host arrays for hns_advance_mixed_host, device arrays for the adjoints below. */
+typedef struct hns_fire_f32 {
+    float* velocity;    /* [3N] */
+    float* density;     /* [N] or NULL */
+    float* temperature; /* [N] */
+    float* fuel;        /* [N] or NULL */
+    float* waste;       /* [N] or NULL */
+    float* flame;       /* [N] or NULL */
+} hns_fire_f32;
+
+typedef struct hns_fire_sources_f32 {
+    const float* velocity;    /* [3N] or NULL */
+    const float* temperature; /* [N] or NULL */
+    const float* density;     /* [N] or NULL */
+    const float* fuel;        /* [N] or NULL */
+} hns_fire_sources_f32;
+
+/* hns_advance_mixed from FP32 HOST arrays updated in place: uploads the fields and sources,
+ * converts them to BF16/FP16 on the device, steps, converts back and downloads (synchronous).
+ * Pinned host memory makes the copies faster. */
+HNS_API hns_status hns_advance_mixed_host(hns_ctx* ctx, const hns_fire_f32* fields, const hns_fire_sources_f32* sources,
+                                          float dt, const hns_combustion_params* params, const hns_force_model* model,
+                                          const hns_mixed_desc* solve, hns_solve_info* info);
+
 /* host uint8[num_voxels]: the activity mask of the last step (the reference's
  * build_activity_mask marks every slot active, src/Cuda/Kernel.cu:75). */
 HNS_API hns_status hns_active_mask(hns_ctx* ctx, unsigned char* out);
@@ -404,6 +440,25 @@ HNS_API hns_status hns_adjoint_step_plain(hns_ctx* ctx, const float* vel_in, con
                                           const float* vel_out_bar, const float* const* scalars_out_bar, float* vel_in_bar,
                                           float* const* scalars_in_bar, float dt, int iterations, float omega);
 
+/* Adjoint of the fire step: hns_advance_model's step (one substep, no disturbance re-solve, no
+ * collider) on FP32 device arrays with `iterations` red-black iterations per solve from p = 0
+ * at HNS_Advance's omega. `in` are the step's inputs and `sources` its sources (as for the
+ * step; NULL entries add nothing); out_bar the adjoints of its outputs (NULL scalar entries:
+ * zero); in_bar receives, added, the adjoints of its inputs (zeroed by the caller; an entry
+ * for every field of `in`). The forward is recomputed inside the call. Branches (MacCormack
+ * clamps, trace cells, the burn's thresholds and minimum, T > ambient) are taken at the
+ * forward's values. The reference has no adjoint path. */
+HNS_API hns_status hns_adjoint_advance(hns_ctx* ctx, const hns_fire_f32* in, const hns_fire_sources_f32* sources,
+                                       const hns_fire_f32* out_bar, const hns_fire_f32* in_bar, float dt, int iterations,
+                                       const hns_combustion_params* params, const hns_force_model* model);
+/* The same for hns_advance_mixed's step: inputs and sources in BF16/FP16 as that step takes them,
+ * adjoints in FP32. Its solves run to solve->tolerance and are taken as exact, so the projection's
+ * transpose is one more refined solve (the Laplacian is symmetric). */
+HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields* in, const hns_fire_sources* sources,
+                                             const hns_fire_f32* out_bar, const hns_fire_f32* in_bar, float dt,
+                                             const hns_combustion_params* params, const hns_force_model* model,
+                                             const hns_mixed_desc* solve);
+
 /* ---- options ----------------------------------------------------------------------------- */
 #define HNS_OPT_RBGS_KERNEL 1 /* which red-black kernel: */
 #define HNS_RBGS_PLAIN 0      /*   plain loads into a padded halo tile */
@@ -417,6 +472,16 @@ HNS_API hns_status hns_adjoint_step_plain(hns_ctx* ctx, const float* vel_in, con
                                     one in-place launch per colour (default). All three give the
                                     same results to the bit; the solver's own arrays, never the
                                     caller's */
+#define HNS_OPT_L2_RESIDENT 4   /* 1: keep the FP16 inner solve's correction and right-hand side (2 x 2
+                                    bytes per voxel, one buffer) in the L2 across its half-sweeps: the
+                                    device's largest persisting L2 portion is set aside for this process
+                                    (released by 0) and the sweeps run under an access-policy window
+                                    over the buffer. 0 (default): plain accesses. Same results. */
+#define HNS_OPT_WAIT_POLLS 3    /* test hook of the timeout path: the poll limit of the first bounded
+                                    copy wait of the HNS_RBGS_BULK kernel (value >= 0; -1 restores the
+                                    default). 0 makes every CTA give up at its first leaf, wait for its
+                                    copies in flight with the normal limit, raise the device error flag
+                                    (hns_device_status) and return, leaving p_out unfinished. */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */

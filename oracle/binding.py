@@ -327,7 +327,7 @@ class RefOracle:
         _sig(lib, "ref_plain_step", None, _p, _p, _i64, _p, _p, _i, _f, _f, _i, _f, _p)
 
         _sig(lib, "ref_hns_advance_model", None, _p, _p, ctypes.POINTER(AdvanceFields), _f, _i, _f,
-             ctypes.POINTER(CombustionParams), _i, _f, _f, _f)
+             ctypes.POINTER(CombustionParams), _i, _f, _f, _f, _f)
 
     def grid(self, coords) -> "RefGrid":
         return RefGrid(self, coords)
@@ -452,16 +452,17 @@ class RefGrid:
 
 
     def hns_advance_model(self, velocity, scalars: dict, sources: dict, dx, iteration, dt, params: CombustionParams,
-                          combustion: int = 0, burn_rate=0.0, heat_release=0.0, ignition_temp=0.0):
+                          combustion: int = 0, burn_rate=0.0, heat_release=0.0, ignition_temp=0.0, omega=0.0):
         """The reference's HNS_Advance sequence with its `combustion` kernel in place of
-        combustion_oxygen when combustion == 1 (the reference has no density buoyancy term)."""
+        combustion_oxygen when combustion == 1 (the reference has no density buoyancy term);
+        omega > 0 replaces the solves' 2/(1+sin(3.14159 dx))."""
         vel = np.ascontiguousarray(velocity, dtype=np.float32).copy()
         sc = {k: np.ascontiguousarray(v, dtype=np.float32).copy() for k, v in scalars.items()}
         created = {k: np.zeros(self.n, np.float32) for k in MODEL_FIELDS[combustion] if k not in sc}
         src = {k: np.ascontiguousarray(v, dtype=np.float32) for k, v in sources.items()}
         f, keep = make_advance_fields(self.n, vel, sc, created, src)
         self.lib.ref_hns_advance_model(self.h, ptr(self.coords), ctypes.byref(f), dx, iteration, dt, ctypes.byref(params),
-                                       combustion, burn_rate, heat_release, ignition_temp)
+                                       combustion, burn_rate, heat_release, ignition_temp, omega)
         del keep
         return vel, sc, created
 

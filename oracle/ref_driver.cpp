@@ -313,9 +313,10 @@ static float* find_scalar(const RefAdvanceFields* f, const char* name) {
 // combustion: 0 runs combustion_oxygen (the reference's step); 1 runs the reference's
 // `combustion` kernel (Kernel.cu:568-588) with burn_rate, heat_release and ignition_temp in its
 // place, creating only fuel and temperature when absent, the sequence otherwise unchanged.
+// omega > 0 replaces HNS_Advance's 2/(1+sin(3.14159 dx)) in its red-black solves.
 void ref_hns_advance_model(void* g, const int32_t* coords, const RefAdvanceFields* F, float dx, int iteration, float dt,
                            const CombustionParams* params, int combustion_model, float burn_rate, float heat_release,
-                           float ignition_temp) {
+                           float ignition_temp, float omega_override) {
     const IndexGrid* grid = static_cast<RefGrid*>(g)->grid;
     const int64_t N = F->n;
     const float inv_dx = 1.0f / dx;
@@ -394,7 +395,7 @@ void ref_hns_advance_model(void* g, const int32_t* coords, const RefAdvanceField
         }
 
         std::fill(p.begin(), p.end(), 0.0f);
-        const float omega = 2.0f / (1.0f + sinf(3.14159f * dx));
+        const float omega = omega_override > 0.0f ? omega_override : 2.0f / (1.0f + sinf(3.14159f * dx));
         ref_rbgs(g, coords, N, div.data(), p.data(), dx, iteration, omega);
         if (params->disturbanceEnable > 0.0f) {
             launch(N, [&] { divergence(grid, cc, V(adv.data()), div.data(), inv_dx, nullptr, (size_t)N); });
@@ -422,7 +423,7 @@ void ref_hns_advance_model(void* g, const int32_t* coords, const RefAdvanceField
 
 void ref_hns_advance(void* g, const int32_t* coords, const RefAdvanceFields* F, float dx, int iteration, float dt,
                      const CombustionParams* params) {
-    ref_hns_advance_model(g, coords, F, dx, iteration, dt, params, 0, 0.0f, 0.0f, 0.0f);
+    ref_hns_advance_model(g, coords, F, dx, iteration, dt, params, 0, 0.0f, 0.0f, 0.0f, 0.0f);
 }
 
 }  // extern "C"

@@ -147,3 +147,36 @@ def test_fire_mixed_rejects_bad_fields(dev):
                                desc)
         assert e.value.status == 1
     grid.close()
+
+
+def test_fire_mixed_host_equals_device(dev):
+    """hns_advance_mixed_host (FP32 host arrays, converted on the device) gives the device form's
+    result on the same rounded inputs, to the bit."""
+    from hnanosolver_b200 import lib as hl
+
+    origins = synth.spheres_topology(80, 3, 8.0, 18.0, seed=9)
+    dens, vel = synth.smoothed_fields(origins, seed=4, box_passes=2)
+    coords = synth.leaf_dense_coords(origins)
+    centres, _ = synth.spheres(80, 3, 8.0, 18.0, 9)
+    mask = synth.sphere_mask(origins, centres[0], 6.0)
+    host = {"velocity": (vel * 5.0).astype(np.float32), "density": dens,
+            "temperature": (1.5 * synth.value_noise(coords, 31)).astype(np.float32),
+            "fuel": np.maximum(0.0, synth.value_noise(coords, 32) - 0.3).astype(np.float32),
+            "flame": np.zeros(len(dens), np.float32)}
+    sources = {"fuel": mask, "temperature": mask * np.float32(2.0)}
+    _, params = _params()
+    model = hl.ForceModel(combustion=1, burn_rate=0.5, heat_release=1.0, density_buoyancy=0.1)
+    desc = hl.MixedDesc(dt=0.0, omega=1.9, tolerance=TOL, max_outer=12, inner_iterations=30, flags=0)
+    grid = hl.Grid(origins, voxel_size=0.1)
+    cur = _to_dev(dev, host)
+    src = _to_dev(dev, sources)
+    nxt = {k: torch.empty_like(v) for k, v in cur.items()}
+    torch.cuda.synchronize()
+    grid.advance_mixed(cur, nxt, src, 1.0 / 24.0, params, model, desc)
+    grid.synchronize()
+    hf = {k: np.ascontiguousarray(v.reshape(-1)).copy() for k, v in host.items()}
+    info = grid.advance_mixed_host(hf, sources, 1.0 / 24.0, params, model, desc, info=True)
+    assert info.residual <= TOL
+    for k, t in nxt.items():
+        assert np.array_equal(hf[k], t.float().cpu().numpy()), k
+    grid.close()

@@ -1,0 +1,62 @@
+"""The timeout path of a bounded device-side wait, made to run out on purpose.
+
+rbgs_stream_kernel (the FP32 red-black iteration) waits for each leaf's bulk copies on an
+mbarrier with a bounded number of polls. The test hook HNS_OPT_WAIT_POLLS lowers the limit of
+that first wait to 0 polls, so every CTA gives up at its first leaf: it raises the device error
+flag, still waits for its copies in flight with the normal limit (no copy is writing when the
+CTA exits), and returns. Nothing hangs or faults: hns_device_status reports HNS_ERR_TIMEOUT
+once and clears it, and the next call with the default limit is clean and gives the same bits
+as a context that never timed out."""
+import numpy as np
+import pytest
+
+from hnanosolver_b200 import synth
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda", 0)
+
+
+def test_bounded_copy_wait_gives_up_then_recovers(dev):
+    from hnanosolver_b200 import lib as hl
+
+    origins = synth.spheres_topology(96, 3, 8.0, 20.0, seed=12)
+    dens, vel = synth.smoothed_fields(origins, seed=3, box_passes=1)
+    n = len(dens)
+    clean = hl.Grid(origins, voxel_size=0.1)
+    grid = hl.Grid(origins, voxel_size=0.1)
+    v = torch.from_numpy(vel).to(dev)
+    div = torch.empty(n, device=dev)
+    p_ref = torch.zeros(n, device=dev)
+    torch.cuda.synchronize()
+    clean.divergence(v, div)
+    clean.rbgs(div, p_ref, 6, 1.7)
+    clean.synchronize()
+
+    grid.set_option(hl.OPT_WAIT_POLLS, 0)
+    p = torch.zeros(n, device=dev)
+    torch.cuda.synchronize()
+    grid.rbgs(div, p, 6, 1.7)  # the launches themselves succeed
+    st = hl.lib.hns_device_status(grid._h)
+    assert st == 8, hl.STATUS_NAMES.get(st)  # HNS_ERR_TIMEOUT
+    assert b"device-side wait" in hl.lib.hns_last_error()
+    assert hl.lib.hns_device_status(grid._h) == 0  # reported once, then cleared
+    assert not torch.equal(p, p_ref)  # the solve did not finish
+
+    grid.set_option(hl.OPT_WAIT_POLLS, -1)
+    p2 = torch.zeros(n, device=dev)
+    torch.cuda.synchronize()
+    grid.rbgs(div, p2, 6, 1.7)
+    assert hl.lib.hns_device_status(grid._h) == 0
+    assert torch.equal(p2, p_ref)
+    with pytest.raises(hl.HnsError):
+        grid.set_option(hl.OPT_WAIT_POLLS, -2)
+    grid.close()
+    clean.close()
+    assert np.isfinite(p2.cpu().numpy()).all()
