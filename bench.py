@@ -65,6 +65,10 @@ FIRE_WORKLOADS = {
     "plume256": dict(desc="256^3 box, leaves inside 8 seeded spheres of radius 20-60; fields density, temperature, "
                           "fuel, flame and velocity (FP32); fire forces and sources; 100 red-black iterations per step",
                      dx=0.1, dt=1.0 / 24.0, iterations=100, precision="fp32", fp32_iterations=100),
+    "fire512": dict(desc="512^3 box, leaves inside 32 seeded spheres of radius 15-60; fields density, temperature, "
+                         "fuel, flame (FP16) and velocity (BF16); fire forces and sources; refined solve to 1e-5",
+                    dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.94, inner=40, cap=8000,
+                    check_every=20, precision="mixed", fp32_iterations=None),
     "fire1024": dict(desc="1024^3 box, leaves inside 32 seeded spheres of radius 30-120; fields density, temperature, "
                           "fuel, flame (FP16) and velocity (BF16); fire forces and sources; refined solve to 1e-5",
                      dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.94, inner=40, cap=8000,

@@ -373,10 +373,6 @@ HNS_API hns_status hns_destroy(hns_ctx* ctx) {
         Context& c = ctx->impl;
         DeviceGuard g(c.device);
         if (c.stream) (void)cudaStreamSynchronize(c.stream);
-        if (c.l2_resident) {  // give back the persisting L2 set-aside
-            (void)cudaCtxResetPersistingL2Cache();
-            (void)cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
-        }
         if (c.aux_stream) {
             (void)cudaStreamSynchronize(c.aux_stream);
             (void)cudaStreamDestroy(c.aux_stream);
@@ -426,23 +422,6 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
             if (value != HNS_INNER_ROWS && value != HNS_INNER_PACKED && value != HNS_INNER_SPLIT)
                 fail(HNS_ERR_INVALID_ARG, "unknown inner layout");
             c->inner_layout = value;
-        } else if (option == HNS_OPT_L2_RESIDENT) {
-            if (value != 0 && value != 1) fail(HNS_ERR_INVALID_ARG, "HNS_OPT_L2_RESIDENT takes 0 or 1");
-            DeviceGuard g(c->device);
-            if (value && !c->l2_resident) {
-                // Set aside the device's largest persisting L2 portion for this process.
-                int max_persist = 0;
-                HNS_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c->device));
-                if (max_persist <= 0) fail(HNS_ERR_UNSUPPORTED, "the device has no persisting L2 set-aside");
-                HNS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)max_persist));
-                c->l2_setaside = (size_t)max_persist;
-            } else if (!value && c->l2_resident) {
-                HNS_CUDA(cudaStreamSynchronize(c->stream));
-                HNS_CUDA(cudaCtxResetPersistingL2Cache());
-                HNS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0));
-                c->l2_setaside = 0;
-            }
-            c->l2_resident = value != 0;
         } else if (option == HNS_OPT_WAIT_POLLS) {
             if (value < -1) fail(HNS_ERR_INVALID_ARG, "the wait limit must be -1 (default) or >= 0");
             c->first_wait_polls = value;

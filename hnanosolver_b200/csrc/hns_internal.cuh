@@ -166,8 +166,6 @@ struct Context {
     int rbgs_kernel = HNS_RBGS_BULK;      // hns_set_option(HNS_OPT_RBGS_KERNEL)
     int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
-    bool l2_resident = false;            // hns_set_option(HNS_OPT_L2_RESIDENT)
-    size_t l2_setaside = 0;              // persisting L2 bytes set aside for this context's device
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -270,10 +268,8 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
 void launch_split_face_table(const Context& c, int* nb8);
 // short_grid: one wave of CTAs looping over the leaves, for a launch expected to find the
 // refinement converged and return at once.
-// window: an L2 access-policy window for the launch (HNS_OPT_L2_RESIDENT), or null.
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
-                            float omega, const double* check, double tol2, bool short_grid = false,
-                            const cudaAccessPolicyWindow* window = nullptr);
+                            float omega, const double* check, double tol2, bool short_grid = false);
 void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
                              void* e_out, void* faces_out, float omega, const double* check, double tol2);
 

@@ -691,26 +691,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     float* scales = reinterpret_cast<float*>(plan.slots + 2 * (plan.max_outer + 1));
     HNS_CUDA(cudaMemsetAsync(plan.slots, 0, sizeof(double) * (size_t)(2 * (plan.max_outer + 1) + plan.max_outer), c.stream));
     float* r = c.scratch_f32("refine_r", (size_t)n);
-    // The FP16 colour-split inner solve kept in L2 (HNS_OPT_L2_RESIDENT): r^ and e in one buffer
-    // under an access-policy window.
-    const bool resident = sizeof(TI) == 2 && c.l2_resident && c.inner_layout == HNS_INNER_SPLIT &&
-                          !(flags & HNS_SOLVE_MULTIGRID);
-    const size_t rhat_bytes = ((size_t)n * sizeof(TI) + 255) / 256 * 256;
-    const size_t ws_bytes = rhat_bytes + (size_t)(n + 512) * sizeof(TI);
-    void* ws = resident ? c.scratch_f32("refine_split_ws", (ws_bytes + 3) / 4) : nullptr;
-    cudaAccessPolicyWindow window{};
-    if (resident) {
-        int max_window = 0;
-        HNS_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, c.device));
-        window.base_ptr = ws;
-        window.num_bytes = std::min(ws_bytes, (size_t)std::max(0, max_window));
-        window.hitRatio = window.num_bytes > 0 ? (float)std::min(1.0, (double)c.l2_setaside / (double)window.num_bytes) : 0.f;
-        window.hitProp = cudaAccessPropertyPersisting;
-        window.missProp = cudaAccessPropertyStreaming;
-    }
-    const cudaAccessPolicyWindow* win = resident && window.num_bytes > 0 ? &window : nullptr;
-    TI* rhat = resident ? reinterpret_cast<TI*>(ws)
-                        : reinterpret_cast<TI*>(c.scratch_f32("refine_rhat", ((size_t)n * sizeof(TI) + 3) / 4));
+    TI* rhat = reinterpret_cast<TI*>(c.scratch_f32("refine_rhat", ((size_t)n * sizeof(TI) + 3) / 4));
     TI* e[2] = {reinterpret_cast<TI*>(c.scratch_f32("refine_e0", ((size_t)n * sizeof(TI) + 3) / 4)),
                 reinterpret_cast<TI*>(c.scratch_f32("refine_e1", ((size_t)n * sizeof(TI) + 3) / 4))};
     const double h2 = (double)c.dx * (double)c.dx;
@@ -723,8 +704,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     TI* e_split = nullptr;
     int* nb8 = nullptr;
     if (layout == HNS_INNER_SPLIT) {
-        e_split = resident ? reinterpret_cast<TI*>(static_cast<char*>(ws) + rhat_bytes)
-                           : reinterpret_cast<TI*>(c.scratch_f32("refine_e_split", ((size_t)(n + 512) * sizeof(TI) + 3) / 4));
+        e_split = reinterpret_cast<TI*>(c.scratch_f32("refine_e_split", ((size_t)(n + 512) * sizeof(TI) + 3) / 4));
         nb8 = reinterpret_cast<int*>(c.scratch_f32("refine_split_nb8", (size_t)c.topo.num_leaves * 8));
         // The zero leaf and the face table depend on the topology alone: made once per buffer.
         if (c.split_setup[0] != e_split || c.split_setup[1] != nb8) {
@@ -793,8 +773,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                 if (layout == HNS_INNER_SPLIT) {
                     // In place: red, then black.
                     dst = e_split;
-                    launch_rbgs_split_half(c, nb8, rhat, dst, 0, it == 0, omega, chk, tol2, spare, win);
-                    launch_rbgs_split_half(c, nb8, rhat, dst, 1, false, omega, chk, tol2, spare, win);
+                    launch_rbgs_split_half(c, nb8, rhat, dst, 0, it == 0, omega, chk, tol2, spare);
+                    launch_rbgs_split_half(c, nb8, rhat, dst, 1, false, omega, chk, tol2, spare);
                 } else if (packed) {
                     launch_rbgs_packed_half(c, rhat, halo, src, src_faces, dst, faces[it & 1], omega, chk, tol2);
                     src_faces = faces[it & 1];

@@ -202,8 +202,7 @@ void launch_split_face_table(const Context& c, int* nb8) {
 }
 
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
-                            float omega, const double* check, double tol2, bool short_grid,
-                            const cudaAccessPolicyWindow* window) {
+                            float omega, const double* check, double tol2, bool short_grid) {
     const int64_t L = c.topo.num_leaves;
     if (L == 0) return;
     if (L >= (int64_t(1) << 22)) fail(HNS_ERR_INVALID_ARG, "too many leaves for the colour-split inner solve");
@@ -219,17 +218,9 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c.stream;
-    cudaLaunchAttribute attr[2];
+    cudaLaunchAttribute attr[1];
     unsigned na = 0;
-    if (window != nullptr) {
-        // The inner solve's arrays kept in the L2 set-aside across half-sweeps.
-        attr[na].id = cudaLaunchAttributeAccessPolicyWindow;
-        attr[na].val.accessPolicyWindow = *window;
-        ++na;
-    }
     if (e_zero) {
-        cfg.attrs = attr;
-        cfg.numAttrs = na;
         HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<true>, nb8, r, x, (int)L, colour, omega, check, tol2,
                                     c.counters));
         HNS_LAUNCHED();

@@ -24,7 +24,6 @@ RBGS_PLAIN, RBGS_BULK = 0, 1
 OPT_INNER_LAYOUT = 2
 INNER_ROWS, INNER_PACKED, INNER_SPLIT = 0, 1, 2
 OPT_WAIT_POLLS = 3
-OPT_L2_RESIDENT = 4
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 

@@ -12,6 +12,7 @@ Workloads (seed 0 unless stated):
   shell512   512^3 box, leaves within 16 voxels (plus the leaf half-diagonal) of a seeded
              radius-200 sphere: about 23M voxels
   box128     128^3 box, 4096 leaves, 2,097,152 voxels (the differentiable rollout)
+  fire512    512^3 box, leaves inside 32 seeded spheres of radius 15-60 (a mid-size fire)
   fire1024   1024^3 box, leaves inside 32 seeded spheres of radius 30-120
 
 fire_state() adds the fire workloads' fields and their sphere source (fuel and heat).
@@ -95,7 +96,8 @@ def shell_topology(extent: int = 512, radius: float = 200.0, band: float = 16.0,
 
 
 # The sphere sets of the fire workloads: (extent, count, rmin, rmax).
-SPHERE_WORKLOADS = {"plume256": (256, 8, 20.0, 60.0), "fire1024": (1024, 32, 30.0, 120.0)}
+SPHERE_WORKLOADS = {"plume256": (256, 8, 20.0, 60.0), "fire512": (512, 32, 15.0, 60.0),
+                    "fire1024": (1024, 32, 30.0, 120.0)}
 
 
 def topology(name: str, seed: int = 0) -> np.ndarray:
@@ -107,8 +109,8 @@ def topology(name: str, seed: int = 0) -> np.ndarray:
         return spheres_topology(256, 8, 20.0, 60.0, seed)
     if name == "shell512":
         return shell_topology(512, 200.0, 16.0, seed)
-    if name == "fire1024":
-        return spheres_topology(1024, 32, 30.0, 120.0, seed)
+    if name in SPHERE_WORKLOADS:
+        return spheres_topology(*SPHERE_WORKLOADS[name], seed)
     raise ValueError(f"unknown workload {name!r}")
 
 

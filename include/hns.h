@@ -472,11 +472,6 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
                                     one in-place launch per colour (default). All three give the
                                     same results to the bit; the solver's own arrays, never the
                                     caller's */
-#define HNS_OPT_L2_RESIDENT 4   /* 1: keep the FP16 inner solve's correction and right-hand side (2 x 2
-                                    bytes per voxel, one buffer) in the L2 across its half-sweeps: the
-                                    device's largest persisting L2 portion is set aside for this process
-                                    (released by 0) and the sweeps run under an access-policy window
-                                    over the buffer. 0 (default): plain accesses. Same results. */
 #define HNS_OPT_WAIT_POLLS 3    /* test hook of the timeout path: the poll limit of the first bounded
                                     copy wait of the HNS_RBGS_BULK kernel (value >= 0; -1 restores the
                                     default). 0 makes every CTA give up at its first leaf, wait for its

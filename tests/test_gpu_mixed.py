@@ -339,3 +339,4 @@ def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
     info = g.step_plain(v, torch.empty_like(v), [d], [torch.empty_like(d)], sd, info=True)
     assert info.residual <= 1e-5
     g.close()
+
