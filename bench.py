@@ -2,7 +2,8 @@
 """Throughput of one solver step on a seeded synthetic sparse grid, on 1..N GPUs.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload shell512|plume256|fire1024] [--forces] [--precision mixed|fp32]
+                    [--workload shell512|box64|plume256|fire512|fire1024] [--forces]
+                    [--precision mixed|fp32]
 
 A step is one pass of the hot path over the grid: the SOP operator chain
 HNanoAdvect + HNanoAdvectVelocity + HNanoProjectNonDivergent (scalars and velocity advected
@@ -67,12 +68,15 @@ FIRE_WORKLOADS = {
                      dx=0.1, dt=1.0 / 24.0, iterations=100, precision="fp32", fp32_iterations=100),
     "fire512": dict(desc="512^3 box, leaves inside 32 seeded spheres of radius 15-60; fields density, temperature, "
                          "fuel, flame (FP16) and velocity (BF16); fire forces and sources; refined solve to 1e-5",
-                    dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.94, inner=40, cap=8000,
+                    dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.95, inner=80, cap=6000,
                     check_every=20, precision="mixed", fp32_iterations=None),
     "fire1024": dict(desc="1024^3 box, leaves inside 32 seeded spheres of radius 30-120; fields density, temperature, "
                           "fuel, flame (FP16) and velocity (BF16); fire forces and sources; refined solve to 1e-5",
-                     dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.94, inner=40, cap=8000,
-                     check_every=20, precision="mixed", fp32_iterations=None),
+                     # omega_refined / inner: the fastest to 1e-5 in a sweep of 1.94-1.99 x 40-160 (mixed and FP32
+                     # refinement alike); plain FP32 SOR stalls above 1e-5 on this grid at every omega of 1.9-1.98
+                     # (1.8e-5 after 6000 iterations at 1.9), so its timing is reported only when it converges.
+                     dx=0.1, dt=1.0 / 24.0, tolerance=1e-5, omega=1.9, omega_refined=1.97, inner=80, cap=6000,
+                     check_every=20, precision="mixed", fp32_iterations=6000),
 }
 
 
@@ -637,24 +641,37 @@ def fire_cpu_sample(args, wl, iters, omega, steps, warmup, budget_s=None):
     state = {k: v for k, v in fields.items() if k != "velocity"}
     ref.lib.ref_set_block_stride(stride)
 
-    def one():
-        return g.hns_advance_model(fields["velocity"], state, sources, wl["dx"], iters, wl["dt"], params,
+    def one(k):
+        return g.hns_advance_model(fields["velocity"], state, sources, wl["dx"], k, wl["dt"], params,
                                    combustion=1, burn_rate=model.burn_rate, heat_release=model.heat_release,
                                    ignition_temp=model.ignition_temp, omega=omega)
 
-    for _ in range(warmup):
-        one()
-    times, t_start = [], time.perf_counter()
-    while len(times) < steps and (budget_s is None or not times or time.perf_counter() - t_start < budget_s):
-        t0 = time.perf_counter()
-        one()
-        times.append(time.perf_counter() - t0)
+    def timed(k, reps):
+        for _ in range(warmup):
+            one(k)
+        times, t_start = [], time.perf_counter()
+        while len(times) < reps and (budget_s is None or not times or time.perf_counter() - t_start < budget_s):
+            t0 = time.perf_counter()
+            one(k)
+            times.append(time.perf_counter() - t0)
+        return sum(times) / len(times), len(times)
+
+    # Up to 200 iterations the step runs as is; above, its fixed part (0 iterations) and 40
+    # iterations are timed and the iterations' cost is extrapolated linearly to `iters`.
+    if iters <= 200:
+        t, reps = timed(iters, steps)
+        how = f"{reps} steps"
+    else:
+        t0, r0 = timed(0, steps)
+        t40, r40 = timed(40, steps)
+        t = t0 + (t40 - t0) / 40.0 * iters
+        how = (f"{r0} steps with 0 and {r40} with 40 red-black iterations, the iterations' time extrapolated "
+               f"linearly to {iters}")
     ref.lib.ref_set_block_stride(1)
     sampled = (blocks + stride - 1) // stride * 256
-    t = sum(times) / len(times)
-    sample = (f"{len(times)} steps of the reference's HNS_Advance kernels with its combustion kernel (no density "
-              f"buoyancy term: the reference has none), every launch over 1/{stride} of its 256-voxel blocks "
-              f"({sampled} of {n} voxels), {iters} red-black iterations at omega {omega or 'from dx'}")
+    sample = (f"{how}, of the reference's HNS_Advance kernels with its combustion kernel (no density buoyancy "
+              f"term: the reference has none), every launch over 1/{stride} of its 256-voxel blocks ({sampled} of "
+              f"{n} voxels), {iters} red-black iterations at omega {omega or 'from dx'}")
     return sampled / t, sample, ref.lib.ref_num_threads(), binding.cpu_model(), os.path.basename(ref.path)
 
 
@@ -677,6 +694,61 @@ def reference_arm_fire(args, wl):
         "e2e": {"value": value, "unit": "voxel-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def fire_adjoint_rollout(torch, hl, g, stream, state0, src, dt, params, model, desc, n, steps=8, every=4):
+    """Reverse pass of a checkpointed rollout of the mixed fire step through the C ABI: `steps`
+    steps of hns_advance_mixed from state0 (BF16/FP16 device tensors), the state kept every
+    `every` steps, loss 1/2 |rho_K - rho_target|^2 (target: seed-1 value noise); the backward
+    recomputes each segment's step inputs from its checkpoint and runs hns_adjoint_advance_mixed
+    on them in reverse (FP32 adjoints). CUDA events on the grid's stream; one untimed pass first."""
+    target = torch.rand(n, device=state0["density"].device, generator=torch.Generator(device=state0["density"].device).manual_seed(1))
+
+    def step(cur):
+        nxt = {k: torch.empty_like(v) for k, v in cur.items()}
+        g.advance_mixed(cur, nxt, src, dt, params, model, desc)
+        return nxt
+
+    def forward():
+        ckpt, cur = [], state0
+        for k in range(steps):
+            if k % every == 0:
+                ckpt.append(cur)  # each step writes new tensors
+            cur = step(cur)
+        return ckpt, cur
+
+    def backward(ckpt, last):
+        bar = {k: torch.zeros(v.numel(), device=v.device) for k, v in last.items()}
+        bar["density"] = last["density"].float() - target
+        for seg in reversed(range(len(ckpt))):
+            states = [ckpt[seg]]
+            for _ in range(seg * every, min(seg * every + every, steps) - 1):
+                states.append(step(states[-1]))
+            for s_in in reversed(states):
+                ib = {k: torch.zeros_like(v) for k, v in bar.items()}
+                g.adjoint_advance_mixed(s_in, src, bar, ib, dt, params, model, desc)
+                bar = ib
+        return bar
+
+    with torch.cuda.stream(stream):
+        backward(*forward())
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        ckpt, last = forward()
+        ev[1].record(stream)
+        grads = backward(ckpt, last)
+        ev[2].record(stream)
+    torch.cuda.synchronize()
+    f_ms, b_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    finite = all(bool(torch.isfinite(v).all()) for v in grads.values())
+    recomputed = steps - (steps + every - 1) // every
+    return {"workload": f"{steps}-step rollout of the mixed fire step, checkpoint every {every} steps, "
+                        "loss 1/2 |rho_K - rho_target|^2; adjoints FP32, solves refined to the step's tolerance",
+            "voxels": n, "steps": steps, "checkpoint_every": every, "recomputed_steps": recomputed,
+            "forward_ms": f_ms, "backward_ms": b_ms, "backward_over_forward": b_ms / f_ms,
+            "value": n * steps / (b_ms / 1e3), "unit": "voxel-steps/s (reverse pass, recomputation included)",
+            "gradients_finite": finite}
 
 
 def ours_fire(args, wl):
@@ -724,26 +796,34 @@ def ours_fire(args, wl):
                     raise
                 return None
 
+        cmp_steps = 0 if args.no_fp32_comparison else max(1, min(args.steps, 3))
         load_fp32()
-        i32 = tolerant(lambda: g.advance_solve(dt, params, model, pdesc(wl["cap"]), info=True)) or g.last_solve()
+        i32 = tolerant(lambda: g.advance_solve(dt, params, model, pdesc(wl["cap"]), info=True))
+        stalled = i32 is None
+        i32 = i32 or g.last_solve()
         cap32 = i32.iterations + 2 * wl["check_every"]
         load_fp32()
         ir = tolerant(lambda: g.advance_solve(dt, params, model, rdesc(60), info=True)) or g.last_refine()
         outer_r = max(1, ir.iterations // wl["inner"]) + 2
-        cmp_steps = 0 if args.no_fp32_comparison else max(1, min(args.steps, 3))
         if cmp_steps:
-            load_fp32()
-            g.advance_solve(dt, params, model, pdesc(cap32))
-            ms_plain = _timed_steps(torch, stream, lambda: g.advance_solve(dt, params, model, pdesc(cap32)),
-                                    cmp_steps) / cmp_steps
-            lp = g.last_solve()
+            if stalled:
+                plain = {"converged": False, "omega": wl["omega"], "red_black_iterations": i32.iterations,
+                         "residual_checked": i32.residual,
+                         "note": "plain FP32 SOR stops above the tolerance (its rounding floor): no equal-residual time"}
+            else:
+                load_fp32()
+                g.advance_solve(dt, params, model, pdesc(cap32))
+                ms_plain = _timed_steps(torch, stream, lambda: g.advance_solve(dt, params, model, pdesc(cap32)),
+                                        cmp_steps) / cmp_steps
+                lp = g.last_solve()
+                plain = {"value": n / (ms_plain / 1e3), "ms_per_step": ms_plain, "omega": wl["omega"],
+                         "red_black_iterations": lp.iterations, "residual_checked": lp.residual}
             load_fp32()
             g.advance_solve(dt, params, model, rdesc(outer_r))
             ms_ref = _timed_steps(torch, stream, lambda: g.advance_solve(dt, params, model, rdesc(outer_r)),
                                   cmp_steps) / cmp_steps
             lr = g.last_refine()
-            fp32 = {"plain": {"value": n / (ms_plain / 1e3), "ms_per_step": ms_plain, "omega": wl["omega"],
-                              "red_black_iterations": lp.iterations, "residual_checked": lp.residual},
+            fp32 = {"plain": plain,
                     "refined": {"value": n / (ms_ref / 1e3), "ms_per_step": ms_ref, "omega": wl["omega_refined"],
                                 "inner_iterations": wl["inner"], "red_black_iterations": lr.iterations,
                                 "residual": lr.residual}}
@@ -848,9 +928,13 @@ def ours_fire(args, wl):
         run_host()
     e2e_s = replicas.max_over_ranks(R, (time.perf_counter() - t0) / e2e_steps, dev)
 
+    adjoint = None
+    if rank == 0 and world == 1 and mixed and not args.no_adjoint:
+        adjoint = fire_adjoint_rollout(torch, hl, g, stream, bufs[0], src, dt, params, model, mdesc(outer + 4), n)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        iters_cpu = wl["iterations"] if not mixed else (fp32["plain"]["red_black_iterations"] if fp32 else cap32)
+        iters_cpu = wl["iterations"] if not mixed else wl["fp32_iterations"] or cap32
         v, sample, cores, cpu_name, library = fire_cpu_sample(args, wl, iters_cpu, wl.get("omega", 0.0), 3, 0,
                                                               budget_s=20.0)
         cpu = {"value": v, "unit": "voxel-steps/s", "cores": cores, "kind": "reference", "sample": sample,
@@ -860,7 +944,7 @@ def ours_fire(args, wl):
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
         det = {"precision": args.precision, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
-               "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
+               "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 and "value" in fp32["plain"] else None,
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
                "timed_solves_logged": logged, "worst_residual_timed_steps": worst,
                "timed_steps_above_tolerance": (sum(1 for e in entries if e.residual > tol) if tol else None)}
@@ -884,7 +968,144 @@ def ours_fire(args, wl):
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps, "path": path},
             "gpu_launches": args.steps * launches_per_step,
             "clocks": clk,
+            "adjoint": adjoint,
         }
+        print(json.dumps(line), flush=True)
+    g.close()
+    replicas.finish(R)
+
+
+# The CPU-runnable single step: a 64^3 box fully active (512 leaves), smoothed noise fields,
+# the plain FP32 step with 40 red-black iterations at omega 1.0 from p = 0.
+BOX64 = dict(desc="64^3 box fully active (512 leaves); density value noise and velocity U(-1,1), each box-filtered "
+                  "3 times; the plain FP32 step, 40 red-black iterations at omega 1.0",
+             dx=0.1, dt=0.1, omega=1.0, iterations=40)
+
+
+def box64_config(args):
+    return {"workload": args.workload, "description": BOX64["desc"], "voxels": 262144, "leaves": 512,
+            "dt": BOX64["dt"], "dx": BOX64["dx"], "red_black_iterations": BOX64["iterations"], "omega": BOX64["omega"],
+            "walls": "zero-gradient (the spec's), the reference's Dirichlet-0 reported beside",
+            "l2": "the 16 MB state fits in L2 (126 MB); no flush between steps"}
+
+
+def box64_cpu(args, steps, warmup):
+    from hnanosolver_b200 import synth
+    from oracle import binding
+
+    ref = binding.RefOracle()
+    origins = synth.topology("box64")
+    dens, vel = synth.smoothed_fields(origins, seed=0, box_passes=3)
+    g = ref.grid(synth.leaf_dense_coords(origins))
+    scratch = None
+    for _ in range(warmup):
+        scratch = g.plain_step(vel, [dens], BOX64["dt"], BOX64["dx"], BOX64["iterations"], BOX64["omega"], scratch)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        scratch = g.plain_step(vel, [dens], BOX64["dt"], BOX64["dx"], BOX64["iterations"], BOX64["omega"], scratch)
+    t = (time.perf_counter() - t0) / steps
+    return {"value": 262144 / t, "unit": "voxel-steps/s", "cores": ref.lib.ref_num_threads(), "kind": "reference",
+            "sample": f"{steps} full steps (no sampling) of the reference's kernels, Dirichlet-0 walls (the reference "
+                      f"has no zero-gradient walls), 40 red-black iterations at omega 1.0",
+            "cpu": binding.cpu_model(), "library": os.path.basename(ref.path)}
+
+
+def box64_reference(args):
+    rank, _, _ = dist_info()
+    if rank != 0:
+        return
+    cpu = box64_cpu(args, args.steps, args.warmup)
+    print(json.dumps({"impl": "reference", "metric": "active voxel-steps/s", "value": cpu["value"],
+                      "unit": "voxel-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": 262144 / cpu["value"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": box64_config(args),
+                      "cpu_baseline": cpu,
+                      "e2e": {"value": cpu["value"], "unit": "voxel-steps/s", "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def box64_ours(args):
+    """The CPU-runnable single step on the GPU, zero-gradient walls (the spec's) and the reference's
+    Dirichlet-0 walls, through hns_step_plain; e2e through hns_step_plain_host."""
+    import torch
+
+    from hnanosolver_b200 import lib as hl
+    from hnanosolver_b200 import replicas, synth
+
+    R = replicas.ranks_from_env()
+    rank, world, local = R.rank, R.world, R.local
+    replicas.start(R, "nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    origins = synth.topology("box64")
+    dens, vel = synth.smoothed_fields(origins, seed=replicas.seed_of(R), box_passes=3)
+    n = len(dens)
+    g = hl.Grid(origins, voxel_size=BOX64["dx"], device=local)
+    stream = torch.cuda.Stream(device=dev)
+    g.set_stream(stream.cuda_stream)
+    v = [torch.from_numpy(vel).to(dev), torch.empty((n, 3), device=dev)]
+    d = [torch.from_numpy(dens).to(dev), torch.empty(n, device=dev)]
+    forms = {}
+    for name, flags in (("dirichlet", 0), ("zero_gradient", hl.SOLVE_NEUMANN)):
+        desc = hl.StepDesc(dt=BOX64["dt"], max_iterations=BOX64["iterations"], omega=BOX64["omega"], tolerance=0.0,
+                           check_every=0, flags=flags)
+        st = [0]
+
+        def step():
+            a = st[0]
+            g.step_plain(v[a], v[1 - a], [d[a]], [d[1 - a]], desc)
+            st[0] = 1 - a
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        replicas.barrier(R)
+        clocks = ClockSampler(local)
+        clocks.start()
+        g.profile_read()
+        g.profile_enable(True)
+        ms = _timed_steps(torch, stream, step, args.steps)
+        g.profile_enable(False)
+        prof = g.profile_read()
+        replicas.barrier(R)
+        clk = clocks.stop()
+        ms = replicas.max_over_ranks(R, ms, dev)
+        info = g.step_plain(v[0], v[1], [d[0]], [d[1]], desc, info=True)
+        forms[name] = {"value": replicas.aggregate_rate(R, n, args.steps, ms), "ms_per_step": ms / args.steps,
+                       "residual_after_40": info.residual, "clocks": clk,
+                       "solve_ms_per_step": prof.phase_ms[hl.PHASES["solve"]] / args.steps,
+                       "launches": int(prof.solver_launches)}
+    hv = torch.from_numpy(vel).pin_memory().numpy()
+    hd = torch.from_numpy(dens).pin_memory().numpy()
+    desc = hl.StepDesc(dt=BOX64["dt"], max_iterations=BOX64["iterations"], omega=BOX64["omega"], tolerance=0.0,
+                       check_every=0, flags=hl.SOLVE_NEUMANN)
+    g.step_plain_host(hv, [hd], desc)
+    e2e_steps = max(1, min(args.steps, 10))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        g.step_plain_host(hv, [hd], desc)
+    e2e_s = replicas.max_over_ranks(R, (time.perf_counter() - t0) / e2e_steps, dev)
+    cpu = box64_cpu(args, 3, 1) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
+    if rank == 0:
+        z = forms["zero_gradient"]
+        # The iteration kernel's pass model: read p, read div, write p (12 B per voxel); the state
+        # sits in L2, so this is a rate, not an HBM bound.
+        it_ms = z["solve_ms_per_step"] / max(1, z["launches"] / args.steps)
+        peak, peak_kind = measured_peak_gbs()
+        achieved = 12 * n / (it_ms / 1e3) / 1e9
+        line = {"metric": "active voxel-steps/s", "value": z["value"], "unit": "voxel-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": z["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": box64_config(args), "details": {"walls": forms},
+                "roofline": {"kernel": "rbgs_iteration_kernel<true> (zero-gradient walls)", "bound": "hbm",
+                             "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "launch_ms": it_ms,
+                             "note": "262,144 voxels sit in L2: launch-bound, the fraction is not an HBM bound"},
+                "cpu_baseline": cpu,
+                "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": 16 * n,
+                        "d2h_bytes_per_step": 16 * n, "steps": e2e_steps,
+                        "path": "hns_step_plain_host (C ABI, pinned FP32 host buffers), zero-gradient walls"},
+                "gpu_launches": args.steps * (4 + BOX64["iterations"]), "clocks": z["clocks"]}
         print(json.dumps(line), flush=True)
     g.close()
     replicas.finish(R)
@@ -896,7 +1117,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(set(WORKLOADS) | set(FIRE_WORKLOADS)), default="shell512")
+    ap.add_argument("--workload", choices=sorted(set(WORKLOADS) | set(FIRE_WORKLOADS) | {"box64"}), default="shell512")
     ap.add_argument("--forces", action="store_true",
                     help="the fire step (HNS_Advance with the configurations' forces) instead of the SOP chain; "
                          "implied by fire1024")
@@ -909,6 +1130,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
+    if args.workload == "box64":
+        (box64_reference if args.impl == "reference" else box64_ours)(args)
+        return
     fire = args.forces or args.workload not in WORKLOADS
     if fire:
         if args.workload not in FIRE_WORKLOADS:

@@ -632,6 +632,7 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
         float* div = c->scratch_f32("project_div", n);
         float* p = c->scratch_f32("project_p", n);
         launch_divergence(*c, vel, div);
+        if (flags & HNS_SOLVE_NEUMANN) remove_divergence_mean(*c, div);  // the singular system's compatibility
         double* acc = nullptr;
         if (info) {
             acc = c->reduce_slots(4);
@@ -641,7 +642,7 @@ HNS_API hns_status hns_project(hns_ctx* ctx, float* vel, int iterations, float o
         }
         rbgs_solve(*c, div, p, iterations, omega, flags | HNS_SOLVE_ZERO_INIT);
         if (info) launch_residual(*c, div, p, acc + 2, flags);
-        launch_subtract_gradient(*c, vel, p, vel);  // pointwise in vel: safe in place
+        launch_subtract_gradient(*c, vel, p, vel, nullptr, flags);  // pointwise in vel: safe in place
         if (info) {
             double h[4];
             HNS_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, c->stream));

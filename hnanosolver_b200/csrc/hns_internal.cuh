@@ -157,6 +157,10 @@ struct Context {
     // 64-bit integer in the last slot). Allocated with the context.
     static constexpr int kSolveLogCap = 4096;
     DeviceBuffer d_solve_log;
+    // Face-connected components of the leaves (hns_neumann.cu), made on the first solve with
+    // zero-gradient walls: the component of each leaf, the voxels of each, FP64 sums.
+    int num_components = 0;
+    DeviceBuffer d_components, d_component_counts, d_component_sums;
     SolvePlan last_solve;   // schedule of the most recent checked solve (hns_last_solve)
     RefinePlan last_refine; // schedule of the most recent refined solve (hns_last_refine)
     // Profiling (hns_profile_*): device counters and per-phase events on the stream.
@@ -240,7 +244,12 @@ void launch_rbgs_bulk(const Context& c, const float* div, const float* p_in, flo
 // mixed-precision refinement, L e = rhs. e_in null means e = 0.
 void launch_rbgs_bulk_half(const Context& c, const void* rhs, const void* e_in, void* e_out, float omega,
                            const double* check, double tol2);
-void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out, const float* sdf = nullptr);
+// flags: HNS_SOLVE_NEUMANN takes a missing neighbour's pressure as the voxel's own.
+void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out, const float* sdf = nullptr,
+                              unsigned flags = 0);
+// Zero-gradient walls (hns_neumann.cu): removes the mean of div (n values) per face-connected
+// component of the leaves, the sums in FP64.
+void remove_divergence_mean(Context& c, float* div);
 void launch_vorticity(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale);
 // acc[0] += sum (b - A p)^2, acc[1] += sum b^2 with b = div dx^2 (FP64).
 void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags);

@@ -174,6 +174,38 @@ constexpr int RT = 10;  // divergence tile edge: leaf + one-voxel halo (local -1
 __device__ __forceinline__ int halo_depth(int a) { return a < 0 ? -a : (a > 7 ? a - 7 : 0); }
 __device__ __forceinline__ int nbr_index(int a) { return a < 0 ? 0 : (a > 7 ? 2 : 1); }
 
+// Calls f(offset into the pressure tile) for each in-domain face neighbour of staged cell
+// (a, b, d), in the order x+, x-, y+, y-, z+, z- (nb: the staged 27-leaf neighbourhood).
+template <typename F>
+__device__ __forceinline__ void staged_neighbours(const int* nb, int a, int b, int d, F&& f) {
+    auto in = [&](int x, int y, int z) { return nb[nbr_index(x) * 9 + nbr_index(y) * 3 + nbr_index(z)] >= 0; };
+    if (in(a + 1, b, d)) f(PT * PT);
+    if (in(a - 1, b, d)) f(-PT * PT);
+    if (in(a, b + 1, d)) f(PT);
+    if (in(a, b - 1, d)) f(-PT);
+    if (in(a, b, d + 1)) f(1);
+    if (in(a, b, d - 1)) f(-1);
+}
+
+// The Gauss-Seidel value of staged cell q (local (a, b, d)) with right-hand side bdx2 = div dx^2:
+// the reference's (sum of the six neighbours, 0 outside - bdx2) / 6, or with zero-gradient walls
+// (sum of the in-domain neighbours - bdx2) / their count.
+template <bool kNeumann>
+__device__ __forceinline__ float relax_target(const float* sp, const int* nb, int q, int a, int b, int d, float bdx2) {
+    if constexpr (kNeumann) {
+        float sum = 0.f;
+        int cnt = 0;
+        staged_neighbours(nb, a, b, d, [&](int off) {
+            sum = cnt == 0 ? sp[q + off] : sum + sp[q + off];
+            ++cnt;
+        });
+        return (sum - bdx2) / (float)cnt;
+    } else {
+        const float sum = sp[q + PT * PT] + sp[q - PT * PT] + sp[q + PT] + sp[q - PT] + sp[q + 1] + sp[q - 1];
+        return (sum - bdx2) * kInv6;
+    }
+}
+
 // One red+black iteration of redBlackGaussSeidelUpdate (src/Cuda/Kernel.cu:459-489):
 // the reference's two launches per iteration (src/Cuda/HNanoSolver.cu:367-372) fused into
 // one pass. Red (colour 0) voxels of the leaf and of its face ring are relaxed from the old
@@ -187,6 +219,11 @@ __device__ __forceinline__ int nbr_index(int a) { return a < 0 ? 0 : (a > 7 ? 2 
 // touching memory. When `resid_out` is set the kernel also accumulates, in FP64, the
 // residual of the iterate it reads (r = div dx^2 - (sum of neighbours - 6 p) over the
 // leaf's voxels), which needs no extra memory traffic: the stencil is already staged.
+//
+// kNeumann: zero-gradient walls instead: a voxel's missing face neighbours take its own value,
+// so it averages its n in-domain neighbours, pgs = (sum of those - div dx^2) / n (the sum in the
+// order x+, x-, y+, y-, z+, z-), and the residual uses the same operator.
+template <bool kNeumann>
 __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, const float* __restrict__ div,
                                                                    const float* __restrict__ p_in,
                                                                    float* __restrict__ p_out, float dx2, float omega,
@@ -228,8 +265,16 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
         for (int n = tid; n < 512; n += kThreads) {
             const int a = n >> 6, b = (n >> 3) & 7, d = n & 7;
             const int q = (a + 2) * PT * PT + (b + 2) * PT + (d + 2);
-            const double lap = (double)sp[q + PT * PT] + (double)sp[q - PT * PT] + (double)sp[q + PT] + (double)sp[q - PT] +
-                               (double)sp[q + 1] + (double)sp[q - 1] - 6.0 * (double)sp[q];
+            double lap;
+            if constexpr (kNeumann) {
+                double sum = 0.0;
+                int cnt = 0;
+                staged_neighbours(nb, a, b, d, [&](int off) { sum += (double)sp[q + off], ++cnt; });
+                lap = sum - (double)cnt * (double)sp[q];
+            } else {
+                lap = (double)sp[q + PT * PT] + (double)sp[q - PT * PT] + (double)sp[q + PT] + (double)sp[q - PT] +
+                      (double)sp[q + 1] + (double)sp[q - 1] - 6.0 * (double)sp[q];
+            }
             const double bb = (double)sb[(a + 1) * RT * RT + (b + 1) * RT + (d + 1)] * h2;
             r2 += (bb - lap) * (bb - lap);
             b2 += bb * bb;
@@ -261,10 +306,8 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
         if (halo_depth(a) + halo_depth(b) + halo_depth(d) > 1 || ((a + b + d) & 1) != 0) continue;
         if (nb[nbr_index(a) * 9 + nbr_index(b) * 3 + nbr_index(d)] < 0) continue;
         const int q = (a + 2) * PT * PT + (b + 2) * PT + (d + 2);
-        const float sum = sp[q + PT * PT] + sp[q - PT * PT] + sp[q + PT] + sp[q - PT] + sp[q + 1] + sp[q - 1];
-        const float pgs = (sum - sb[c] * dx2) * kInv6;
         const float po = sp[q];
-        sp[q] = po + omega * (pgs - po);
+        sp[q] = po + omega * (relax_target<kNeumann>(sp, nb, q, a, b, d, sb[c] * dx2) - po);
     }
     __syncthreads();
     for (int n = tid; n < 512; n += kThreads) {
@@ -272,10 +315,8 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
         if (((a + b + d) & 1) != 1) continue;
         const int q = (a + 2) * PT * PT + (b + 2) * PT + (d + 2);
         const int r = (a + 1) * RT * RT + (b + 1) * RT + (d + 1);
-        const float sum = sp[q + PT * PT] + sp[q - PT * PT] + sp[q + PT] + sp[q - PT] + sp[q + 1] + sp[q - 1];
-        const float pgs = (sum - sb[r] * dx2) * kInv6;
         const float po = sp[q];
-        sp[q] = po + omega * (pgs - po);
+        sp[q] = po + omega * (relax_target<kNeumann>(sp, nb, q, a, b, d, sb[r] * dx2) - po);
     }
     __syncthreads();
     for (int n = tid; n < 512; n += kThreads) {
@@ -286,6 +327,8 @@ __global__ void __launch_bounds__(kThreads) rbgs_iteration_kernel(TopoView t, co
 
 // subtractPressureGradient (src/Cuda/Kernel.cu:495-541); sdf (or null): the collision
 // treatment of the result (Kernel.cu:528-538).
+// kNeumann: zero-gradient walls, a missing neighbour's pressure is the voxel's own.
+template <bool kNeumann>
 __global__ void __launch_bounds__(kThreads) subtract_gradient_kernel(TopoView t, const float* __restrict__ vel,
                                                                       const float* __restrict__ p,
                                                                       float* __restrict__ out, float inv_dx,
@@ -297,9 +340,17 @@ __global__ void __launch_bounds__(kThreads) subtract_gradient_kernel(TopoView t,
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
     const int64_t s = (v.leaf << 9) + v.n;
     const float h = 0.5f * inv_dx;
-    const float gx = (near_s(t, L, p, i + 1, j, k) - near_s(t, L, p, i - 1, j, k)) * h;
-    const float gy = (near_s(t, L, p, i, j + 1, k) - near_s(t, L, p, i, j - 1, k)) * h;
-    const float gz = (near_s(t, L, p, i, j, k + 1) - near_s(t, L, p, i, j, k - 1)) * h;
+    auto pn = [&](int x, int y, int z) {
+        if constexpr (kNeumann) {
+            const int64_t q = slot_of(t, L, x, y, z);
+            return q < 0 ? __ldg(p + s) : __ldg(p + q);
+        } else {
+            return near_s(t, L, p, x, y, z);
+        }
+    };
+    const float gx = (pn(i + 1, j, k) - pn(i - 1, j, k)) * h;
+    const float gy = (pn(i, j + 1, k) - pn(i, j - 1, k)) * h;
+    const float gz = (pn(i, j, k + 1) - pn(i, j, k - 1)) * h;
     const float3 u = ld3(vel, s);
     float3 r = make_float3(u.x - gx, u.y - gy, u.z - gz);
     if (sdf != nullptr) collide(t, L, sdf, s, i, j, k, inv_dx, 0.1f, r);
@@ -322,6 +373,7 @@ __global__ void __launch_bounds__(kThreads) collision_enforce_kernel(TopoView t,
 }
 
 // FP64 residual of the relaxed system: r = div dx^2 - (sum of 6 neighbours - 6 p).
+template <bool kNeumann>
 __global__ void __launch_bounds__(kThreads) residual_kernel(TopoView t, const float* __restrict__ div,
                                                              const float* __restrict__ p, double* __restrict__ acc,
                                                              double h2) {
@@ -332,10 +384,23 @@ __global__ void __launch_bounds__(kThreads) residual_kernel(TopoView t, const fl
     __syncthreads();
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
     const int64_t s = (v.leaf << 9) + v.n;
-    const double lap = (double)near_s(t, L, p, i + 1, j, k) + (double)near_s(t, L, p, i - 1, j, k) +
-                       (double)near_s(t, L, p, i, j + 1, k) + (double)near_s(t, L, p, i, j - 1, k) +
-                       (double)near_s(t, L, p, i, j, k + 1) + (double)near_s(t, L, p, i, j, k - 1) -
-                       6.0 * (double)__ldg(p + s);
+    double lap;
+    if constexpr (kNeumann) {
+        // The in-domain neighbours only (zero-gradient walls).
+        const int di[6] = {1, -1, 0, 0, 0, 0}, dj[6] = {0, 0, 1, -1, 0, 0}, dk[6] = {0, 0, 0, 0, 1, -1};
+        double sum = 0.0;
+        int cnt = 0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int64_t ns = slot_of(t, L, i + di[q], j + dj[q], k + dk[q]);
+            if (ns >= 0) sum += (double)__ldg(p + ns), ++cnt;
+        }
+        lap = sum - (double)cnt * (double)__ldg(p + s);
+    } else {
+        lap = (double)near_s(t, L, p, i + 1, j, k) + (double)near_s(t, L, p, i - 1, j, k) +
+              (double)near_s(t, L, p, i, j + 1, k) + (double)near_s(t, L, p, i, j - 1, k) +
+              (double)near_s(t, L, p, i, j, k + 1) + (double)near_s(t, L, p, i, j, k - 1) - 6.0 * (double)__ldg(p + s);
+    }
     const double b = (double)__ldg(div + s) * h2;
     double r2 = (b - lap) * (b - lap), b2 = b * b;
 #pragma unroll
@@ -429,18 +494,31 @@ void launch_divergence(const Context& c, const float* vel, float* div) {
 
 void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in, float* p_out, float omega,
                            unsigned flags, const double* check, double tol2, double* resid_out) {
-    if (flags & HNS_SOLVE_NEUMANN) fail(HNS_ERR_UNSUPPORTED, "Neumann walls are not supported by this solver build");
+    if (flags & HNS_SOLVE_NEUMANN) {  // zero-gradient walls: the staged kernel's Neumann form
+        rbgs_iteration_kernel<true><<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+            c.topo.view, div, p_in, p_out, c.dx * c.dx, omega, check, tol2, resid_out, c.counters);
+        HNS_LAUNCHED();
+        return;
+    }
     if (c.rbgs_kernel == HNS_RBGS_BULK && rbgs_bulk_eligible(div, p_in, p_out)) {
         launch_rbgs_bulk(c, div, p_in, p_out, omega, check, tol2, resid_out);
         return;
     }
-    rbgs_iteration_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+    rbgs_iteration_kernel<false><<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
         c.topo.view, div, p_in, p_out, c.dx * c.dx, omega, check, tol2, resid_out, c.counters);
     HNS_LAUNCHED();
 }
 
-void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out, const float* sdf) {
-    subtract_gradient_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, out, 1.0f / c.dx, sdf);
+void launch_subtract_gradient(const Context& c, const float* vel, const float* p, float* out, const float* sdf,
+                              unsigned flags) {
+    if (flags & HNS_SOLVE_NEUMANN) {
+        if (sdf) fail(HNS_ERR_UNSUPPORTED, "zero-gradient walls do not take a collider");
+        subtract_gradient_kernel<true><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, out, 1.0f / c.dx,
+                                                                                    nullptr);
+    } else {
+        subtract_gradient_kernel<false><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, p, out,
+                                                                                     1.0f / c.dx, sdf);
+    }
     HNS_LAUNCHED();
 }
 
@@ -451,9 +529,11 @@ void launch_vorticity(const Context& c, const float* vel, float* out, float dt, 
 }
 
 void launch_residual(const Context& c, const float* div, const float* p, double* acc, unsigned flags) {
-    if (flags & HNS_SOLVE_NEUMANN) fail(HNS_ERR_UNSUPPORTED, "Neumann walls are not supported by this solver build");
     const double h = (double)c.dx;
-    residual_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, acc, h * h);
+    if (flags & HNS_SOLVE_NEUMANN)
+        residual_kernel<true><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, acc, h * h);
+    else
+        residual_kernel<false><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, acc, h * h);
     HNS_LAUNCHED();
 }
 

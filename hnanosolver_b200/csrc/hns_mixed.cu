@@ -679,6 +679,8 @@ void convert_array(const Context& c, const void* src, int src_dt, void* dst, int
 template <typename TI>
 RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, int inner, float omega, double tol,
                         unsigned flags) {
+    if (flags & HNS_SOLVE_NEUMANN)
+        fail(HNS_ERR_UNSUPPORTED, "zero-gradient walls are supported by the plain red-black solve only");
     const int64_t n = c.num_voxels();
     RefinePlan plan;
     plan.max_outer = std::max(1, max_outer);

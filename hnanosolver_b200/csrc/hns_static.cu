@@ -56,6 +56,8 @@ HNS_API hns_status hns_project_static(hns_ctx* ctx, float* vel, int iterations, 
         if (!vel) fail(HNS_ERR_INVALID_ARG, "null velocity");
         if (((uintptr_t)vel & 3u) != 0) fail(HNS_ERR_INVALID_ARG, "velocity must be 4-byte aligned");
         if (iterations < 0) fail(HNS_ERR_INVALID_ARG, "negative iteration count");
+        if (flags & HNS_SOLVE_NEUMANN)
+            fail(HNS_ERR_UNSUPPORTED, "hns_project_static takes the reference's walls only (its component sums would allocate)");
         const size_t n = (size_t)c->num_voxels();
         if (n > kStaticMaxVoxels)
             fail(HNS_ERR_UNSUPPORTED, "hns_project_static: the grid has " + std::to_string(n) +

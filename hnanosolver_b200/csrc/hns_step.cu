@@ -141,8 +141,11 @@ SolveOutcome project_in_place(Context& c, float* vel, const hns_step_desc& d) {
     SolveOutcome o;
     o.div = c.scratch_f32("project_div", n);
     o.p = c.scratch_f32("project_p", n);
+    if ((d.flags & HNS_SOLVE_NEUMANN) && (d.flags & (HNS_SOLVE_REFINE | HNS_SOLVE_MULTIGRID)))
+        fail(HNS_ERR_UNSUPPORTED, "zero-gradient walls are supported by the plain red-black solve only");
     c.phase_begin(HNS_PHASE_DIVERGENCE);
     launch_divergence(c, vel, o.div);
+    if (d.flags & HNS_SOLVE_NEUMANN) remove_divergence_mean(c, o.div);  // the singular system's compatibility
     c.phase_end();
     c.phase_begin(HNS_PHASE_SOLVE);
     if (d.flags & HNS_SOLVE_REFINE) {
@@ -164,7 +167,7 @@ SolveOutcome project_in_place(Context& c, float* vel, const hns_step_desc& d) {
     c.phase_end();
     c.last_solve = o.plan;
     c.phase_begin(HNS_PHASE_GRADIENT);
-    launch_subtract_gradient(c, vel, o.p, vel);  // pointwise in vel: safe in place
+    launch_subtract_gradient(c, vel, o.p, vel, nullptr, d.flags);  // pointwise in vel: safe in place
     c.phase_end();
     return o;
 }

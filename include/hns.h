@@ -115,7 +115,14 @@ HNS_API hns_status hns_divergence(hns_ctx* ctx, const float* vel, float* div);
 
 /* Flags of the pressure solve. */
 #define HNS_SOLVE_ZERO_INIT 1u   /* start from p = 0 (p is not read; the reference's memset) */
-#define HNS_SOLVE_NEUMANN 2u     /* zero-gradient walls instead of the reference's p = 0 outside */
+#define HNS_SOLVE_NEUMANN 2u     /* zero-gradient walls instead of the reference's p = 0 outside: a
+                                    voxel averages its in-domain face neighbours, (sum - div dx^2) / n,
+                                    and the gradient takes a missing neighbour's pressure as the
+                                    voxel's own. hns_project and hns_step_plain first remove the
+                                    divergence's mean per face-connected component of leaves (FP64
+                                    sums), which the singular system needs; hns_rbgs relaxes the div
+                                    it is given. Plain red-black solves only (not with
+                                    HNS_SOLVE_REFINE, the mixed step or hns_project_static). */
 
 /* `iterations` red-black SOR iterations on div (redBlackGaussSeidelUpdate,
  * src/Cuda/Kernel.cu:459-489, looped as src/Cuda/HNanoSolver.cu:366-373): colour

@@ -141,6 +141,10 @@ class Oracle:
             _sig(lib, "hnso_add_velocity_source_xyz" + s, None, _i64, _p, _p, _p, _p, r)
             _sig(lib, "hnso_add_gravity" + s, None, _i64, _p, r, r)
             _sig(lib, "hnso_project" + s, None, _p, _p, _p, _p, r, _i, r)
+            _sig(lib, "hnso_rbgs_neumann" + s, None, _p, _p, _p, r, _i, r)
+            _sig(lib, "hnso_residual_neumann" + s, None, _p, _p, _p, r, _p, _p)
+            _sig(lib, "hnso_remove_mean" + s, None, _p, _p)
+            _sig(lib, "hnso_project_neumann" + s, None, _p, _p, _p, _p, r, _i, r)
         for suf, real in (("_f32", _f), ("_f64", _d)):
             _sig(lib, "hnso_hns_advance_model" + suf, None, _p, ctypes.POINTER(AdvanceFields), real, _i, real,
                  ctypes.POINTER(CombustionParams), ctypes.POINTER(ForceModel))
@@ -250,6 +254,34 @@ class OracleTopo:
         getattr(self.o.lib, "hnso_vorticity_confinement" + self._dt(vel))(self.h, ptr(vel), ptr(out), dt, inv_dx,
                                                                           scale, factor_scale)
         return out
+
+    def rbgs_neumann(self, div, p, dx, iterations, omega):
+        """Red-black SOR with zero-gradient walls (no mean removal)."""
+        p = np.ascontiguousarray(p).copy()
+        div = np.ascontiguousarray(div, dtype=p.dtype)
+        getattr(self.o.lib, "hnso_rbgs_neumann" + self._dt(p))(self.h, ptr(div), ptr(p), dx, iterations, omega)
+        return p
+
+    def residual_neumann(self, div, p, dx):
+        div = np.ascontiguousarray(div)
+        p = np.ascontiguousarray(p, dtype=div.dtype)
+        r2, b2 = ctypes.c_double(), ctypes.c_double()
+        getattr(self.o.lib, "hnso_residual_neumann" + self._dt(div))(self.h, ptr(div), ptr(p), dx, ctypes.byref(r2),
+                                                                     ctypes.byref(b2))
+        return r2.value, b2.value
+
+    def remove_mean(self, div):
+        div = np.ascontiguousarray(div).copy()
+        getattr(self.o.lib, "hnso_remove_mean" + self._dt(div))(self.h, ptr(div))
+        return div
+
+    def project_neumann(self, vel, dx, iterations, omega):
+        vel = np.ascontiguousarray(vel).copy()
+        div = np.zeros(len(vel), dtype=vel.dtype)
+        p = np.zeros(len(vel), dtype=vel.dtype)
+        getattr(self.o.lib, "hnso_project_neumann" + self._dt(vel))(self.h, ptr(vel), ptr(div), ptr(p), dx, iterations,
+                                                                    omega)
+        return vel, div, p
 
     def project(self, vel, dx, iterations, omega):
         vel = np.ascontiguousarray(vel).copy()

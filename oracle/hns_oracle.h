@@ -88,6 +88,12 @@ typedef struct {
     void hnso_add_velocity_source_xyz##S(int64_t n, R* vel, const R* sx, const R* sy, const R* sz, R dt);          \
     void hnso_add_gravity##S(int64_t n, R* vel, R g, R dt);                                                        \
     void hnso_project##S(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterations, R omega);                \
+    void hnso_rbgs_sweep_neumann##S(const hnso_topo* t, const R* div, R* p, R dx, int color, R omega);            \
+    void hnso_rbgs_neumann##S(const hnso_topo* t, const R* div, R* p, R dx, int iterations, R omega);             \
+    void hnso_residual_neumann##S(const hnso_topo* t, const R* div, const R* p, R dx, double* r2, double* b2);    \
+    void hnso_remove_mean##S(const hnso_topo* t, R* div);                                                        \
+    void hnso_subtract_gradient_neumann##S(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx);       \
+    void hnso_project_neumann##S(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterations, R omega);        \
     void hnso_enforce_collision##S(const hnso_topo* t, R* vel, const R* sdf, R inv_dx);
 
 HNSO_DECLARE(float, _f32)

@@ -373,6 +373,154 @@ void FN(hnso_residual)(const hnso_topo* t, const R* div, const R* p, R dx, doubl
     *b2 = sb;
 }
 
+/* ---- zero-gradient (Neumann) walls: the configurations' boundary, an extension ----------
+ * The reference reads p = 0 outside the domain with a fixed 1/6 (Dirichlet-0). With zero-
+ * gradient walls the pressure outside equals that of the voxel inside, so a voxel's update
+ * averages its n in-domain face neighbours: p += omega ((sum of those - div dx^2) / n - p),
+ * the sum in the order x+, x-, y+, y-, z+, z-. The operator is singular, one constant per
+ * face-connected component of leaves, so the divergence's mean is removed per component in
+ * FP64 first (FN(hnso_remove_mean)). */
+static int FN(inside)(const hnso_topo* t, int32_t i, int32_t j, int32_t k) { return hnso_offset(t, i, j, k) != 0; }
+
+void FN(hnso_rbgs_sweep_neumann)(const hnso_topo* t, const R* div, R* p, R dx, int color, R omega) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R dx2 = dx * dx;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        if (((i + j + k) & 1) != color) continue;
+        const int32_t d[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        R sum = 0;
+        int cnt = 0;
+        for (int q = 0; q < 6; ++q) {
+            if (!FN(inside)(t, i + d[q][0], j + d[q][1], k + d[q][2])) continue;
+            sum = cnt == 0 ? FN(near_s)(t, p, i + d[q][0], j + d[q][1], k + d[q][2])
+                           : sum + FN(near_s)(t, p, i + d[q][0], j + d[q][1], k + d[q][2]);
+            ++cnt;
+        }
+        const R pgs = (sum - div[s] * dx2) / (R)cnt;
+        const R pold = p[s];
+        p[s] = pold + omega * (pgs - pold);
+    }
+}
+
+void FN(hnso_rbgs_neumann)(const hnso_topo* t, const R* div, R* p, R dx, int iterations, R omega) {
+    for (int it = 0; it < iterations; ++it) {
+        FN(hnso_rbgs_sweep_neumann)(t, div, p, dx, 0, omega);
+        FN(hnso_rbgs_sweep_neumann)(t, div, p, dx, 1, omega);
+    }
+}
+
+/* r = div dx^2 - (sum of the in-domain neighbours - n p), accumulated in double. */
+void FN(hnso_residual_neumann)(const hnso_topo* t, const R* div, const R* p, R dx, double* r2, double* b2) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const double h2 = (double)dx * (double)dx;
+    double sr = 0.0, sb = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : sr, sb)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const int32_t d[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+        double lap = 0.0;
+        int cnt = 0;
+        for (int q = 0; q < 6; ++q)
+            if (FN(inside)(t, i + d[q][0], j + d[q][1], k + d[q][2])) {
+                lap += (double)FN(near_s)(t, p, i + d[q][0], j + d[q][1], k + d[q][2]);
+                ++cnt;
+            }
+        lap -= (double)cnt * (double)p[s];
+        const double b = (double)div[s] * h2;
+        sr += (b - lap) * (b - lap);
+        sb += b * b;
+    }
+    *r2 = sr;
+    *b2 = sb;
+}
+
+/* Face-connected components of the leaves (two leaves sharing a face share voxel faces):
+ * comp[leaf] in [0, ncomp), labelled in leaf order of first appearance. Returns ncomp. */
+static int64_t FN(components)(const hnso_topo* t, int64_t* comp) {
+    const int64_t L = t->num_leaves;
+    for (int64_t l = 0; l < L; ++l) comp[l] = -1;
+    int64_t* stack = (int64_t*)malloc(sizeof(int64_t) * (size_t)(L > 0 ? L : 1));
+    int64_t nc = 0;
+    for (int64_t l0 = 0; l0 < L; ++l0) {
+        if (comp[l0] >= 0) continue;
+        int64_t top = 0;
+        stack[top++] = l0;
+        comp[l0] = nc;
+        while (top > 0) {
+            const int64_t l = stack[--top];
+            const int32_t* o = t->origins + 3 * l;
+            const int32_t d[6][3] = {{8, 0, 0}, {-8, 0, 0}, {0, 8, 0}, {0, -8, 0}, {0, 0, 8}, {0, 0, -8}};
+            for (int q = 0; q < 6; ++q) {
+                const int64_t m = find_leaf(t, o[0] + d[q][0], o[1] + d[q][1], o[2] + d[q][2]);
+                if (m >= 0 && comp[m] < 0) {
+                    comp[m] = nc;
+                    stack[top++] = m;
+                }
+            }
+        }
+        ++nc;
+    }
+    free(stack);
+    return nc;
+}
+
+/* Removes the mean of div per component: sums in double, the mean subtracted in R. */
+void FN(hnso_remove_mean)(const hnso_topo* t, R* div) {
+    const int64_t L = t->num_leaves;
+    int64_t* comp = (int64_t*)malloc(sizeof(int64_t) * (size_t)(L > 0 ? L : 1));
+    const int64_t nc = FN(components)(t, comp);
+    double* sum = (double*)calloc((size_t)(nc > 0 ? nc : 1), sizeof(double));
+    double* cnt = (double*)calloc((size_t)(nc > 0 ? nc : 1), sizeof(double));
+    for (int64_t s = 0; s < 512 * L; ++s) {
+        sum[comp[s >> 9]] += (double)div[s];
+        cnt[comp[s >> 9]] += 1.0;
+    }
+    for (int64_t s = 0; s < 512 * L; ++s) div[s] = div[s] - (R)(sum[comp[s >> 9]] / cnt[comp[s >> 9]]);
+    free(sum);
+    free(cnt);
+    free(comp);
+}
+
+/* u = u* - grad p with the wall's ghost pressure equal to the voxel's own. */
+void FN(hnso_subtract_gradient_neumann)(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R h = (R)0.5 * inv_dx;
+#pragma omp parallel for schedule(static)
+    for (int64_t s = 0; s < N; ++s) {
+        int32_t i, j, k;
+        FN(coord_of)(t, s, &i, &j, &k);
+        const R c = p[s];
+#define HNSO_NP(a, b, cc) (FN(inside)(t, a, b, cc) ? FN(near_s)(t, p, a, b, cc) : c)
+        const R gx = (HNSO_NP(i + 1, j, k) - HNSO_NP(i - 1, j, k)) * h;
+        const R gy = (HNSO_NP(i, j + 1, k) - HNSO_NP(i, j - 1, k)) * h;
+        const R gz = (HNSO_NP(i, j, k + 1) - HNSO_NP(i, j, k - 1)) * h;
+#undef HNSO_NP
+        out[3 * s] = vel[3 * s] - gx;
+        out[3 * s + 1] = vel[3 * s + 1] - gy;
+        out[3 * s + 2] = vel[3 * s + 2] - gz;
+    }
+}
+
+/* The projection with zero-gradient walls: divergence, its mean removed per component,
+ * p = 0, iterations x (red, black), gradient subtraction. omega < 0: 2/(1+sin(3.14159 dx)). */
+void FN(hnso_project_neumann)(const hnso_topo* t, R* vel, R* div, R* p, R dx, int iterations, R omega) {
+    const int64_t N = hnso_topo_num_voxels(t);
+    const R inv_dx = (R)1 / dx;
+    if (omega < (R)0) omega = (R)(2.0f / (1.0f + sin(3.14159 * (double)dx)));
+    FN(hnso_divergence)(t, vel, div, inv_dx);
+    FN(hnso_remove_mean)(t, div);
+    for (int64_t s = 0; s < N; ++s) p[s] = 0;
+    FN(hnso_rbgs_neumann)(t, div, p, dx, iterations, omega);
+    R* tmp = (R*)malloc(sizeof(R) * 3 * (size_t)N);
+    memcpy(tmp, vel, sizeof(R) * 3 * (size_t)N);
+    FN(hnso_subtract_gradient_neumann)(t, tmp, p, vel, inv_dx);
+    free(tmp);
+}
+
 /* subtractPressureGradient (src/Cuda/Kernel.cu:495-541), no collision: u = u* - grad p,
  * central differences, p = 0 outside. */
 static void FN(subtract_gradient_impl)(const hnso_topo* t, const R* vel, const R* p, R* out, R inv_dx, const R* sdf) {
