@@ -779,7 +779,7 @@ def ours_fire(args, wl):
     # ---- FP32 forms of the fire step at the same residual (the solve-to-tolerance workloads) ----
     fp32 = None
     cap32 = None
-    if tol is not None:
+    if tol is not None and not args.no_fp32_comparison:
         def pdesc(cap):
             return hl.StepDesc(dt=0.0, max_iterations=cap, omega=wl["omega"], tolerance=tol,
                                check_every=wl["check_every"], flags=0)
@@ -934,7 +934,7 @@ def ours_fire(args, wl):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        iters_cpu = wl["iterations"] if not mixed else wl["fp32_iterations"] or cap32
+        iters_cpu = wl["iterations"] if not mixed else (wl["fp32_iterations"] or cap32 or wl["cap"])
         v, sample, cores, cpu_name, library = fire_cpu_sample(args, wl, iters_cpu, wl.get("omega", 0.0), 3, 0,
                                                               budget_s=20.0)
         cpu = {"value": v, "unit": "voxel-steps/s", "cores": cores, "kind": "reference", "sample": sample,

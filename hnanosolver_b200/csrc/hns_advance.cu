@@ -28,6 +28,7 @@
 #include <string>
 #include <vector>
 
+#include "hns_confine.cuh"
 #include "hns_internal.cuh"
 #include "hns_stencil.cuh"
 
@@ -91,6 +92,41 @@ __global__ void __launch_bounds__(kThreads) confine_sources_kernel(TopoView t, c
     if (gravity != 0.0f) r.y -= gravity * dt;
     st3(out, s, r);
     for (int q = 0; q < ss.count; ++q) ss.dst[q][s] += dt * __ldg(ss.src[q] + s);
+}
+
+// confine_sources_kernel on a shared-memory leaf tile (hns_confine.cuh), for |fs| <= 1: one CTA
+// per leaf, the same values.
+__global__ void __launch_bounds__(kThreads) confine_sources_tile_kernel(TopoView t, const float* __restrict__ vel,
+                                                                         float* __restrict__ out, float dt, float inv_dx,
+                                                                         float scale, int fs,
+                                                                         const float* __restrict__ src_v3,
+                                                                         const float* __restrict__ sx,
+                                                                         const float* __restrict__ sy,
+                                                                         const float* __restrict__ sz, float gravity,
+                                                                         ScalarSources ss) {
+    __shared__ LeafNbhd L;
+    __shared__ ConfineTile T;
+    const int64_t leaf = blockIdx.x;
+    load_nbhd(L, t, leaf);
+    __syncthreads();
+    confine_tile(L, vel, T, 0.5f * inv_dx);
+    for (int n = threadIdx.x; n < 512; n += blockDim.x) {
+        const int64_t s = (leaf << 9) + n;
+        float3 r = confine_at(T, n >> 6, (n >> 3) & 7, n & 7, fs, inv_dx, dt, scale);
+        if (src_v3 != nullptr) {
+            const float3 a = ld3(src_v3, s);
+            r.x += a.x * dt;
+            r.y += a.y * dt;
+            r.z += a.z * dt;
+        } else if (sx != nullptr && sy != nullptr && sz != nullptr) {
+            r.x += dt * __ldg(sx + s);
+            r.y += dt * __ldg(sy + s);
+            r.z += dt * __ldg(sz + s);
+        }
+        if (gravity != 0.0f) r.y -= gravity * dt;
+        st3(out, s, r);
+        for (int q = 0; q < ss.count; ++q) ss.dst[q][s] += dt * __ldg(ss.src[q] + s);
+    }
 }
 
 // The burn model and the buoyancy's density term of one step (hns_force_model), with the
@@ -196,9 +232,14 @@ void launch_div_combust_buoy(const Context& c, const float* vel, float* vel_out,
 
 void launch_confine_sources(const Context& c, const float* vel, float* out, float dt, float scale, float factor_scale,
                             const float* src_v3, float gravity) {
-    confine_sources_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, out, dt, 1.0f / c.dx, scale,
-                                                                       (int)factor_scale, src_v3, nullptr, nullptr,
-                                                                       nullptr, gravity, ScalarSources{});
+    const int fs = (int)factor_scale;
+    if (fs >= -1 && fs <= 1)
+        confine_sources_tile_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+            c.topo.view, vel, out, dt, 1.0f / c.dx, scale, fs, src_v3, nullptr, nullptr, nullptr, gravity, ScalarSources{});
+    else
+        confine_sources_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, vel, out, dt, 1.0f / c.dx, scale, fs,
+                                                                           src_v3, nullptr, nullptr, nullptr, gravity,
+                                                                           ScalarSources{});
     HNS_LAUNCHED();
 }
 
@@ -299,11 +340,17 @@ void run_advance(Context& c, int iterations, float dt, const hns_combustion_para
             }
         }
         c.phase_begin(HNS_PHASE_FORCES);
-        confine_sources_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-            c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, (int)P.factorScale,
-            (sv && sv->components == 3) ? sv->buf.as<float>() : nullptr,
-            (sx && sx->components == 1) ? sx->buf.as<float>() : nullptr, (sy && sy->components == 1) ? sy->buf.as<float>() : nullptr,
-            (sz && sz->components == 1) ? sz->buf.as<float>() : nullptr, P.gravity, ss);
+        const float* sv3 = (sv && sv->components == 3) ? sv->buf.as<float>() : nullptr;
+        const float* svx = (sx && sx->components == 1) ? sx->buf.as<float>() : nullptr;
+        const float* svy = (sy && sy->components == 1) ? sy->buf.as<float>() : nullptr;
+        const float* svz = (sz && sz->components == 1) ? sz->buf.as<float>() : nullptr;
+        const int fs = (int)P.factorScale;
+        if (fs >= -1 && fs <= 1)
+            confine_sources_tile_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+                c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, fs, sv3, svx, svy, svz, P.gravity, ss);
+        else
+            confine_sources_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+                c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, fs, sv3, svx, svy, svz, P.gravity, ss);
         HNS_LAUNCHED();
 
         // The combustion model's fields are created zero-filled on first use (:326-338 for

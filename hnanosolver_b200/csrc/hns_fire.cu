@@ -13,8 +13,8 @@
 //   refined solve                   div -> p (FP64)                      (redBlackGaussSeidelUpdate loop,
 //   [divergence of adv3, refined solve]  disturbanceEnable > 0           to a tolerance)
 //   gradient_mixed                  out velocity -= grad p, in place     (subtractPressureGradient)
-//   advect_scalars_mixed            scalars -> out scalars along the     (advect_scalars)
-//                                   projected velocity
+//   pack_fire_records +             scalars -> out scalars along the     (advect_scalars)
+//   advect_scalars_records          projected velocity
 // The scalar sources are pointwise and independent of the velocity, so adding them in the
 // divergence pass instead of the confinement pass (where HNS_Advance launches them) gives the
 // same values, and the sourced value feeds the burn in FP32 without an FP16 rounding between.
@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <string>
 
+#include "hns_confine.cuh"
 #include "hns_internal.cuh"
 #include "hns_stencil.cuh"
 #include "hns_types.cuh"
@@ -102,6 +103,32 @@ __global__ void __launch_bounds__(kThreads) confine_mixed_kernel(TopoView t, con
     }
     if (gravity != 0.0f) r.y -= gravity * dt;
     vstore(out, s, r);
+}
+
+// confine_mixed_kernel on a shared-memory leaf tile (hns_confine.cuh), for |fs| <= 1: one CTA
+// per leaf, the same values.
+__global__ void __launch_bounds__(kThreads) confine_tile_mixed_kernel(TopoView t, const bf16* __restrict__ vel,
+                                                                       bf16* __restrict__ out, float dt, float inv_dx,
+                                                                       float scale, int fs, const bf16* __restrict__ src_v3,
+                                                                       float gravity) {
+    __shared__ LeafNbhd L;
+    __shared__ ConfineTile T;
+    const int64_t leaf = blockIdx.x;
+    load_nbhd(L, t, leaf);
+    __syncthreads();
+    confine_tile(L, vel, T, 0.5f * inv_dx);
+    for (int n = threadIdx.x; n < 512; n += blockDim.x) {
+        const int64_t s = (leaf << 9) + n;
+        float3 r = confine_at(T, n >> 6, (n >> 3) & 7, n & 7, fs, inv_dx, dt, scale);
+        if (src_v3 != nullptr) {
+            const float3 a = vload(src_v3, s);
+            r.x += a.x * dt;
+            r.y += a.y * dt;
+            r.z += a.z * dt;
+        }
+        if (gravity != 0.0f) r.y -= gravity * dt;
+        vstore(out, s, r);
+    }
 }
 
 // The scalar fields of one pass (FP16; null: absent) and the burned outputs (null: the pass
@@ -204,61 +231,95 @@ struct HalfFields {
     int count;
 };
 
+// Voxel records for the scalar advection: the BF16 velocity and up to five FP16 scalars in 16
+// bytes (u | v << 16, w | s0 << 16, s1 | s2 << 16, s3 | s4 << 16; absent scalars 0), so that each
+// of the 2 x 8 trace taps and 6 clamp neighbours is one load instead of one per field.
+__global__ void __launch_bounds__(kThreads) pack_fire_records_kernel(const bf16* __restrict__ vel, HalfFields f,
+                                                                      uint4* __restrict__ rec, int64_t n) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned short* v = reinterpret_cast<const unsigned short*>(vel) + 3 * s;
+        uint32_t h[kFireFields] = {0u, 0u, 0u, 0u, 0u};
+#pragma unroll
+        for (int q = 0; q < kFireFields; ++q)
+            if (q < f.count) h[q] = __half_as_ushort(__ldg(f.in[q] + s));
+        rec[s] = make_uint4((uint32_t)__ldg(v) | ((uint32_t)__ldg(v + 1) << 16), (uint32_t)__ldg(v + 2) | (h[0] << 16),
+                            h[1] | (h[2] << 16), h[3] | (h[4] << 16));
+    }
+}
+
+__device__ __forceinline__ float bf_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+__device__ __forceinline__ float hf(uint32_t w, int hi) {
+    return __half2float(__ushort_as_half((unsigned short)(hi ? (w >> 16) : (w & 0xFFFFu))));
+}
+// Scalar q of a record (word 1 high half, then words 2 and 3).
+__device__ __forceinline__ float rec_s(const uint4& r, int q) {
+    return q == 0 ? hf(r.y, 1) : q == 1 ? hf(r.z, 0) : q == 2 ? hf(r.z, 1) : q == 3 ? hf(r.w, 0) : hf(r.w, 1);
+}
+
 // HNS_Advance's multi-field advection (advect_scalars, src/Cuda/Kernel.cu:163-289) on FP16
-// fields along a BF16 velocity: the back-trace uses the voxel's own velocity, the taps'
-// weight-sum trilinear (setupInterpolation, Kernel.cu:204-233) reads slot 0 outside the
-// domain, and the MacCormack correction is clamped to the centre, its six face neighbours
-// and the forward sample; the FP32 step's operations in its order.
-__global__ void __launch_bounds__(kThreads) advect_scalars_mixed_kernel(TopoView t, const bf16* __restrict__ vel,
-                                                                         HalfFields f, float sdt) {
+// fields along a BF16 velocity, from voxel records: the back-trace uses the voxel's own
+// velocity, the taps' weight-sum trilinear (setupInterpolation, Kernel.cu:204-233) reads slot 0
+// outside the domain, and the MacCormack correction is clamped to the centre, its six face
+// neighbours and the forward sample; the FP32 step's operations in its order, one 16-byte load
+// per tap for the velocity and every field.
+template <int kCount>
+__global__ void __launch_bounds__(kThreads) advect_scalars_records_kernel(TopoView t, const uint4* __restrict__ rec,
+                                                                           HalfFields f, float sdt) {
     __shared__ LeafNbhd L;
     const VoxelIdx v = voxel_of_block();
     load_nbhd(L, t, v.leaf);
     __syncthreads();
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
     const int64_t s = (v.leaf << 9) + v.n;
-    const float3 vc = vload(vel, s);
-    const float bx = (float)i - vc.x * sdt, by = (float)j - vc.y * sdt, bz = (float)k - vc.z * sdt;
+    const uint4 o = __ldg(rec + s);
+    const float bx = (float)i - bf_lo(o.x) * sdt, by = (float)j - bf_hi(o.x) * sdt, bz = (float)k - bf_lo(o.y) * sdt;
     int64_t bi[8], fi[8], ni[6];
     float bw[8], fw[8];
     interp_setup(t, L, bx, by, bz, bi, bw);
     float3 vf = make_float3(0.f, 0.f, 0.f);
+    float pf[kCount], pb[kCount];
+#pragma unroll
+    for (int c = 0; c < kCount; ++c) pf[c] = 0.f, pb[c] = 0.f;
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const float3 a = vload(vel, bi[q]);
-        vf.x = vf.x + a.x * bw[q];
-        vf.y = vf.y + a.y * bw[q];
-        vf.z = vf.z + a.z * bw[q];
+        const uint4 a = __ldg(rec + bi[q]);
+        vf.x = vf.x + bf_lo(a.x) * bw[q];
+        vf.y = vf.y + bf_hi(a.x) * bw[q];
+        vf.z = vf.z + bf_lo(a.y) * bw[q];
+#pragma unroll
+        for (int c = 0; c < kCount; ++c) pf[c] = __fmaf_rn(rec_s(a, c), bw[q], pf[c]);
     }
     interp_setup(t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt, fi, fw);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const uint4 a = __ldg(rec + fi[q]);
+#pragma unroll
+        for (int c = 0; c < kCount; ++c) pb[c] = __fmaf_rn(rec_s(a, c), fw[q], pb[c]);
+    }
     ni[0] = tap_slot(t, L, i - 1, j, k);
     ni[1] = tap_slot(t, L, i + 1, j, k);
     ni[2] = tap_slot(t, L, i, j - 1, k);
     ni[3] = tap_slot(t, L, i, j + 1, k);
     ni[4] = tap_slot(t, L, i, j, k - 1);
     ni[5] = tap_slot(t, L, i, j, k + 1);
+    float mn[kCount], mx[kCount], po[kCount];
 #pragma unroll
-    for (int c = 0; c < kFireFields; ++c) {
-        if (c >= f.count) break;
-        const __half* __restrict__ d = f.in[c];
-        const float po = sload(d, s);
-        float pf = 0.f, pb = 0.f;
+    for (int c = 0; c < kCount; ++c) po[c] = rec_s(o, c), mn[c] = po[c], mx[c] = po[c];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            pf = __fmaf_rn(sload(d, bi[q]), bw[q], pf);
-            pb = __fmaf_rn(sload(d, fi[q]), fw[q], pb);
+    for (int q = 0; q < 6; ++q) {
+        const uint4 a = __ldg(rec + ni[q]);
+#pragma unroll
+        for (int c = 0; c < kCount; ++c) {
+            const float x = rec_s(a, c);
+            mn[c] = fminf(mn[c], x);
+            mx[c] = fmaxf(mx[c], x);
         }
-        const float corr = __fmaf_rn(0.5f, po - pb, pf);
-        float mn = po, mx = po;
+    }
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            const float a = sload(d, ni[q]);
-            mn = fminf(mn, a);
-            mx = fmaxf(mx, a);
-        }
-        mn = fminf(mn, pf);
-        mx = fmaxf(mx, pf);
-        sstore(f.out[c], s, fmaxf(mn, fminf(corr, mx)));
+    for (int c = 0; c < kCount; ++c) {
+        const float corr = __fmaf_rn(0.5f, po[c] - pb[c], pf[c]);
+        sstore(f.out[c], s, fmaxf(fminf(mn[c], pf[c]), fminf(corr, fmaxf(mx[c], pf[c]))));
     }
 }
 
@@ -314,9 +375,15 @@ RefinePlan run_advance_mixed(Context& c, const hns_fire_fields& in, const hns_fi
         c.phase_end();
 
         c.phase_begin(HNS_PHASE_FORCES);
-        confine_mixed_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
-            c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, (int)P.factorScale,
-            static_cast<const bf16*>(src.velocity), P.gravity);
+        const int fs = (int)P.factorScale;
+        if (fs >= -1 && fs <= 1)
+            confine_tile_mixed_kernel<<<(unsigned)c.topo.num_leaves, kThreads, 0, c.stream>>>(
+                c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, fs, static_cast<const bf16*>(src.velocity),
+                P.gravity);
+        else
+            confine_mixed_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(
+                c.topo.view, adv, adv2, dt_sub, inv_dx, P.vorticityScale, fs, static_cast<const bf16*>(src.velocity),
+                P.gravity);
         HNS_LAUNCHED();
         // The burned scalars: the fields this pass changes go to solver-owned arrays, which the
         // scalar advection then reads; the others are advected from the substep's input.
@@ -381,8 +448,20 @@ RefinePlan run_advance_mixed(Context& c, const hns_fire_fields& in, const hns_fi
                 ++f.count;
             }
         if (f.count > 0) {
-            advect_scalars_mixed_kernel<<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, nxt.vel, f,
-                                                                                   dt_sub * inv_dx);
+            // Voxel records of the projected velocity and the fields, then one load per tap.
+            uint4* rec = reinterpret_cast<uint4*>(c.scratch_f32("fire_records", 4 * n));
+            const unsigned pg = (unsigned)std::min<int64_t>((int64_t)(n + kThreads - 1) / kThreads,
+                                                            (int64_t)c.sm_count() * 8);
+            pack_fire_records_kernel<<<pg, kThreads, 0, c.stream>>>(nxt.vel, f, rec, (int64_t)n);
+            HNS_LAUNCHED();
+            const float sdt = dt_sub * inv_dx;
+            switch (f.count) {
+                case 1: advect_scalars_records_kernel<1><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+                case 2: advect_scalars_records_kernel<2><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+                case 3: advect_scalars_records_kernel<3><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+                case 4: advect_scalars_records_kernel<4><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+                default: advect_scalars_records_kernel<5><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+            }
             HNS_LAUNCHED();
         }
         c.phase_end();

@@ -125,13 +125,7 @@ __global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half
     // Within a launch a thread reads and writes only its own rows of the launch's colour and
     // only reads the other colour, so the passes of a CTA are independent.
     const int groups = (num_leaves + kLeavesPerBlock * kLeavesPerThread - 1) / (kLeavesPerBlock * kLeavesPerThread);
-    // Snake order: a black half-sweep of a full grid walks the leaf groups from the last to the
-    // first, so it starts on the leaves the red half-sweep touched last (still in L2), and the
-    // next red half-sweep starts where it ended. A half-sweep reads only the other colour, so the
-    // order of its leaves changes no value.
-    const bool reverse = colour == 1 && (int)gridDim.x >= groups;
-    for (int g0 = blockIdx.x; g0 < groups; g0 += gridDim.x) {
-    const int g = reverse ? groups - 1 - g0 : g0;
+    for (int g = blockIdx.x; g < groups; g += gridDim.x) {
     const int leaf0 = g * (kLeavesPerBlock * kLeavesPerThread) + (int)(threadIdx.x >> 6);
     uint32_t own[kLeavesPerThread];
     bool live[kLeavesPerThread];

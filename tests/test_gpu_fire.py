@@ -61,9 +61,10 @@ def _host64(t, n):
     return a.reshape(n, 3) if a.size == 3 * n else a
 
 
-@pytest.mark.parametrize("combustion,alpha,substeps,disturbance",
-                         [(1, 0.1, 1, 0.0), (0, 0.1, 1, 0.0), (1, 0.0, 2, 1.0), (2, 0.1, 1, 0.0)])
-def test_fire_mixed_against_fp64_oracle(dev, oracle, combustion, alpha, substeps, disturbance):
+@pytest.mark.parametrize("combustion,alpha,substeps,disturbance,factor",
+                         [(1, 0.1, 1, 0.0, 1.0), (0, 0.1, 1, 0.0, 1.0), (1, 0.0, 2, 1.0, 1.0), (2, 0.1, 1, 0.0, 1.0),
+                          (1, 0.1, 1, 0.0, 2.0)])
+def test_fire_mixed_against_fp64_oracle(dev, oracle, combustion, alpha, substeps, disturbance, factor):
     from oracle.binding import ForceModel as OM
 
     from hnanosolver_b200 import lib as hl
@@ -85,7 +86,7 @@ def test_fire_mixed_against_fp64_oracle(dev, oracle, combustion, alpha, substeps
     if combustion == 2:
         del state["fuel"]
     sources = {"fuel": mask, "temperature": mask * np.float32(2.0)}
-    op, params = _params(substeps=substeps, disturbanceEnable=disturbance)
+    op, params = _params(substeps=substeps, disturbanceEnable=disturbance, factorScale=factor)
     om = OM(combustion=combustion, burn_rate=0.5, heat_release=1.0, ignition_temp=0.0, density_buoyancy=alpha,
             omega=1.9)
     gm = hl.ForceModel(combustion=combustion, burn_rate=0.5, heat_release=1.0, ignition_temp=0.0,

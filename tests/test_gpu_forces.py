@@ -68,8 +68,11 @@ def _run_both(grid, t, vel, state, sources, calls, iterations, dt, op, params, o
     return ov, state
 
 
-@pytest.mark.parametrize("combustion,alpha,substeps", [(1, 0.1, 1), (1, 0.0, 2), (0, 0.1, 1), (2, 0.1, 1)])
-def test_force_models_three_calls(dev, oracle, combustion, alpha, substeps):
+@pytest.mark.parametrize("combustion,alpha,substeps,factor", [(1, 0.1, 1, 1.0), (1, 0.0, 2, 1.0), (0, 0.1, 1, 1.0),
+                                                                (2, 0.1, 1, 1.0), (1, 0.1, 1, 2.0), (1, 0.1, 1, -1.0)])
+def test_force_models_three_calls(dev, oracle, combustion, alpha, substeps, factor):
+    """factor: factorScale; |int(factorScale)| <= 1 takes the shared-memory confinement tile, 2 the
+    gather form."""
     from hnanosolver_b200 import lib as hl
 
     origins = synth.spheres_topology(80, 3, 8.0, 18.0, seed=6)
@@ -83,7 +86,7 @@ def test_force_models_three_calls(dev, oracle, combustion, alpha, substeps):
     state = {"density": dens, "temperature": (rng.random(n, dtype=np.float32) * 1.5).astype(np.float32),
              "fuel": (rng.random(n, dtype=np.float32) * (rng.random(n) < 0.5)).astype(np.float32),
              "flame": np.zeros(n, np.float32)}
-    op, params = _params(substeps=substeps)
+    op, params = _params(substeps=substeps, factorScale=factor)
     om, gm = _models(combustion, alpha)
     grid = hl.Grid(origins, voxel_size=0.1)
     grid.field_set("velocity", vel)
