@@ -237,6 +237,10 @@ void rbgs_solve(Context& c, const float* div, float* p, int iterations, float om
         if (flags & HNS_SOLVE_ZERO_INIT) HNS_CUDA(cudaMemsetAsync(p, 0, sizeof(float) * c.num_voxels(), c.stream));
         return;
     }
+    if (use_split32(c, flags, div, p)) {
+        split32_solve(c, div, p, iterations, omega, flags, nullptr);
+        return;
+    }
     const size_t n = (size_t)c.num_voxels();
     float* tmp = c.scratch_f32("rbgs_pingpong", n);
     // Ping-pong so that the last iteration writes into p.
@@ -416,7 +420,8 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
     return guarded([&] {
         Context* c = check_ctx(ctx);
         if (option == HNS_OPT_RBGS_KERNEL) {
-            if (value != HNS_RBGS_PLAIN && value != HNS_RBGS_BULK) fail(HNS_ERR_INVALID_ARG, "unknown red-black kernel");
+            if (value != HNS_RBGS_PLAIN && value != HNS_RBGS_BULK && value != HNS_RBGS_SPLIT)
+                fail(HNS_ERR_INVALID_ARG, "unknown red-black kernel");
             c->rbgs_kernel = value;
         } else if (option == HNS_OPT_INNER_LAYOUT) {
             if (value != HNS_INNER_ROWS && value != HNS_INNER_PACKED && value != HNS_INNER_SPLIT)

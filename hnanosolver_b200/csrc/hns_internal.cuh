@@ -167,7 +167,7 @@ struct Context {
     DeviceBuffer d_counters;
     unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
     bool profiling = false;
-    int rbgs_kernel = HNS_RBGS_BULK;      // hns_set_option(HNS_OPT_RBGS_KERNEL)
+    int rbgs_kernel = HNS_RBGS_SPLIT;     // hns_set_option(HNS_OPT_RBGS_KERNEL)
     int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
     struct PhaseEvent {
@@ -194,8 +194,15 @@ struct Context {
     double refine_echo_tol = 0.0;   // its tolerance
     int refine_forecast = 0;        // outer iterations the last read-back solve needed; 0: unknown
     static constexpr int kEchoSlots = 2 * (64 + 1);
-    // The colour-split inner solve's e and face-table buffers whose zero leaf and table are made.
-    const void* split_setup[2] = {nullptr, nullptr};
+    // Colour-split solves: the face-table buffer whose table is built, and the e buffers whose
+    // zero leaf (past the last leaf) is cleared: the FP16 inner solve's, the FP32 solve's, the FP32
+    // inner solve's.
+    const void* split_faces_built = nullptr;
+    const void* split_zero_leaf[3] = {nullptr, nullptr, nullptr};
+    // The face table (built once) and a colour-split e buffer of n + 512 elements of `bytes`
+    // each whose zero leaf is cleared once (which: index into split_zero_leaf).
+    int* split_faces();
+    void* split_e(const char* name, size_t bytes, int which);
     mutable int sms = 0;
     int sm_count() const;  // multiprocessors of the device (queried once)
 
@@ -279,6 +286,18 @@ void launch_split_face_table(const Context& c, int* nb8);
 // refinement converged and return at once.
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
                             float omega, const double* check, double tol2, bool short_grid = false);
+// The FP32 half-sweep on colour-split leaves (the reference's update and precision): rhs the
+// divergence in the split layout, scaled by dx2 in each update; e in place with the zero leaf.
+// Launches with e_zero false are programmatic dependent launches: pdl false for one that follows
+// a kernel other than a half-sweep.
+void launch_rbgs_split_half_f32(const Context& c, const int* nb8, const float* rhs, float* e, int colour, bool e_zero,
+                                float omega, float dx2, const double* check, double tol2, bool short_grid = false,
+                                bool pdl = true);
+// FP32 slot order <-> colour-split order (n values).
+void convert_split_f32(const Context& c, const float* src, float* dst, bool to_split);
+// acc += {sum r^2, sum b^2} of the FP32 split iterate e (FP64), unless check has passed.
+void launch_split_residual_f32(const Context& c, const int* nb8, const float* rhs, const float* e, double h2,
+                               const double* check, double tol2, double* acc);
 void launch_rbgs_packed_half(const Context& c, const void* rhs, const void* halo, const void* e_in, const void* faces_in,
                              void* e_out, void* faces_out, float omega, const double* check, double tol2);
 
@@ -330,6 +349,10 @@ void launch_div_combust_buoy(const Context& c, const float* vel, float* vel_out,
 
 // Runs `iterations` fused RBGS iterations from `p` (or zero) and leaves the result in `p`.
 void rbgs_solve(Context& c, const float* div, float* p, int iterations, float omega, unsigned flags);
+// The FP32 solve on colour-split leaves (hns_step.cu): whether a solve with these flags takes it,
+// and the solve (plan: the convergence checks of rbgs_solve_checked, or null).
+bool use_split32(const Context& c, unsigned flags, const float* div, const float* p);
+void split32_solve(Context& c, const float* div, float* p, int K, float omega, unsigned flags, const SolvePlan* plan);
 
 // Convergence-checked solve: at most `max_iterations` (rounded up to even) iterations; the
 // FP64 residual of the iterate is evaluated inside the sweep every `check_every` iterations

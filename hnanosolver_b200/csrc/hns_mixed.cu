@@ -699,22 +699,19 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     const double h2 = (double)c.dx * (double)c.dx;
     const double tol2 = tol * tol;
     const unsigned g = stream_blocks(c, n);
-    // The FP16 inner solve's layout is an option (colour-split, colour-packed or plain order).
-    const int layout = sizeof(TI) == 2 ? c.inner_layout : HNS_INNER_ROWS;
+    // The FP16 inner solve's layout is an option (colour-split, colour-packed or plain order); the
+    // FP32 inner solve takes the colour-split layout with the colour-split FP32 kernel.
+    const int layout = sizeof(TI) == 2 ? c.inner_layout
+                                       : (c.rbgs_kernel == HNS_RBGS_SPLIT ? HNS_INNER_SPLIT : HNS_INNER_ROWS);
     const bool packed = layout == HNS_INNER_PACKED;
-    // Colour-split: e in place with one extra all-zero leaf, and the face-neighbour table.
+    // Colour-split: e in place with one extra all-zero leaf, and the face-neighbour table (both
+    // depend on the topology alone: made once per buffer).
     TI* e_split = nullptr;
     int* nb8 = nullptr;
     if (layout == HNS_INNER_SPLIT) {
-        e_split = reinterpret_cast<TI*>(c.scratch_f32("refine_e_split", ((size_t)(n + 512) * sizeof(TI) + 3) / 4));
-        nb8 = reinterpret_cast<int*>(c.scratch_f32("refine_split_nb8", (size_t)c.topo.num_leaves * 8));
-        // The zero leaf and the face table depend on the topology alone: made once per buffer.
-        if (c.split_setup[0] != e_split || c.split_setup[1] != nb8) {
-            HNS_CUDA(cudaMemsetAsync(e_split + n, 0, 512 * sizeof(TI), c.stream));
-            launch_split_face_table(c, nb8);
-            c.split_setup[0] = e_split;
-            c.split_setup[1] = nb8;
-        }
+        e_split = sizeof(TI) == 2 ? static_cast<TI*>(c.split_e("refine_e_split", sizeof(TI), 0))
+                                  : static_cast<TI*>(c.split_e("refine_e_split32", sizeof(TI), 2));
+        nb8 = c.split_faces();
     }
     // Packed: the face buffers of e[0] and e[1] and the rhs halo records.
     void* faces[2] = {nullptr, nullptr};
@@ -782,6 +779,13 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                     src_faces = faces[it & 1];
                 } else
                     launch_rbgs_bulk_half(c, rhat, src, dst, omega, chk, tol2);
+            } else if (layout == HNS_INNER_SPLIT) {
+                // In place on the FP32 colour-split e: red, then black (unit dx^2).
+                dst = e_split;
+                auto* ef = reinterpret_cast<float*>(dst);
+                const auto* rf = reinterpret_cast<const float*>(rhat);
+                launch_rbgs_split_half_f32(c, nb8, rf, ef, 0, it == 0, omega, 1.0f, chk, tol2, spare);
+                launch_rbgs_split_half_f32(c, nb8, rf, ef, 1, false, omega, 1.0f, chk, tol2, spare);
             } else
                 launch_rbgs_bulk_unit(c, reinterpret_cast<const float*>(rhat), reinterpret_cast<const float*>(src),
                                       reinterpret_cast<float*>(dst), omega, chk, tol2);

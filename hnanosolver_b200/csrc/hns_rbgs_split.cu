@@ -192,7 +192,241 @@ __global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half
     }
 }
 
+// ---- FP32 ---------------------------------------------------------------------------------
+// The same half-sweep on FP32 values, the reference's precision: the colour-split layout of e
+// with rows of 4 floats (16 bytes), the right-hand side the divergence in the same layout, and
+// the update of redBlackGaussSeidelUpdate as the staged FP32 kernel computes it:
+// pgs = (x+ + x- + y+ + y- + z+ + z- - div dx^2) * 0.166666667f, p = p + omega (pgs - p), so the
+// two kernels give the same values. Rows of 16 bytes hold twice the registers of the FP16 rows:
+// two leaves per thread.
+constexpr int kF32LeavesPerBlock = 2;
+constexpr int kF32LeavesPerThread = 2;
+constexpr int kF32Threads = 64 * kF32LeavesPerBlock;
+constexpr int kF32ShortGridCtasPerSm = 8;
+
+__device__ __forceinline__ float4 ldf4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ float4 ldf4_rw(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float at4(const float4& v, int j) { return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w)); }
+
+__device__ __forceinline__ float relax_f32(float xp, float xm, float yp, float ym, float zp, float zm, float b, float c,
+                                           float omega, float dx2) {
+    const float sum = xp + xm + yp + ym + zp + zm;
+    const float pgs = (sum - b * dx2) * dev::kInv6;
+    return c + omega * (pgs - c);
+}
+
+template <int P>
+__device__ __forceinline__ float4 relax_row_f32(float4 XP, float4 XM, float4 YP, float4 YM, float4 K, float ZC, float4 B,
+                                                float4 C, float omega, float dx2) {
+    float v[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float zm = P ? at4(K, j) : (j > 0 ? at4(K, j - 1) : ZC);
+        const float zp = P ? (j < 3 ? at4(K, j + 1) : ZC) : at4(K, j);
+        v[j] = relax_f32(at4(XP, j), at4(XM, j), at4(YP, j), at4(YM, j), zp, zm, at4(B, j), at4(C, j), omega, dx2);
+    }
+    return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// rbgs_split_half_kernel on FP32 (see there); dx2 scales the right-hand side.
+template <bool kZero>
+__global__ void __launch_bounds__(kF32Threads, kF32ShortGridCtasPerSm)
+    rbgs_split_half_f32_kernel(const int* __restrict__ nb8, const float* __restrict__ rhs, float* e, int num_leaves,
+                               int colour, float omega, float dx2, const double* __restrict__ check, double tol2,
+                               unsigned long long* __restrict__ counters) {
+    if (check != nullptr && check[0] <= tol2 * check[1]) return;
+    if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, 1ull);
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
+    const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
+    const int p = (w + colour) & 1;
+    const uint32_t rowc = ((uint32_t)colour << 8) | (uint32_t)(4 * (32 * w + lane));
+    constexpr int kPer = kF32LeavesPerBlock * kF32LeavesPerThread;
+    const int groups = (num_leaves + kPer - 1) / kPer;
+    for (int g = blockIdx.x; g < groups; g += gridDim.x) {
+        const int leaf0 = g * kPer + (int)(threadIdx.x >> 6);
+        uint32_t own[kF32LeavesPerThread];
+        bool live[kF32LeavesPerThread];
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k) {
+            const int leaf = leaf0 + k * kF32LeavesPerBlock;
+            live[k] = leaf < num_leaves;
+            own[k] = ((uint32_t)(live[k] ? leaf : 0) << 9) | rowc;
+        }
+        float4 B[kF32LeavesPerThread], out[kF32LeavesPerThread];
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k) B[k] = ldf4(rhs + own[k]);
+        if constexpr (kZero) {
+#pragma unroll
+            for (int k = 0; k < kF32LeavesPerThread; ++k) {
+                float v[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) v[j] = relax_f32(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, at4(B[k], j), 0.f, omega, dx2);
+                out[k] = make_float4(v[0], v[1], v[2], v[3]);
+                if (live[k]) *reinterpret_cast<float4*>(e + (own[k] ^ 256u)) = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        } else {
+            const uint32_t co = ((uint32_t)(colour ^ 1) << 8) | (uint32_t)(128 * (w ^ 1));
+            auto row = [&](uint32_t n, int a2, int b2) { return (n << 9) | co | (uint32_t)(16 * a2 + 4 * (b2 >> 1)); };
+            const int sx = a == 7 ? 0 : a == 0 ? 1 : 6, sy = b == 7 ? 2 : b == 0 ? 3 : 6, sz = 5 - p;
+            uint32_t nx[kF32LeavesPerThread], ny[kF32LeavesPerThread], nz[kF32LeavesPerThread];
+#pragma unroll
+            for (int k = 0; k < kF32LeavesPerThread; ++k) {
+                const int* nb = nb8 + 8 * (own[k] >> 9);
+                nx[k] = (uint32_t)__ldg(nb + sx);
+                ny[k] = (uint32_t)__ldg(nb + sy);
+                nz[k] = (uint32_t)__ldg(nb + sz);
+            }
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+            float4 C[kF32LeavesPerThread], K[kF32LeavesPerThread], XP[kF32LeavesPerThread], XM[kF32LeavesPerThread],
+                YP[kF32LeavesPerThread], YM[kF32LeavesPerThread];
+            float ZC[kF32LeavesPerThread];
+#pragma unroll
+            for (int k = 0; k < kF32LeavesPerThread; ++k) {
+                C[k] = ldf4_rw(e + own[k]);
+                K[k] = ldf4(e + (own[k] ^ 256u));
+            }
+#pragma unroll
+            for (int k = 0; k < kF32LeavesPerThread; ++k) {
+                const uint32_t lf = own[k] >> 9;
+                XP[k] = ldf4(e + row(a == 7 ? nx[k] : lf, (a + 1) & 7, b));
+                XM[k] = ldf4(e + row(a == 0 ? nx[k] : lf, (a - 1) & 7, b));
+                YP[k] = ldf4(e + row(b == 7 ? ny[k] : lf, a, (b + 1) & 7));
+                YM[k] = ldf4(e + row(b == 0 ? ny[k] : lf, a, (b - 1) & 7));
+                ZC[k] = __ldg(e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1));
+            }
+#pragma unroll
+            for (int k = 0; k < kF32LeavesPerThread; ++k)
+                out[k] = p ? relax_row_f32<1>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2)
+                           : relax_row_f32<0>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2);
+        }
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k)
+            if (live[k]) *reinterpret_cast<float4*>(e + own[k]) = out[k];
+    }
+}
+
+// Entry base of the half row (z = 4h .. 4h + 3) that starts at slot q (a multiple of 4), in the
+// colour block of its z = 4h voxel, and that colour (p0); z = 4h + 1 and 4h + 3 sit at the same
+// entries of the other colour.
+__device__ __forceinline__ int64_t split_base(int64_t q, int& p0) {
+    const int loc = (int)(q & 511), a = loc >> 6, b = (loc >> 3) & 7, h = (loc >> 2) & 1;
+    p0 = (a + b) & 1;
+    return (q & ~int64_t(511)) + 4 * (32 * p0 + 4 * a + (b >> 1)) + 2 * h;
+}
+
+// FP32 slot order <-> colour-split order, four values per thread.
+__global__ void __launch_bounds__(256) to_split_f32_kernel(const float* __restrict__ src, float* __restrict__ dst, int64_t n) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < (n >> 2); u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = u << 2;
+        int p0;
+        const int64_t base = split_base(q, p0);
+        const float4 v = __ldg(reinterpret_cast<const float4*>(src + q));
+        *reinterpret_cast<float2*>(dst + base + ((int64_t)p0 << 8)) = make_float2(v.x, v.z);
+        *reinterpret_cast<float2*>(dst + base + ((int64_t)(p0 ^ 1) << 8)) = make_float2(v.y, v.w);
+    }
+}
+
+__global__ void __launch_bounds__(256) from_split_f32_kernel(const float* __restrict__ src, float* __restrict__ dst, int64_t n) {
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < (n >> 2); u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = u << 2;
+        int p0;
+        const int64_t base = split_base(q, p0);
+        const float2 x = __ldg(reinterpret_cast<const float2*>(src + base + ((int64_t)p0 << 8)));
+        const float2 y = __ldg(reinterpret_cast<const float2*>(src + base + ((int64_t)(p0 ^ 1) << 8)));
+        *reinterpret_cast<float4*>(dst + q) = make_float4(x.x, y.x, x.y, y.y);
+    }
+}
+
+// The FP64 residual {sum r^2, sum b^2} of the iterate e (FP32, colour-split), r = div dx^2 -
+// (x+ + x- + y+ + y- + z+ + z- - 6 p), the staged kernel's residual per voxel, into acc. One
+// thread per row of a leaf (both colours, 8 voxels), 2 leaves per CTA, one wave looping; returns
+// at once when `check` has passed.
+__global__ void __launch_bounds__(128) split_residual_f32_kernel(const int* __restrict__ nb8, const float* __restrict__ rhs,
+                                                                 const float* __restrict__ e, int num_leaves, double h2,
+                                                                 const double* __restrict__ check, double tol2,
+                                                                 double* __restrict__ acc) {
+    if (check != nullptr && check[0] <= tol2 * check[1]) return;
+    const int r = threadIdx.x & 63, a = r >> 3, b = r & 7, par = (a + b) & 1;
+    const uint32_t rp = (uint32_t)(4 * (32 * par + 4 * a + (b >> 1)));  // this row's entries in each colour block
+    auto rowpos = [](int a2, int b2) { return (uint32_t)(4 * (32 * ((a2 + b2) & 1) + 4 * a2 + (b2 >> 1))); };
+    // The row's 8 values from its two colour blocks: z = 2 j + ((a + b + c) & 1) is entry j of colour c.
+    auto row8 = [&](uint32_t leaf, uint32_t pos, int parity, float v[8]) {
+        const float4 c0 = ldf4(e + (leaf << 9) + pos), c1 = ldf4(e + (leaf << 9) + 256u + pos);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[2 * j + parity] = at4(c0, j);
+            v[2 * j + (parity ^ 1)] = at4(c1, j);
+        }
+    };
+    double r2 = 0.0, b2 = 0.0;
+    const int groups = (num_leaves + 1) / 2;
+    for (int g = blockIdx.x; g < groups; g += gridDim.x) {
+        const int leaf = 2 * g + (int)(threadIdx.x >> 6);
+        if (leaf >= num_leaves) continue;
+        const int* nb = nb8 + 8 * leaf;
+        const uint32_t lf = (uint32_t)leaf;
+        const uint32_t nxp = a == 7 ? (uint32_t)__ldg(nb + 0) : lf, nxm = a == 0 ? (uint32_t)__ldg(nb + 1) : lf;
+        const uint32_t nyp = b == 7 ? (uint32_t)__ldg(nb + 2) : lf, nym = b == 0 ? (uint32_t)__ldg(nb + 3) : lf;
+        const uint32_t nzp = (uint32_t)__ldg(nb + 4), nzm = (uint32_t)__ldg(nb + 5);
+        float c[8], xp[8], xm[8], yp[8], ym[8], bv[8];
+        row8(lf, rp, par, c);
+        row8(nxp, rowpos((a + 1) & 7, b), par ^ 1, xp);
+        row8(nxm, rowpos((a - 1) & 7, b), par ^ 1, xm);
+        row8(nyp, rowpos(a, (b + 1) & 7), par ^ 1, yp);
+        row8(nym, rowpos(a, (b - 1) & 7), par ^ 1, ym);
+        {
+            const float4 c0 = ldf4(rhs + (lf << 9) + rp), c1 = ldf4(rhs + (lf << 9) + 256u + rp);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) bv[2 * j + par] = at4(c0, j), bv[2 * j + (par ^ 1)] = at4(c1, j);
+        }
+        // Across the z faces: z = 7 of the -z leaf's row (entry 3 of colour (a + b + 1) & 1), z = 0
+        // of the +z leaf's row (entry 0 of colour (a + b) & 1).
+        const float zlo = __ldg(e + (nzm << 9) + ((uint32_t)(par ^ 1) << 8) + rp + 3u);
+        const float zhi = __ldg(e + (nzp << 9) + ((uint32_t)par << 8) + rp);
+#pragma unroll
+        for (int z = 0; z < 8; ++z) {
+            const double lap = (double)xp[z] + (double)xm[z] + (double)yp[z] + (double)ym[z] +
+                               (double)(z < 7 ? c[z + 1] : zhi) + (double)(z > 0 ? c[z - 1] : zlo) - 6.0 * (double)c[z];
+            const double bb = (double)bv[z] * h2;
+            r2 += (bb - lap) * (bb - lap);
+            b2 += bb * bb;
+        }
+    }
+    __shared__ double red[2][4];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+        b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+    }
+    if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = r2, red[1][threadIdx.x >> 5] = b2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(acc, red[0][0] + red[0][1] + red[0][2] + red[0][3]);
+        atomicAdd(acc + 1, red[1][0] + red[1][1] + red[1][2] + red[1][3]);
+    }
+}
+
 }  // namespace
+
+int* Context::split_faces() {
+    int* nb8 = reinterpret_cast<int*>(scratch_f32("split_faces", (size_t)topo.num_leaves * 8));
+    if (split_faces_built != nb8) {
+        launch_split_face_table(*this, nb8);
+        split_faces_built = nb8;
+    }
+    return nb8;
+}
+
+void* Context::split_e(const char* name, size_t bytes, int which) {
+    const size_t n = (size_t)num_voxels();
+    char* e = reinterpret_cast<char*>(scratch_f32(name, ((n + 512) * bytes + 3) / 4));
+    if (split_zero_leaf[which] != e) {
+        HNS_CUDA(cudaMemsetAsync(e + n * bytes, 0, 512 * bytes, stream));
+        split_zero_leaf[which] = e;
+    }
+    return e;
+}
 
 void launch_split_face_table(const Context& c, int* nb8) {
     const int64_t L = c.topo.num_leaves;
@@ -237,6 +471,65 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     cfg.numAttrs = na;
     HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<false>, nb8, r, x, (int)L, colour, omega, check, tol2,
                                 c.counters));
+    HNS_LAUNCHED();
+}
+
+}  // namespace hns
+
+namespace hns {
+
+void launch_rbgs_split_half_f32(const Context& c, const int* nb8, const float* rhs, float* e, int colour, bool e_zero,
+                                float omega, float dx2, const double* check, double tol2, bool short_grid, bool pdl) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0) return;
+    if (L >= (int64_t(1) << 22)) fail(HNS_ERR_INVALID_ARG, "too many leaves for the colour-split solve");
+    const int per_block = kF32LeavesPerBlock * kF32LeavesPerThread;
+    unsigned blocks = (unsigned)((L + per_block - 1) / per_block);
+    if (short_grid) blocks = std::min(blocks, (unsigned)(c.sm_count() * kF32ShortGridCtasPerSm));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kF32Threads);
+    cfg.stream = c.stream;
+    if (e_zero) {
+        HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_f32_kernel<true>, nb8, rhs, e, (int)L, colour, omega, dx2, check,
+                                    tol2, c.counters));
+        HNS_LAUNCHED();
+        return;
+    }
+    if (!pdl) {
+        HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_f32_kernel<false>, nb8, rhs, e, (int)L, colour, omega, dx2, check,
+                                    tol2, c.counters));
+        HNS_LAUNCHED();
+        return;
+    }
+    // Programmatic dependent launch, as the FP16 half-sweep (launch_rbgs_split_half).
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_f32_kernel<false>, nb8, rhs, e, (int)L, colour, omega, dx2, check,
+                                tol2, c.counters));
+    HNS_LAUNCHED();
+}
+
+void convert_split_f32(const Context& c, const float* src, float* dst, bool to_split) {
+    const int64_t n = c.num_voxels();
+    if (n == 0) return;
+    const unsigned g = (unsigned)std::min<int64_t>((n / 4 + 255) / 256, (int64_t)c.sm_count() * 16);
+    if (to_split)
+        to_split_f32_kernel<<<g, 256, 0, c.stream>>>(src, dst, n);
+    else
+        from_split_f32_kernel<<<g, 256, 0, c.stream>>>(src, dst, n);
+    HNS_LAUNCHED();
+}
+
+void launch_split_residual_f32(const Context& c, const int* nb8, const float* rhs, const float* e, double h2,
+                               const double* check, double tol2, double* acc) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0) return;
+    const unsigned g = (unsigned)std::min<int64_t>((L + 1) / 2, (int64_t)c.sm_count() * 8);
+    split_residual_f32_kernel<<<g, 128, 0, c.stream>>>(nb8, rhs, e, (int)L, h2, check, tol2, acc);
     HNS_LAUNCHED();
 }
 

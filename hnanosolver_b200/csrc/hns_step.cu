@@ -13,6 +13,60 @@
 
 namespace hns {
 
+// The FP32 colour-split workspace: the right-hand side and e (with the zero leaf after the last
+// leaf) in the split layout, and the face table (shared with the FP16 inner solve's).
+struct Split32 {
+    float* rhs;
+    float* e;
+    int* nb8;
+};
+
+Split32 split32_workspace(Context& c) {
+    Split32 w;
+    w.rhs = c.scratch_f32("split32_rhs", (size_t)c.num_voxels());
+    w.e = static_cast<float*>(c.split_e("split32_e", sizeof(float), 1));
+    w.nb8 = c.split_faces();
+    return w;
+}
+
+// `K` red-black iterations of the FP32 solve on colour-split leaves, result in p (slot order):
+// the divergence and (unless HNS_SOLVE_ZERO_INIT) p are converted in, the half-sweeps run in place,
+// and e is converted out. With a plan, the residual of the iterate check c reads is evaluated
+// before iteration (c + 1) E - 1 into its slot and every later half-sweep tests the latest slot,
+// the schedule of the staged kernel (rbgs_solve_checked), so both give the same iterates.
+void split32_solve(Context& c, const float* div, float* p, int K, float omega, unsigned flags, const SolvePlan* plan) {
+    const Split32 w = split32_workspace(c);
+    const float dx2 = c.dx * c.dx;
+    convert_split_f32(c, div, w.rhs, true);
+    const bool zero = (flags & HNS_SOLVE_ZERO_INIT) != 0;
+    if (!zero) convert_split_f32(c, p, w.e, true);
+    const double tol2 = plan ? plan->tol * plan->tol : 0.0;
+    bool after_half = false;  // the preceding kernel on the stream is a half-sweep
+    for (int it = 0; it < K; ++it) {
+        const double* chk = nullptr;
+        if (plan) {
+            const int E = plan->check_every;
+            const int last_check = it / E - 1;
+            chk = last_check >= 0 ? plan->slots + 2 * last_check : nullptr;
+            if ((it + 1) % E == 0) {
+                launch_split_residual_f32(c, w.nb8, w.rhs, w.e, (double)dx2, chk, tol2, plan->slots + 2 * ((it + 1) / E - 1));
+                after_half = false;
+            }
+        }
+        launch_rbgs_split_half_f32(c, w.nb8, w.rhs, w.e, 0, zero && it == 0, omega, dx2, chk, tol2, false, after_half);
+        launch_rbgs_split_half_f32(c, w.nb8, w.rhs, w.e, 1, false, omega, dx2, chk, tol2, false, true);
+        after_half = true;
+    }
+    convert_split_f32(c, w.e, p, false);
+}
+
+bool use_split32(const Context& c, unsigned flags, const float* div, const float* p) {
+    // The layout conversions move 16-byte vectors of div and p.
+    auto a16 = [](const float* q) { return ((uintptr_t)q & 15u) == 0; };
+    return c.rbgs_kernel == HNS_RBGS_SPLIT && !(flags & HNS_SOLVE_NEUMANN) && c.topo.num_leaves < (int64_t(1) << 22) &&
+           a16(div) && a16(p);
+}
+
 // Schedule: iterations 0..K-1 (K even). Check c is evaluated inside iteration
 // k_c = (c+1)E - 1 (E even, so k_c is odd) on the iterate that iteration reads; every later
 // iteration reads the latest check's slot and returns at once if it passed. Skipping thus
@@ -35,6 +89,11 @@ SolvePlan rbgs_solve_checked(Context& c, const float* div, float* p, int max_ite
     plan.tol = tol;
     plan.slots = c.reduce_slots(8 + 2 * std::max(1, plan.num_checks)) + 8;  // first 8 doubles: exact residuals
     HNS_CUDA(cudaMemsetAsync(plan.slots, 0, sizeof(double) * 2 * (size_t)std::max(1, plan.num_checks), c.stream));
+    if (use_split32(c, flags, div, p)) {
+        split32_solve(c, div, p, K, omega, flags, &plan);
+        log_solve(c, plan.slots, plan.num_checks, tol, E, 1, K);
+        return plan;
+    }
     const size_t n = (size_t)c.num_voxels();
     float* tmp = c.scratch_f32("rbgs_pingpong", n);
     const float* src = (flags & HNS_SOLVE_ZERO_INIT) ? nullptr : p;

@@ -20,7 +20,7 @@ STATUS_NAMES = {
     5: "HNS_ERR_LAYOUT", 6: "HNS_ERR_NOT_CONVERGED", 7: "HNS_ERR_UNSUPPORTED", 8: "HNS_ERR_TIMEOUT",
 }
 OPT_RBGS_KERNEL = 1
-RBGS_PLAIN, RBGS_BULK = 0, 1
+RBGS_PLAIN, RBGS_BULK, RBGS_SPLIT = 0, 1, 2
 OPT_INNER_LAYOUT = 2
 INNER_ROWS, INNER_PACKED, INNER_SPLIT = 0, 1, 2
 OPT_WAIT_POLLS = 3

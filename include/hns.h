@@ -468,9 +468,11 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
 
 /* ---- options ----------------------------------------------------------------------------- */
 #define HNS_OPT_RBGS_KERNEL 1 /* which red-black kernel: */
-#define HNS_RBGS_PLAIN 0      /*   plain loads into a padded halo tile */
-#define HNS_RBGS_BULK 1       /*   bulk async copies of the contiguous leaf payload (default;
-                                   used when div and p are 16-byte aligned) */
+#define HNS_RBGS_PLAIN 0      /*   plain loads into a padded halo tile (also the zero-gradient walls' kernel) */
+#define HNS_RBGS_BULK 1       /*   bulk async copies of the contiguous leaf payload into a staged tile, both
+                                   colours per launch (used when div and p are 16-byte aligned) */
+#define HNS_RBGS_SPLIT 2      /*   the solve on colour-split leaves, one in-place launch per colour, no
+                                   staging (default). The three give the same results to the bit. */
 #define HNS_OPT_INNER_LAYOUT 2 /* layout of the FP16 inner solve of the mixed-precision refinement: */
 #define HNS_INNER_ROWS 0       /*   the leaf-dense slot order, relaxed by the HNS_RBGS_BULK kernel */
 #define HNS_INNER_PACKED 1     /*   colour-packed rows (z = 0,2,4,6 then 1,3,5,7) with face buffers,

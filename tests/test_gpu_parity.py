@@ -151,10 +151,11 @@ def test_project(case, dev):
     assert info.initial_residual == pytest.approx(1.0, rel=1e-9)
 
 
-@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("kernel", [0, 1, 2])
 @pytest.mark.parametrize("iters,zero", [(1, True), (6, False), (11, True)])
 def test_rbgs_kernels_bit_exact(case, dev, kernel, iters, zero):
-    """Both red-black kernels (plain-load halo tile, bulk async copies) equal the oracle."""
+    """The three FP32 red-black kernels (plain-load halo tile, bulk async copies into a staged
+    tile, colour-split leaves) equal the oracle."""
     from conftest import bit_exact
     from hnanosolver_b200 import lib as hl
 
@@ -166,7 +167,7 @@ def test_rbgs_kernels_bit_exact(case, dev, kernel, iters, zero):
     g.rbgs(T(div, dev), p, iters, 1.8, hl.SOLVE_ZERO_INIT if zero else 0)
     g.device_status()
     assert bit_exact(H(p), t.rbgs(div, p0, 0.1, iters, 1.8))
-    g.set_option(hl.OPT_RBGS_KERNEL, hl.RBGS_BULK)
+    g.set_option(hl.OPT_RBGS_KERNEL, hl.RBGS_SPLIT)
 
 
 def test_rbgs_unaligned_pointers_fall_back(case, dev):

@@ -31,6 +31,8 @@ def test_bounded_copy_wait_gives_up_then_recovers(dev):
     n = len(dens)
     clean = hl.Grid(origins, voxel_size=0.1)
     grid = hl.Grid(origins, voxel_size=0.1)
+    for g in (clean, grid):  # the staged kernel, whose copies the bounded wait guards
+        g.set_option(hl.OPT_RBGS_KERNEL, hl.RBGS_BULK)
     v = torch.from_numpy(vel).to(dev)
     div = torch.empty(n, device=dev)
     p_ref = torch.zeros(n, device=dev)
