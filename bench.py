@@ -53,6 +53,12 @@ WORKLOADS = {
                      check_every=10, fp32_iterations=None),
 }
 RBGS_BYTES_PER_VOXEL = 12  # one fused red+black iteration: read p, read div, write p (FP32)
+# The solve kernels' unit of work is a half-sweep (one colour): half an iteration's pass-model
+# bytes, counted by the library's device counter of red-black sweeps that ran.
+F32_HALF_SWEEP_BYTES = RBGS_BYTES_PER_VOXEL // 2
+F16_HALF_SWEEP_BYTES = 3  # read e, read r, write e at 2 bytes each, halved
+F32_KERNEL = "rbgs_split_solve_kernel<float> (FP32 solve, colour-split leaves, persistent: one launch per run of half-sweeps between checks)"
+F16_KERNEL = "rbgs_split_solve_kernel<__half> (FP16 inner solve, colour-split leaves, persistent: one launch per inner solve)"
 
 # The fire step (HNS_Advance with the configurations' forces): the sparse plume runs it in FP32
 # with a fixed 100 red-black iterations per step, the large sparse fire on BF16/FP16 storage with
@@ -495,16 +501,12 @@ def ours(args, wl):
         # record packing, advection, divergence, first residual, convergence log, gradient; per
         # outer iteration scale, 2 half-sweeps per inner iteration, update, residual (the face
         # table is made once per context).
-        launches_per_step = 6 + outer * (3 + 2 * wl["inner"])
-        # One launch is a half-sweep: half of an iteration's pass-model bytes (read e, read r,
-        # write e at 2 bytes each).
-        kernel_bytes, kernel_name, phase = 3, "rbgs_split_half_kernel (FP16 inner solve, colour-split, one colour per launch)", "inner"
+        kernel_bytes, kernel_name, phase = F16_HALF_SWEEP_BYTES, F16_KERNEL, "inner"
     else:
         info, outer = info32, None
         st = plain_desc(cap32)
         step = step32(st)
-        launches_per_step = 4 + cap32
-        kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_stream_kernel<float>", "solve"
+        kernel_bytes, kernel_name, phase = F32_HALF_SWEEP_BYTES, F32_KERNEL, "solve"
 
     for _ in range(args.warmup):
         step()
@@ -591,7 +593,7 @@ def ours(args, wl):
             "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 16 * n, "steps": e2e_steps,
                     "path": ("hns_step_mixed_host" if mixed else "hns_step_plain_host") + " (C ABI, pinned FP32 host buffers)"},
-            "gpu_launches": args.steps * launches_per_step,
+            "gpu_launches": int(prof.kernel_launches),
             "clocks": clk,
             "adjoint": adjoint,
         }
@@ -864,8 +866,7 @@ def ours_fire(args, wl):
         # record packing, velocity advection, confinement, divergence/burn/buoyancy, first residual,
         # convergence log, gradient, scalar advection; per outer iteration scale, 2 half-sweeps per
         # inner iteration, update, residual.
-        launches_per_step = 8 + outer * (3 + 2 * wl["inner"])
-        kernel_bytes, kernel_name, phase = 3, "rbgs_split_half_kernel (FP16 inner solve, colour-split, one colour per launch)", "inner"
+        kernel_bytes, kernel_name, phase = F16_HALF_SWEEP_BYTES, F16_KERNEL, "inner"
     else:
         load_fp32()
         iters = wl["iterations"]
@@ -876,8 +877,7 @@ def ours_fire(args, wl):
 
         # velocity advection, confinement and sources, divergence/burn/buoyancy, the red-black
         # iterations, gradient, scalar advection.
-        launches_per_step = 5 + iters
-        kernel_bytes, kernel_name, phase = RBGS_BYTES_PER_VOXEL, "rbgs_stream_kernel<float>", "solve"
+        kernel_bytes, kernel_name, phase = F32_HALF_SWEEP_BYTES, F32_KERNEL, "solve"
 
     for _ in range(args.warmup):
         step()
@@ -966,7 +966,7 @@ def ours_fire(args, wl):
             "cpu_baseline": cpu,
             "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps, "path": path},
-            "gpu_launches": args.steps * launches_per_step,
+            "gpu_launches": int(prof.kernel_launches),
             "clocks": clk,
             "adjoint": adjoint,
         }
@@ -1074,7 +1074,7 @@ def box64_ours(args):
         forms[name] = {"value": replicas.aggregate_rate(R, n, args.steps, ms), "ms_per_step": ms / args.steps,
                        "residual_after_40": info.residual, "clocks": clk,
                        "solve_ms_per_step": prof.phase_ms[hl.PHASES["solve"]] / args.steps,
-                       "launches": int(prof.solver_launches)}
+                       "launches": int(prof.solver_launches), "kernel_launches": int(prof.kernel_launches)}
     hv = torch.from_numpy(vel).pin_memory().numpy()
     hd = torch.from_numpy(dens).pin_memory().numpy()
     desc = hl.StepDesc(dt=BOX64["dt"], max_iterations=BOX64["iterations"], omega=BOX64["omega"], tolerance=0.0,
@@ -1105,7 +1105,7 @@ def box64_ours(args):
                 "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": 16 * n,
                         "d2h_bytes_per_step": 16 * n, "steps": e2e_steps,
                         "path": "hns_step_plain_host (C ABI, pinned FP32 host buffers), zero-gradient walls"},
-                "gpu_launches": args.steps * (4 + BOX64["iterations"]), "clocks": z["clocks"]}
+                "gpu_launches": z["kernel_launches"], "clocks": z["clocks"]}
         print(json.dumps(line), flush=True)
     g.close()
     replicas.finish(R)

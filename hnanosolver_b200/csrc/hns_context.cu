@@ -2,6 +2,8 @@
 // of include/hns.h.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -427,6 +429,10 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
             if (value != HNS_INNER_ROWS && value != HNS_INNER_PACKED && value != HNS_INNER_SPLIT)
                 fail(HNS_ERR_INVALID_ARG, "unknown inner layout");
             c->inner_layout = value;
+        } else if (option == HNS_OPT_SPLIT_SOLVE) {
+            if (value != HNS_SPLIT_PER_COLOUR && value != HNS_SPLIT_PERSISTENT)
+                fail(HNS_ERR_INVALID_ARG, "unknown inner-solve launch form");
+            c->split_solve = value;
         } else if (option == HNS_OPT_WAIT_POLLS) {
             if (value < -1) fail(HNS_ERR_INVALID_ARG, "the wait limit must be -1 (default) or >= 0");
             c->first_wait_polls = value;
@@ -449,7 +455,7 @@ HNS_API hns_status hns_device_status(hns_ctx* ctx) {
         }
     });
     if (s != HNS_OK) return s;
-    return flag ? record_error(HNS_ERR_TIMEOUT, "a device-side wait gave up (bulk copy did not complete)") : HNS_OK;
+    return flag ? record_error(HNS_ERR_TIMEOUT, "a device-side wait gave up (a bulk copy or a neighbour's sweep did not complete)") : HNS_OK;
 }
 
 HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable) {
@@ -458,6 +464,13 @@ HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable) {
         c->profiling = enable != 0;
     });
 }
+
+namespace hns {
+namespace {
+std::atomic<unsigned long long> g_kernel_launches{0};
+}
+void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace hns
 
 HNS_API hns_status hns_profile_read(hns_ctx* ctx, hns_profile_data* out) {
     return guarded([&] {
@@ -480,6 +493,7 @@ HNS_API hns_status hns_profile_read(hns_ctx* ctx, hns_profile_data* out) {
         HNS_CUDA(cudaMemcpy(&out->solver_launches, c->counters, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         HNS_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(unsigned long long), c->stream));
         HNS_CUDA(cudaStreamSynchronize(c->stream));
+        out->kernel_launches = g_kernel_launches.exchange(0, std::memory_order_relaxed);
     });
 }
 

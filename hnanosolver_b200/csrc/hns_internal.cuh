@@ -24,7 +24,9 @@ struct Error : std::runtime_error {
 [[noreturn]] void fail(hns_status s, const std::string& msg);
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 #define HNS_CUDA(call) ::hns::cuda_check((call), #call, __FILE__, __LINE__)
-#define HNS_LAUNCHED() ::hns::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+#define HNS_LAUNCHED() (::hns::note_launch(), ::hns::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
+// Counts the library's kernel launches (process-wide; hns_profile_read reports and resets it).
+void note_launch();
 
 hns_status record_error(hns_status s, const std::string& msg);
 void clear_error();
@@ -165,11 +167,12 @@ struct Context {
     RefinePlan last_refine; // schedule of the most recent refined solve (hns_last_refine)
     // Profiling (hns_profile_*): device counters and per-phase events on the stream.
     DeviceBuffer d_counters;
-    unsigned long long* counters = nullptr;  // [0] solver launches that ran (not skipped)
+    unsigned long long* counters = nullptr;  // [0] red-black sweeps that ran (not skipped), [1] device error flag
     bool profiling = false;
     int rbgs_kernel = HNS_RBGS_SPLIT;     // hns_set_option(HNS_OPT_RBGS_KERNEL)
     int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
+    int split_solve = HNS_SPLIT_PERSISTENT;  // hns_set_option(HNS_OPT_SPLIT_SOLVE)
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;
@@ -286,6 +289,14 @@ void launch_split_face_table(const Context& c, int* nb8);
 // refinement converged and return at once.
 void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, void* e, int colour, bool e_zero,
                             float omega, const double* check, double tol2, bool short_grid = false);
+// A whole FP16 inner solve on colour-split leaves in one cooperative launch: half_sweeps
+// half-sweeps (red first), the values of as many launch_rbgs_split_half calls to the bit. e_zero:
+// e = 0 before it. Follows any kernel (no programmatic dependency).
+void launch_rbgs_split_solve(Context& c, const int* nb8, const void* rhs, void* e, int half_sweeps, bool e_zero,
+                             float omega, const double* check, double tol2);
+// The same for the FP32 solve (the half-sweeps of launch_rbgs_split_half_f32).
+void launch_rbgs_split_solve_f32(Context& c, const int* nb8, const float* rhs, float* e, int half_sweeps, bool e_zero,
+                                 float omega, float dx2, const double* check, double tol2);
 // The FP32 half-sweep on colour-split leaves (the reference's update and precision): rhs the
 // divergence in the split layout, scaled by dx2 in each update; e in place with the zero leaf.
 // Launches with e_zero false are programmatic dependent launches: pdl false for one that follows

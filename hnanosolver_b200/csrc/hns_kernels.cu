@@ -500,7 +500,8 @@ void launch_rbgs_iteration(const Context& c, const float* div, const float* p_in
         HNS_LAUNCHED();
         return;
     }
-    if (c.rbgs_kernel == HNS_RBGS_BULK && rbgs_bulk_eligible(div, p_in, p_out)) {
+    // One iteration at a time (the colour-split form runs whole solves): the staged kernel.
+    if ((c.rbgs_kernel == HNS_RBGS_BULK || c.rbgs_kernel == HNS_RBGS_SPLIT) && rbgs_bulk_eligible(div, p_in, p_out)) {
         launch_rbgs_bulk(c, div, p_in, p_out, omega, check, tol2, resid_out);
         return;
     }

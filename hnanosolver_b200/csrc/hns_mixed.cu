@@ -766,7 +766,17 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         const TI* src = nullptr;
         const void* src_faces = nullptr;
         c.phase_begin(HNS_PHASE_INNER);
-        for (int it = 0; it < plan.inner; ++it) {
+        // The persistent form: the whole inner solve in one launch.
+        const bool persistent = layout == HNS_INNER_SPLIT && c.split_solve == HNS_SPLIT_PERSISTENT;
+        if (persistent) {
+            if constexpr (sizeof(TI) == 2)
+                launch_rbgs_split_solve(c, nb8, rhat, e_split, 2 * plan.inner, true, omega, chk, tol2);
+            else
+                launch_rbgs_split_solve_f32(c, nb8, reinterpret_cast<const float*>(rhat), reinterpret_cast<float*>(e_split),
+                                            2 * plan.inner, true, omega, 1.0f, chk, tol2);
+            src = e_split;
+        }
+        for (int it = 0; it < (persistent ? 0 : plan.inner); ++it) {
             TI* dst = e[it & 1];
             if constexpr (sizeof(TI) == 2) {
                 if (layout == HNS_INNER_SPLIT) {

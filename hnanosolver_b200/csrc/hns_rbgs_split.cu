@@ -95,8 +95,15 @@ __device__ __forceinline__ uint2 relax_row(uint2 XP, uint2 XM, uint2 YP, uint2 Y
     return make_uint2(pack2(v[0], v[1]), pack2(v[2], v[3]));
 }
 
+// One CTA pass of a half-sweep: relax the rows of colour `colour` in leaf group g (the
+// kLeavesPerBlock * kLeavesPerThread leaves from g * kLeavesPerGroup).
+//
 // kZero: e = 0 before this (red) half-sweep, the first of a solve: every neighbour and old
 // value is 0, nothing of e is read, and the row's black entries are written as 0.
+// kShared: other CTAs of the same launch write e (the persistent solve): every load of e takes
+// the coherent path; otherwise the colour not being updated is read-only during the launch and
+// goes through the read-only cache. kPdl: wait for the preceding launch (griddepcontrol.wait)
+// before the first load of e.
 //
 // Warp w of a leaf takes the 32 rows of parity w of a + b, lane l the row at R = 32 w + l
 // (a = l / 4, b = 2 (l % 4) + ((a + w) & 1)), so the z parity of the colour is uniform in a warp
@@ -105,28 +112,17 @@ __device__ __forceinline__ uint2 relax_row(uint2 XP, uint2 XM, uint2 YP, uint2 Y
 // memory latency, and this multiplies the bytes each thread has in flight. Loads are
 // unconditional: a row on a leaf face reads the neighbour leaf's row, a missing neighbour the
 // zero leaf. Offsets are 32-bit element counts (fewer than 2^22 leaves).
-template <bool kZero>
-__global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half_kernel(const int* __restrict__ nb8,
-                                                                    const __half* __restrict__ rhs, __half* e,
-                                                                    int num_leaves, int colour, float omega,
-                                                                    const double* __restrict__ check, double tol2,
-                                                                    unsigned long long* __restrict__ counters) {
-    if (check != nullptr && check[0] <= tol2 * check[1]) return;  // the refinement has converged
-    if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, 1ull);  // launches that ran
-    // The next half-sweep may be scheduled as soon as every block of this one has started: its
-    // blocks take the SM slots this launch's last wave frees and load what no sweep writes
-    // before they wait for this launch to finish.
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+constexpr int kLeavesPerGroup = kLeavesPerBlock * kLeavesPerThread;
+
+template <bool kZero, bool kShared, bool kPdl>
+__device__ __forceinline__ void relax_group(const int* __restrict__ nb8, const __half* __restrict__ rhs, __half* e,
+                                            int num_leaves, int g, int colour, float omega) {
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
     const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
     const int p = (w + colour) & 1;  // z parity of this colour in the warp's rows
     const uint32_t rowc = ((uint32_t)colour << 8) | (uint32_t)(4 * (32 * w + lane));  // own entries within a leaf
-    // Leaf groups (the leaves of one CTA pass): one per CTA in a full grid; a short grid loops.
-    // Within a launch a thread reads and writes only its own rows of the launch's colour and
-    // only reads the other colour, so the passes of a CTA are independent.
-    const int groups = (num_leaves + kLeavesPerBlock * kLeavesPerThread - 1) / (kLeavesPerBlock * kLeavesPerThread);
-    for (int g = blockIdx.x; g < groups; g += gridDim.x) {
-    const int leaf0 = g * (kLeavesPerBlock * kLeavesPerThread) + (int)(threadIdx.x >> 6);
+    auto lde = [](const __half* q) { return kShared ? ld8_rw(q) : ld8(q); };
+    const int leaf0 = g * kLeavesPerGroup + (int)(threadIdx.x >> 6);
     uint32_t own[kLeavesPerThread];
     bool live[kLeavesPerThread];
 #pragma unroll
@@ -162,24 +158,24 @@ __global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half
         }
         // e is written by the preceding half-sweep: wait until it has finished (a no-op for a
         // launch without the programmatic-serialization attribute).
-        asm volatile("griddepcontrol.wait;" ::: "memory");
+        if constexpr (kPdl) asm volatile("griddepcontrol.wait;" ::: "memory");
         uint2 C[kLeavesPerThread], K[kLeavesPerThread], XP[kLeavesPerThread], XM[kLeavesPerThread],
             YP[kLeavesPerThread], YM[kLeavesPerThread];
         uint32_t ZC[kLeavesPerThread];
 #pragma unroll
         for (int k = 0; k < kLeavesPerThread; ++k) {
             C[k] = ld8_rw(e + own[k]);
-            K[k] = ld8(e + (own[k] ^ 256u));
+            K[k] = lde(e + (own[k] ^ 256u));
         }
 #pragma unroll
         for (int k = 0; k < kLeavesPerThread; ++k) {
             const uint32_t lf = own[k] >> 9;
-            XP[k] = ld8(e + row(a == 7 ? nx[k] : lf, (a + 1) & 7, b));
-            XM[k] = ld8(e + row(a == 0 ? nx[k] : lf, (a - 1) & 7, b));
-            YP[k] = ld8(e + row(b == 7 ? ny[k] : lf, a, (b + 1) & 7));
-            YM[k] = ld8(e + row(b == 0 ? ny[k] : lf, a, (b - 1) & 7));
-            ZC[k] = (uint32_t)__half_as_ushort(
-                __ldg(e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1)));
+            XP[k] = lde(e + row(a == 7 ? nx[k] : lf, (a + 1) & 7, b));
+            XM[k] = lde(e + row(a == 0 ? nx[k] : lf, (a - 1) & 7, b));
+            YP[k] = lde(e + row(b == 7 ? ny[k] : lf, a, (b + 1) & 7));
+            YM[k] = lde(e + row(b == 0 ? ny[k] : lf, a, (b - 1) & 7));
+            const __half* zq = e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1);
+            ZC[k] = kShared ? (uint32_t)*reinterpret_cast<const unsigned short*>(zq) : (uint32_t)__half_as_ushort(__ldg(zq));
         }
 #pragma unroll
         for (int k = 0; k < kLeavesPerThread; ++k)
@@ -189,7 +185,26 @@ __global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half
 #pragma unroll
     for (int k = 0; k < kLeavesPerThread; ++k)
         if (live[k]) *reinterpret_cast<uint2*>(e + own[k]) = out[k];
-    }
+}
+
+// One half-sweep per launch. Leaf groups: one per CTA in a full grid; a short grid loops. Within
+// a launch a thread reads and writes only its own rows of the launch's colour and only reads the
+// other colour, so the passes of a CTA are independent.
+template <bool kZero>
+__global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half_kernel(const int* __restrict__ nb8,
+                                                                    const __half* __restrict__ rhs, __half* e,
+                                                                    int num_leaves, int colour, float omega,
+                                                                    const double* __restrict__ check, double tol2,
+                                                                    unsigned long long* __restrict__ counters) {
+    if (check != nullptr && check[0] <= tol2 * check[1]) return;  // the refinement has converged
+    if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, 1ull);  // half-sweeps that ran
+    // The next half-sweep may be scheduled as soon as every block of this one has started: its
+    // blocks take the SM slots this launch's last wave frees and load what no sweep writes
+    // before they wait for this launch to finish.
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int groups = (num_leaves + kLeavesPerGroup - 1) / kLeavesPerGroup;
+    for (int g = blockIdx.x; g < groups; g += gridDim.x)
+        relax_group<kZero, false, true>(nb8, rhs, e, num_leaves, g, colour, omega);
 }
 
 // ---- FP32 ---------------------------------------------------------------------------------
@@ -228,7 +243,81 @@ __device__ __forceinline__ float4 relax_row_f32(float4 XP, float4 XM, float4 YP,
     return make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// rbgs_split_half_kernel on FP32 (see there); dx2 scales the right-hand side.
+// relax_group on FP32 (see there): a pass over the kF32LeavesPerGroup leaves of group g; dx2
+// scales the right-hand side.
+constexpr int kF32LeavesPerGroup = kF32LeavesPerBlock * kF32LeavesPerThread;
+
+template <bool kZero, bool kShared, bool kPdl>
+__device__ __forceinline__ void relax_group_f32(const int* __restrict__ nb8, const float* __restrict__ rhs, float* e,
+                                                int num_leaves, int g, int colour, float omega, float dx2) {
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
+    const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
+    const int p = (w + colour) & 1;
+    const uint32_t rowc = ((uint32_t)colour << 8) | (uint32_t)(4 * (32 * w + lane));
+    auto lde = [](const float* q) { return kShared ? ldf4_rw(q) : ldf4(q); };
+    const int leaf0 = g * kF32LeavesPerGroup + (int)(threadIdx.x >> 6);
+    uint32_t own[kF32LeavesPerThread];
+    bool live[kF32LeavesPerThread];
+#pragma unroll
+    for (int k = 0; k < kF32LeavesPerThread; ++k) {
+        const int leaf = leaf0 + k * kF32LeavesPerBlock;
+        live[k] = leaf < num_leaves;
+        own[k] = ((uint32_t)(live[k] ? leaf : 0) << 9) | rowc;
+    }
+    float4 B[kF32LeavesPerThread], out[kF32LeavesPerThread];
+#pragma unroll
+    for (int k = 0; k < kF32LeavesPerThread; ++k) B[k] = ldf4(rhs + own[k]);
+    if constexpr (kZero) {
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k) {
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = relax_f32(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, at4(B[k], j), 0.f, omega, dx2);
+            out[k] = make_float4(v[0], v[1], v[2], v[3]);
+            if (live[k]) *reinterpret_cast<float4*>(e + (own[k] ^ 256u)) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    } else {
+        const uint32_t co = ((uint32_t)(colour ^ 1) << 8) | (uint32_t)(128 * (w ^ 1));
+        auto row = [&](uint32_t n, int a2, int b2) { return (n << 9) | co | (uint32_t)(16 * a2 + 4 * (b2 >> 1)); };
+        const int sx = a == 7 ? 0 : a == 0 ? 1 : 6, sy = b == 7 ? 2 : b == 0 ? 3 : 6, sz = 5 - p;
+        uint32_t nx[kF32LeavesPerThread], ny[kF32LeavesPerThread], nz[kF32LeavesPerThread];
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k) {
+            const int* nb = nb8 + 8 * (own[k] >> 9);
+            nx[k] = (uint32_t)__ldg(nb + sx);
+            ny[k] = (uint32_t)__ldg(nb + sy);
+            nz[k] = (uint32_t)__ldg(nb + sz);
+        }
+        if constexpr (kPdl) asm volatile("griddepcontrol.wait;" ::: "memory");
+        float4 C[kF32LeavesPerThread], K[kF32LeavesPerThread], XP[kF32LeavesPerThread], XM[kF32LeavesPerThread],
+            YP[kF32LeavesPerThread], YM[kF32LeavesPerThread];
+        float ZC[kF32LeavesPerThread];
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k) {
+            C[k] = ldf4_rw(e + own[k]);
+            K[k] = lde(e + (own[k] ^ 256u));
+        }
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k) {
+            const uint32_t lf = own[k] >> 9;
+            XP[k] = lde(e + row(a == 7 ? nx[k] : lf, (a + 1) & 7, b));
+            XM[k] = lde(e + row(a == 0 ? nx[k] : lf, (a - 1) & 7, b));
+            YP[k] = lde(e + row(b == 7 ? ny[k] : lf, a, (b + 1) & 7));
+            YM[k] = lde(e + row(b == 0 ? ny[k] : lf, a, (b - 1) & 7));
+            const float* zq = e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1);
+            ZC[k] = kShared ? *zq : __ldg(zq);
+        }
+#pragma unroll
+        for (int k = 0; k < kF32LeavesPerThread; ++k)
+            out[k] = p ? relax_row_f32<1>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2)
+                       : relax_row_f32<0>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2);
+    }
+#pragma unroll
+    for (int k = 0; k < kF32LeavesPerThread; ++k)
+        if (live[k]) *reinterpret_cast<float4*>(e + own[k]) = out[k];
+}
+
+// rbgs_split_half_kernel on FP32 (see there).
 template <bool kZero>
 __global__ void __launch_bounds__(kF32Threads, kF32ShortGridCtasPerSm)
     rbgs_split_half_f32_kernel(const int* __restrict__ nb8, const float* __restrict__ rhs, float* e, int num_leaves,
@@ -237,72 +326,114 @@ __global__ void __launch_bounds__(kF32Threads, kF32ShortGridCtasPerSm)
     if (check != nullptr && check[0] <= tol2 * check[1]) return;
     if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, 1ull);
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
-    const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
-    const int p = (w + colour) & 1;
-    const uint32_t rowc = ((uint32_t)colour << 8) | (uint32_t)(4 * (32 * w + lane));
-    constexpr int kPer = kF32LeavesPerBlock * kF32LeavesPerThread;
-    const int groups = (num_leaves + kPer - 1) / kPer;
-    for (int g = blockIdx.x; g < groups; g += gridDim.x) {
-        const int leaf0 = g * kPer + (int)(threadIdx.x >> 6);
-        uint32_t own[kF32LeavesPerThread];
-        bool live[kF32LeavesPerThread];
-#pragma unroll
-        for (int k = 0; k < kF32LeavesPerThread; ++k) {
-            const int leaf = leaf0 + k * kF32LeavesPerBlock;
-            live[k] = leaf < num_leaves;
-            own[k] = ((uint32_t)(live[k] ? leaf : 0) << 9) | rowc;
-        }
-        float4 B[kF32LeavesPerThread], out[kF32LeavesPerThread];
-#pragma unroll
-        for (int k = 0; k < kF32LeavesPerThread; ++k) B[k] = ldf4(rhs + own[k]);
-        if constexpr (kZero) {
-#pragma unroll
-            for (int k = 0; k < kF32LeavesPerThread; ++k) {
-                float v[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) v[j] = relax_f32(0.f, 0.f, 0.f, 0.f, 0.f, 0.f, at4(B[k], j), 0.f, omega, dx2);
-                out[k] = make_float4(v[0], v[1], v[2], v[3]);
-                if (live[k]) *reinterpret_cast<float4*>(e + (own[k] ^ 256u)) = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int groups = (num_leaves + kF32LeavesPerGroup - 1) / kF32LeavesPerGroup;
+    for (int g = blockIdx.x; g < groups; g += gridDim.x)
+        relax_group_f32<kZero, false, true>(nb8, rhs, e, num_leaves, g, colour, omega, dx2);
+}
+
+// ---- The persistent solve -------------------------------------------------------------------
+// A whole solve, `half_sweeps` half-sweeps (red, black, red, ...), in one cooperative launch
+// instead of one launch per colour: no launch gap and no draining of a grid between the
+// colours. Work item i = h * groups + g is half-sweep h of leaf group g; CTA c takes the items
+// c, c + G, c + 2G, ... in order (G CTAs, all resident). Before item (h, g) the CTA waits until
+// progress[x] >= h for g itself and for every group x that holds a face neighbour of g's leaves:
+// those groups have finished half-sweep h - 1, so the other colour the item reads is current and
+// no neighbour still has to read the colour the item overwrites. After the item it publishes
+// progress[g] = h + 1 (its stores fenced first). The values are those of the launch-per-colour
+// kernel to the bit: each voxel sees the same operands in the same order.
+//
+// Every wait ends: an item waits only on smaller items, and the CTA of the smallest unfinished
+// item has finished its own earlier items, so that item's dependencies are all done. Waits are
+// bounded all the same (kSolveMaxPolls polls with a short sleep, about a second): one that gives
+// up raises the device error flag (counters[1]) and the abort word progress[groups], which every
+// other wait watches, and every CTA returns, leaving e unfinished. `unreachable` (0 but in the
+// test of that path) raises every wait's target out of reach.
+constexpr uint32_t kSolveMaxPolls = 1u << 20;
+static_assert(kThreads == kF32Threads, "one block shape for both precisions");
+static_assert(64 + 6 * kLeavesPerGroup + 1 <= kThreads, "dependency threads");
+
+__device__ __forceinline__ uint32_t ld_acquire_u32(const unsigned* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(unsigned* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// T = __half: the FP16 inner solve (relax_group, unit spacing); T = float: the FP32 solve
+// (relax_group_f32, dx2). Groups of kLeavesPerGroup or kF32LeavesPerGroup leaves.
+template <typename T, bool kZeroFirst>
+__global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? kShortGridCtasPerSm : kF32ShortGridCtasPerSm)
+    rbgs_split_solve_kernel(
+    const int* __restrict__ nb8, const T* __restrict__ rhs, T* e, int num_leaves, int half_sweeps, float omega, float dx2,
+    const double* __restrict__ check, double tol2, unsigned long long* __restrict__ counters, unsigned* progress,
+    uint32_t max_polls, uint32_t unreachable) {
+    constexpr bool kHalf = sizeof(T) == 2;
+    constexpr int kPerGroup = kHalf ? kLeavesPerGroup : kF32LeavesPerGroup;
+    constexpr int kDepThreads = 6 * kPerGroup;  // one face of one leaf each, threads 64 ...
+    if (check != nullptr && check[0] <= tol2 * check[1]) return;  // the refinement has converged
+    if (counters != nullptr && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(counters, (unsigned long long)half_sweeps);
+    const int tid = threadIdx.x;
+    const int groups = (num_leaves + kPerGroup - 1) / kPerGroup;
+    unsigned* abort_word = progress + groups;
+    const int64_t items = (int64_t)half_sweeps * groups;
+    // The dependency this thread watches: face df of leaf dl of the item's group (threads 64 ...),
+    // or the group itself (the thread after them).
+    const int dt = tid - 64, dl = dt / 6, df = dt - 6 * dl;
+    const bool watches_face = dt >= 0 && dt < kDepThreads, watches_self = dt == kDepThreads;
+    int h = (int)(blockIdx.x / (unsigned)groups), g = (int)(blockIdx.x % (unsigned)groups);
+    const int step_h = (int)(gridDim.x / (unsigned)groups), step_g = (int)(gridDim.x % (unsigned)groups);
+    for (int64_t i = blockIdx.x; i < items; i += gridDim.x) {
+        if (h > 0) {
+            int x = -1;
+            if (watches_face) {
+                const int leaf = g * kPerGroup + dl;
+                if (leaf < num_leaves) {
+                    const int n = __ldg(nb8 + 8 * leaf + df);
+                    if (n < num_leaves) x = n / kPerGroup;  // the zero leaf is never written
+                }
+            } else if (watches_self) {
+                x = g;
             }
+            bool failed = false;
+            if (x >= 0) {
+                uint32_t polls = 0;
+                while (ld_acquire_u32(progress + x) < (uint32_t)h + unreachable) {
+                    if (++polls >= max_polls) {
+                        atomicExch(abort_word, 1u);
+                        if (counters != nullptr) atomicExch(counters + 1, 1ull);
+                        failed = true;
+                        break;
+                    }
+                    if ((polls & 31u) == 0 && *reinterpret_cast<volatile unsigned*>(abort_word) != 0u) {
+                        failed = true;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            if (__syncthreads_or(failed)) return;
+        }
+        if constexpr (kHalf) {
+            if (kZeroFirst && h == 0)
+                relax_group<true, true, false>(nb8, rhs, e, num_leaves, g, 0, omega);
+            else
+                relax_group<false, true, false>(nb8, rhs, e, num_leaves, g, h & 1, omega);
         } else {
-            const uint32_t co = ((uint32_t)(colour ^ 1) << 8) | (uint32_t)(128 * (w ^ 1));
-            auto row = [&](uint32_t n, int a2, int b2) { return (n << 9) | co | (uint32_t)(16 * a2 + 4 * (b2 >> 1)); };
-            const int sx = a == 7 ? 0 : a == 0 ? 1 : 6, sy = b == 7 ? 2 : b == 0 ? 3 : 6, sz = 5 - p;
-            uint32_t nx[kF32LeavesPerThread], ny[kF32LeavesPerThread], nz[kF32LeavesPerThread];
-#pragma unroll
-            for (int k = 0; k < kF32LeavesPerThread; ++k) {
-                const int* nb = nb8 + 8 * (own[k] >> 9);
-                nx[k] = (uint32_t)__ldg(nb + sx);
-                ny[k] = (uint32_t)__ldg(nb + sy);
-                nz[k] = (uint32_t)__ldg(nb + sz);
-            }
-            asm volatile("griddepcontrol.wait;" ::: "memory");
-            float4 C[kF32LeavesPerThread], K[kF32LeavesPerThread], XP[kF32LeavesPerThread], XM[kF32LeavesPerThread],
-                YP[kF32LeavesPerThread], YM[kF32LeavesPerThread];
-            float ZC[kF32LeavesPerThread];
-#pragma unroll
-            for (int k = 0; k < kF32LeavesPerThread; ++k) {
-                C[k] = ldf4_rw(e + own[k]);
-                K[k] = ldf4(e + (own[k] ^ 256u));
-            }
-#pragma unroll
-            for (int k = 0; k < kF32LeavesPerThread; ++k) {
-                const uint32_t lf = own[k] >> 9;
-                XP[k] = ldf4(e + row(a == 7 ? nx[k] : lf, (a + 1) & 7, b));
-                XM[k] = ldf4(e + row(a == 0 ? nx[k] : lf, (a - 1) & 7, b));
-                YP[k] = ldf4(e + row(b == 7 ? ny[k] : lf, a, (b + 1) & 7));
-                YM[k] = ldf4(e + row(b == 0 ? ny[k] : lf, a, (b - 1) & 7));
-                ZC[k] = __ldg(e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1));
-            }
-#pragma unroll
-            for (int k = 0; k < kF32LeavesPerThread; ++k)
-                out[k] = p ? relax_row_f32<1>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2)
-                           : relax_row_f32<0>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2);
+            if (kZeroFirst && h == 0)
+                relax_group_f32<true, true, false>(nb8, rhs, e, num_leaves, g, 0, omega, dx2);
+            else
+                relax_group_f32<false, true, false>(nb8, rhs, e, num_leaves, g, h & 1, omega, dx2);
         }
-#pragma unroll
-        for (int k = 0; k < kF32LeavesPerThread; ++k)
-            if (live[k]) *reinterpret_cast<float4*>(e + own[k]) = out[k];
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_relaxed_u32(progress + g, (uint32_t)(h + 1));
+        }
+        h += step_h;
+        g += step_g;
+        if (g >= groups) g -= groups, ++h;
     }
 }
 
@@ -472,6 +603,58 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<false>, nb8, r, x, (int)L, colour, omega, check, tol2,
                                 c.counters));
     HNS_LAUNCHED();
+}
+
+namespace {
+
+template <typename T>
+void launch_split_solve(Context& c, const int* nb8, const T* rhs, T* e, int half_sweeps, bool e_zero, float omega,
+                        float dx2, const double* check, double tol2) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0 || half_sweeps <= 0) return;
+    if (L >= (int64_t(1) << 22)) fail(HNS_ERR_INVALID_ARG, "too many leaves for the colour-split solve");
+    const int per_group = sizeof(T) == 2 ? kLeavesPerGroup : kF32LeavesPerGroup;
+    const int groups = (int)((L + per_group - 1) / per_group);
+    // Progress counters of the leaf groups and the abort word, zero before each launch.
+    auto* progress = reinterpret_cast<unsigned*>(
+        c.scratch_f32(sizeof(T) == 2 ? "split_progress16" : "split_progress32", (size_t)groups + 1));
+    HNS_CUDA(cudaMemsetAsync(progress, 0, sizeof(unsigned) * ((size_t)groups + 1), c.stream));
+    auto kern = e_zero ? rbgs_split_solve_kernel<T, true> : rbgs_split_solve_kernel<T, false>;
+    int per_sm = 0;
+    HNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0));
+    if (per_sm < 1) fail(HNS_ERR_CUDA, "the persistent solve does not fit on an SM");
+    const int64_t items = (int64_t)half_sweeps * groups;
+    const unsigned blocks = (unsigned)std::min<int64_t>(items, (int64_t)per_sm * c.sm_count());
+    // The test hook: every wait gives up after first_wait_polls polls, its target out of reach.
+    const bool stall = c.first_wait_polls >= 0;
+    const uint32_t max_polls = stall ? (uint32_t)c.first_wait_polls : kSolveMaxPolls;
+    const uint32_t unreachable = stall ? (1u << 30) : 0u;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = c.stream;
+    // Cooperative: every CTA resident at once, which the progress waits rely on.
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HNS_CUDA(cudaLaunchKernelEx(&cfg, kern, nb8, rhs, e, (int)L, half_sweeps, omega, dx2, check, tol2, c.counters,
+                                progress, max_polls, unreachable));
+    HNS_LAUNCHED();
+}
+
+}  // namespace
+
+void launch_rbgs_split_solve(Context& c, const int* nb8, const void* rhs, void* e, int half_sweeps, bool e_zero,
+                             float omega, const double* check, double tol2) {
+    launch_split_solve(c, nb8, static_cast<const __half*>(rhs), static_cast<__half*>(e), half_sweeps, e_zero, omega, 1.0f,
+                       check, tol2);
+}
+
+void launch_rbgs_split_solve_f32(Context& c, const int* nb8, const float* rhs, float* e, int half_sweeps, bool e_zero,
+                                 float omega, float dx2, const double* check, double tol2) {
+    launch_split_solve(c, nb8, rhs, e, half_sweeps, e_zero, omega, dx2, check, tol2);
 }
 
 }  // namespace hns

@@ -41,6 +41,30 @@ void split32_solve(Context& c, const float* div, float* p, int K, float omega, u
     const bool zero = (flags & HNS_SOLVE_ZERO_INIT) != 0;
     if (!zero) convert_split_f32(c, p, w.e, true);
     const double tol2 = plan ? plan->tol * plan->tol : 0.0;
+    if (c.split_solve == HNS_SPLIT_PERSISTENT) {
+        // Persistent launches over the runs of iterations that share a check slot and have no
+        // residual evaluation inside: [cE, (c+1)E - 1) and the single iteration (c+1)E - 1.
+        for (int it = 0; it < K;) {
+            const double* chk = nullptr;
+            int end = K;
+            if (plan) {
+                const int E = plan->check_every;
+                const int last_check = it / E - 1;
+                chk = last_check >= 0 ? plan->slots + 2 * last_check : nullptr;
+                if ((it + 1) % E == 0) {
+                    launch_split_residual_f32(c, w.nb8, w.rhs, w.e, (double)dx2, chk, tol2,
+                                              plan->slots + 2 * ((it + 1) / E - 1));
+                    end = it + 1;
+                } else {
+                    end = std::min(K, (it / E + 1) * E - 1);
+                }
+            }
+            launch_rbgs_split_solve_f32(c, w.nb8, w.rhs, w.e, 2 * (end - it), zero && it == 0, omega, dx2, chk, tol2);
+            it = end;
+        }
+        convert_split_f32(c, w.e, p, false);
+        return;
+    }
     bool after_half = false;  // the preceding kernel on the stream is a half-sweep
     for (int it = 0; it < K; ++it) {
         const double* chk = nullptr;

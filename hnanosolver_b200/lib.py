@@ -24,6 +24,8 @@ RBGS_PLAIN, RBGS_BULK, RBGS_SPLIT = 0, 1, 2
 OPT_INNER_LAYOUT = 2
 INNER_ROWS, INNER_PACKED, INNER_SPLIT = 0, 1, 2
 OPT_WAIT_POLLS = 3
+OPT_SPLIT_SOLVE = 4
+SPLIT_PER_COLOUR, SPLIT_PERSISTENT = 0, 1
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 
@@ -112,7 +114,7 @@ PHASES = {"advect": 0, "divergence": 1, "solve": 2, "gradient": 3, "forces": 4, 
 
 class ProfileData(ctypes.Structure):
     _fields_ = [("phase_ms", ctypes.c_double * NUM_PHASES), ("phase_count", _i * NUM_PHASES),
-                ("solver_launches", ctypes.c_ulonglong)]
+                ("solver_launches", ctypes.c_ulonglong), ("kernel_launches", ctypes.c_ulonglong)]
 
 
 def _sig(lib, name, res, *args):

@@ -472,7 +472,9 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
 #define HNS_RBGS_BULK 1       /*   bulk async copies of the contiguous leaf payload into a staged tile, both
                                    colours per launch (used when div and p are 16-byte aligned) */
 #define HNS_RBGS_SPLIT 2      /*   the solve on colour-split leaves, one in-place launch per colour, no
-                                   staging (default). The three give the same results to the bit. */
+                                   staging (default; a call that runs single iterations, such as
+                                   hns_project_static, takes HNS_RBGS_BULK). The three give the same
+                                   results to the bit. */
 #define HNS_OPT_INNER_LAYOUT 2 /* layout of the FP16 inner solve of the mixed-precision refinement: */
 #define HNS_INNER_ROWS 0       /*   the leaf-dense slot order, relaxed by the HNS_RBGS_BULK kernel */
 #define HNS_INNER_PACKED 1     /*   colour-packed rows (z = 0,2,4,6 then 1,3,5,7) with face buffers,
@@ -481,11 +483,21 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
                                     one in-place launch per colour (default). All three give the
                                     same results to the bit; the solver's own arrays, never the
                                     caller's */
-#define HNS_OPT_WAIT_POLLS 3    /* test hook of the timeout path: the poll limit of the first bounded
-                                    copy wait of the HNS_RBGS_BULK kernel (value >= 0; -1 restores the
-                                    default). 0 makes every CTA give up at its first leaf, wait for its
-                                    copies in flight with the normal limit, raise the device error flag
-                                    (hns_device_status) and return, leaving p_out unfinished. */
+#define HNS_OPT_WAIT_POLLS 3    /* test hook of the timeout paths (value >= 0; -1 restores the
+                                    defaults). The HNS_RBGS_BULK kernel: the poll limit of its first
+                                    bounded copy wait; 0 makes every CTA give up at its first leaf, wait
+                                    for its copies in flight with the normal limit, raise the device
+                                    error flag (hns_device_status) and return, leaving p_out
+                                    unfinished. The persistent colour-split solves (HNS_SPLIT_PERSISTENT):
+                                    every dependency wait behaves as if the neighbour never finished and
+                                    gives up after `value` polls, raising the flag; every CTA then
+                                    returns, leaving the solve unfinished. */
+#define HNS_OPT_SPLIT_SOLVE 4   /* how the colour-split solves (HNS_RBGS_SPLIT, HNS_INNER_SPLIT) launch: */
+#define HNS_SPLIT_PER_COLOUR 0  /*   one launch per half-sweep (programmatic dependent launches) */
+#define HNS_SPLIT_PERSISTENT 1  /*   one cooperative launch per inner solve, or per run of iterations
+                                     between convergence checks, leaf groups ordered by per-group
+                                     progress counters instead of launch boundaries (default). Both
+                                     give the same results to the bit. */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */
@@ -505,7 +517,10 @@ HNS_API hns_status hns_device_status(hns_ctx* ctx);
 typedef struct hns_profile_data {
     double phase_ms[HNS_NUM_PHASES];        /* device time per phase since the last read */
     int phase_count[HNS_NUM_PHASES];        /* phase executions since the last read */
-    unsigned long long solver_launches;     /* red-black launches that ran (not skipped) */
+    unsigned long long solver_launches;     /* red-black sweeps that ran (not skipped): launches, and
+                                               the half-sweeps inside a persistent inner solve */
+    unsigned long long kernel_launches;     /* the library's kernel launches since the last read, of
+                                               every context of the process (memsets not counted) */
 } hns_profile_data;
 
 HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable);

@@ -53,6 +53,7 @@ def _to_dev(dev, fields):
     for k, a in fields.items():
         t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
         out[k] = (t.to(torch.bfloat16) if k == "velocity" else t.to(torch.float16)).reshape(-1).contiguous()
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     return out
 
 

@@ -38,9 +38,11 @@ def test_conversions_round_to_nearest(dev, shell):
     g = hl.Grid(origins, voxel_size=0.1)
     v = torch.from_numpy(vel).to(dev).reshape(-1)
     b = torch.empty(v.numel(), dtype=torch.bfloat16, device=dev)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     g.convert(v, hl.DTYPE_F32, b, hl.DTYPE_BF16, v.numel())
     d = torch.from_numpy(dens).to(dev)
     h = torch.empty(d.numel(), dtype=torch.float16, device=dev)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     g.convert(d, hl.DTYPE_F32, h, hl.DTYPE_F16, d.numel())
     back = torch.empty_like(v)
     g.convert(b, hl.DTYPE_BF16, back, hl.DTYPE_F32, v.numel())
@@ -58,6 +60,7 @@ def _mixed(g, dev, dens, vel, tol=1e-5, inner=40, outer=8):
     dh = torch.from_numpy(dens).to(dev).to(torch.float16).contiguous()
     vo, do = torch.empty_like(vb), torch.empty_like(dh)
     desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=tol, max_outer=outer, inner_iterations=inner, flags=0)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     info = g.step_mixed(vb, vo, [dh], [do], desc, info=True)
     return vb, dh, vo, do, info
 
@@ -135,6 +138,7 @@ def test_mixed_step_scalar_counts(dev, oracle, shell, nscalars):
     outs = [torch.empty_like(h) for h in hs]
     vo = torch.empty_like(vb)
     desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=8, inner_iterations=40, flags=0)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     info = g.step_mixed(vb, vo, hs, outs, desc, info=True)
     assert info.residual <= 1e-5
     vb1, dh1, vo1, do1, _ = _mixed(g, dev, dens, vel)
@@ -182,6 +186,7 @@ def test_unaligned_arrays_match_aligned(dev, shell):
     sd = hl.StepDesc(dt=0.1, max_iterations=0, omega=1.9, tolerance=1e-5, check_every=10,
                      flags=hl.SOLVE_REFINE, max_outer=10, inner_iterations=40)
     va, da = torch.empty_like(v32), torch.empty_like(d32)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     g.step_plain(v32, va, [d32], [da], sd)
     torch.cuda.synchronize()
     vi, di = shifted(v32), shifted(d32)
@@ -221,6 +226,7 @@ def test_fp32_refined_reaches_tolerance_plain_fp32_cannot(dev, shell):
     v_out, d_out = torch.empty_like(v_in), torch.empty_like(d_in)
     desc = hl.StepDesc(dt=0.1, max_iterations=0, omega=1.9, tolerance=1e-6, check_every=10,
                        flags=hl.SOLVE_REFINE, max_outer=10, inner_iterations=40)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     info = g.step_plain(v_in, v_out, [d_in], [d_out], desc, info=True)
     assert info.residual <= 1e-6
     plain = hl.StepDesc(dt=0.1, max_iterations=3000, omega=1.9, tolerance=1e-6, check_every=10, flags=0)
@@ -232,10 +238,10 @@ def test_fp32_refined_reaches_tolerance_plain_fp32_cannot(dev, shell):
 
 @pytest.mark.parametrize("grid", ["shell", "spheres"])
 def test_inner_solve_layouts_bit_exact(dev, shell, grid):
-    """The FP16 inner solve on colour-split leaves (the default), on colour-packed rows and on
-    the plain slot order relax every voxel with the same arithmetic, so the whole mixed step --
-    refined pressure, outer iteration count, projected velocity, advected density -- is
-    identical to the bit.
+    """The FP16 inner solve on colour-split leaves (the default, as one persistent launch per
+    inner solve or one launch per colour), on colour-packed rows and on the plain slot order
+    relax every voxel with the same arithmetic, so the whole mixed step -- refined pressure,
+    outer iteration count, projected velocity, advected density -- is identical to the bit.
     The sparse spheres exercise missing neighbour leaves (face rings and z rings left at 0)."""
     from hnanosolver_b200 import lib as hl
 
@@ -245,9 +251,13 @@ def test_inner_solve_layouts_bit_exact(dev, shell, grid):
         origins = synth.spheres_topology(96, 3, 8.0, 20.0, seed=11)
         dens, vel = synth.noise_fields(origins, seed=7)
     out = {}
-    for layout in (hl.INNER_ROWS, hl.INNER_PACKED, hl.INNER_SPLIT):
+    forms = [(hl.INNER_ROWS, None), (hl.INNER_PACKED, None), (hl.INNER_SPLIT, hl.SPLIT_PER_COLOUR),
+             (hl.INNER_SPLIT, hl.SPLIT_PERSISTENT)]
+    for layout in forms:
         g = hl.Grid(origins, voxel_size=0.1)
-        g.set_option(hl.OPT_INNER_LAYOUT, layout)
+        g.set_option(hl.OPT_INNER_LAYOUT, layout[0])
+        if layout[1] is not None:
+            g.set_option(hl.OPT_SPLIT_SOLVE, layout[1])
         vb, dh, vo, do, info = _mixed(g, dev, dens, vel, inner=30, outer=12)
         p = torch.empty(g.num_voxels, dtype=torch.float64, device=dev)
         outer, res = g.refine_pressure(p)
@@ -255,8 +265,8 @@ def test_inner_solve_layouts_bit_exact(dev, shell, grid):
         torch.cuda.synchronize()
         out[layout] = (vo.cpu(), do.cpu(), p.cpu(), outer, res, info.iterations)
         g.close()
-    a = out[hl.INNER_ROWS]
-    for layout in (hl.INNER_PACKED, hl.INNER_SPLIT):
+    a = out[forms[0]]
+    for layout in forms[1:]:
         b = out[layout]
         assert a[3] == b[3] and a[5] == b[5]
         assert a[4] == pytest.approx(b[4], rel=1e-12)  # FP64 atomics: summation order varies
@@ -320,6 +330,7 @@ def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
     for flags in (0, hl.SOLVE_MULTIGRID):
         vo, do = torch.empty_like(vb), torch.empty_like(dh)
         desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=40, inner_iterations=30, flags=flags)
+        torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
         info = g.step_mixed(vb, vo, [dh], [do], desc, info=True)
         assert info.residual <= 1e-5
         p = torch.empty(g.num_voxels, dtype=torch.float64, device=dev)
@@ -336,6 +347,7 @@ def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
     d = torch.from_numpy(dens).to(dev)
     sd = hl.StepDesc(dt=0.1, max_iterations=0, omega=1.9, tolerance=1e-5, check_every=0,
                      flags=hl.SOLVE_REFINE | hl.SOLVE_MULTIGRID, max_outer=40, inner_iterations=30)
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     info = g.step_plain(v, torch.empty_like(v), [d], [torch.empty_like(d)], sd, info=True)
     assert info.residual <= 1e-5
     g.close()

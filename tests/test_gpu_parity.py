@@ -21,7 +21,10 @@ def dev():
 
 
 def T(a, dev):
-    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    """Uploads on torch's stream and waits: the library's own stream does not wait for torch's."""
+    t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    torch.cuda.synchronize()
+    return t
 
 
 def H(t):
@@ -151,16 +154,17 @@ def test_project(case, dev):
     assert info.initial_residual == pytest.approx(1.0, rel=1e-9)
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel,form", [(0, None), (1, None), (2, 0), (2, 1)])
 @pytest.mark.parametrize("iters,zero", [(1, True), (6, False), (11, True)])
-def test_rbgs_kernels_bit_exact(case, dev, kernel, iters, zero):
-    """The three FP32 red-black kernels (plain-load halo tile, bulk async copies into a staged
-    tile, colour-split leaves) equal the oracle."""
+def test_rbgs_kernels_bit_exact(case, dev, kernel, form, iters, zero):
+    """The FP32 red-black kernels (plain-load halo tile, bulk async copies into a staged tile,
+    colour-split leaves launched per colour or as one persistent launch) equal the oracle."""
     from conftest import bit_exact
     from hnanosolver_b200 import lib as hl
 
     g, t = case["grid"], case["topo"]
     g.set_option(hl.OPT_RBGS_KERNEL, kernel)
+    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT if form is None else form)
     div = t.divergence(case["vel"], 10.0)
     p0 = np.zeros_like(div) if zero else (case["dens"] * 0.01).astype(np.float32)
     p = T(p0, dev)
@@ -168,6 +172,7 @@ def test_rbgs_kernels_bit_exact(case, dev, kernel, iters, zero):
     g.device_status()
     assert bit_exact(H(p), t.rbgs(div, p0, 0.1, iters, 1.8))
     g.set_option(hl.OPT_RBGS_KERNEL, hl.RBGS_SPLIT)
+    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT)
 
 
 def test_rbgs_unaligned_pointers_fall_back(case, dev):

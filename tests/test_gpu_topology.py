@@ -121,6 +121,7 @@ def test_tables_equal_host_build(dev):
     outs = []
     for g in (gd, gh):
         div, p = torch.empty(n, device=dev), torch.empty(n, device=dev)
+        torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
         g.divergence(v, div)
         g.rbgs(div, p, 20, 1.5, flags=hl.SOLVE_ZERO_INIT)
         torch.cuda.synchronize()

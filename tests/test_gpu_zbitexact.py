@@ -32,6 +32,7 @@ def test_operators_bit_exact(dev, oracle, golden_kernels):
     v, d = T(vel), T(dens)
     out3, out1 = torch.empty_like(v), torch.empty_like(d)
     checks = {}
+    torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     grid.advect_vec3(v, out3, 0.1)
     grid.synchronize()
     checks["advect_vec3"] = bit_exact(out3.cpu().numpy(), t.advect_vector(vel, 0.1, 10.0))
