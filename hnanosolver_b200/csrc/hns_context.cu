@@ -198,6 +198,9 @@ double* Context::reduce_slots(int count) {
     return d_reduce.as<double>();
 }
 
+std::atomic<unsigned long long> g_kernel_launches{0};
+void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+
 int Context::sm_count() const {
     if (sms == 0) HNS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     return sms;
@@ -465,13 +468,6 @@ HNS_API hns_status hns_profile_enable(hns_ctx* ctx, int enable) {
     });
 }
 
-namespace hns {
-namespace {
-std::atomic<unsigned long long> g_kernel_launches{0};
-}
-void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
-}  // namespace hns
-
 HNS_API hns_status hns_profile_read(hns_ctx* ctx, hns_profile_data* out) {
     return guarded([&] {
         Context* c = check_ctx(ctx);
@@ -493,7 +489,7 @@ HNS_API hns_status hns_profile_read(hns_ctx* ctx, hns_profile_data* out) {
         HNS_CUDA(cudaMemcpy(&out->solver_launches, c->counters, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
         HNS_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(unsigned long long), c->stream));
         HNS_CUDA(cudaStreamSynchronize(c->stream));
-        out->kernel_launches = g_kernel_launches.exchange(0, std::memory_order_relaxed);
+        out->kernel_launches = ::hns::g_kernel_launches.exchange(0, std::memory_order_relaxed);
     });
 }
 

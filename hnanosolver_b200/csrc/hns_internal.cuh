@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <stdexcept>
@@ -27,6 +28,7 @@ void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 #define HNS_LAUNCHED() (::hns::note_launch(), ::hns::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 // Counts the library's kernel launches (process-wide; hns_profile_read reports and resets it).
 void note_launch();
+extern std::atomic<unsigned long long> g_kernel_launches;
 
 hns_status record_error(hns_status s, const std::string& msg);
 void clear_error();
