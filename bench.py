@@ -95,6 +95,12 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
+def apply_options(g, hl, args):
+    """The library options the command line selects."""
+    form = getattr(args, "split_solve", "persistent")
+    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT if form == "persistent" else hl.SPLIT_PER_COLOUR)
+
+
 def profiled_traffic(workload: str, kind: str):
     """DRAM bytes per launch of the red-black kernel (kind f32 or split) from the committed ncu
     summary profiles/rbgs_<kind>_<workload>.md (line `dram_bytes_per_launch: <int>`), or None."""
@@ -418,6 +424,7 @@ def ours(args, wl):
     dens, vel = synth.noise_fields(origins, seed=replicas.seed_of(R))
     n = len(dens)
     g = hl.Grid(origins, voxel_size=wl["dx"], device=local)
+    apply_options(g, hl, args)
     stream = torch.cuda.Stream(device=dev)
     g.set_stream(stream.cuda_stream)
     mixed = args.precision == "mixed"
@@ -566,7 +573,7 @@ def ours(args, wl):
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
         cfg = workload_config(args, wl, origins)
-        det = {"precision": args.precision, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+        det = {"precision": args.precision, "split_solve": args.split_solve, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
                "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
@@ -767,6 +774,7 @@ def ours_fire(args, wl):
     origins, fields, sources = synth.fire_state(args.workload, seed=replicas.seed_of(R))
     n = 512 * len(origins)
     g = hl.Grid(origins, voxel_size=wl["dx"], device=local)
+    apply_options(g, hl, args)
     stream = torch.cuda.Stream(device=dev)
     g.set_stream(stream.cuda_stream)
     params, model = fire_params(hl)
@@ -942,7 +950,7 @@ def ours_fire(args, wl):
 
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
-        det = {"precision": args.precision, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+        det = {"precision": args.precision, "split_solve": args.split_solve, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
                "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 and "value" in fp32["plain"] else None,
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
@@ -1041,6 +1049,7 @@ def box64_ours(args):
     dens, vel = synth.smoothed_fields(origins, seed=replicas.seed_of(R), box_passes=3)
     n = len(dens)
     g = hl.Grid(origins, voxel_size=BOX64["dx"], device=local)
+    apply_options(g, hl, args)
     stream = torch.cuda.Stream(device=dev)
     g.set_stream(stream.cuda_stream)
     v = [torch.from_numpy(vel).to(dev), torch.empty((n, 3), device=dev)]
@@ -1125,6 +1134,8 @@ def main():
                     help="mixed (default for the SOP chain and fire1024) or fp32 (default for plume256 --forces)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout measured beside the step")
+    ap.add_argument("--split-solve", choices=["persistent", "per-colour"], default="persistent",
+                    help="launch form of the colour-split red-black solves (same results to the bit)")
     ap.add_argument("--no-fp32-comparison", action="store_true",
                     help="skip the FP32 forms measured beside the mixed one (profiling runs)")
     args = ap.parse_args()

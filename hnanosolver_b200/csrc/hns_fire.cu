@@ -263,7 +263,8 @@ __device__ __forceinline__ float rec_s(const uint4& r, int q) {
 // outside the domain, and the MacCormack correction is clamped to the centre, its six face
 // neighbours and the forward sample; the FP32 step's operations in its order, one 16-byte load
 // per tap for the velocity and every field.
-template <int kCount>
+// I: the slot type, int32_t where the grid has fewer than 2^22 leaves (32-bit addressing).
+template <int kCount, typename I>
 __global__ void __launch_bounds__(kThreads) advect_scalars_records_kernel(TopoView t, const uint4* __restrict__ rec,
                                                                            HalfFields f, float sdt) {
     __shared__ LeafNbhd L;
@@ -271,12 +272,12 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_records_kernel(TopoVi
     load_nbhd(L, t, v.leaf);
     __syncthreads();
     const int i = (L.lx << 3) + (v.n >> 6), j = (L.ly << 3) + ((v.n >> 3) & 7), k = (L.lz << 3) + (v.n & 7);
-    const int64_t s = (v.leaf << 9) + v.n;
+    const I s = (I(v.leaf) << 9) + I(v.n);
     const uint4 o = __ldg(rec + s);
     const float bx = (float)i - bf_lo(o.x) * sdt, by = (float)j - bf_hi(o.x) * sdt, bz = (float)k - bf_lo(o.y) * sdt;
-    int64_t bi[8], fi[8], ni[6];
+    I bi[8], fi[8], ni[6];
     float bw[8], fw[8];
-    interp_setup(t, L, bx, by, bz, bi, bw);
+    interp_setup_fast<I>(t, L, bx, by, bz, bi, bw);
     float3 vf = make_float3(0.f, 0.f, 0.f);
     float pf[kCount], pb[kCount];
 #pragma unroll
@@ -290,19 +291,16 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_records_kernel(TopoVi
 #pragma unroll
         for (int c = 0; c < kCount; ++c) pf[c] = __fmaf_rn(rec_s(a, c), bw[q], pf[c]);
     }
-    interp_setup(t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt, fi, fw);
+    interp_setup_fast<I>(t, L, bx + vf.x * sdt, by + vf.y * sdt, bz + vf.z * sdt, fi, fw);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const uint4 a = __ldg(rec + fi[q]);
 #pragma unroll
         for (int c = 0; c < kCount; ++c) pb[c] = __fmaf_rn(rec_s(a, c), fw[q], pb[c]);
     }
-    ni[0] = tap_slot(t, L, i - 1, j, k);
-    ni[1] = tap_slot(t, L, i + 1, j, k);
-    ni[2] = tap_slot(t, L, i, j - 1, k);
-    ni[3] = tap_slot(t, L, i, j + 1, k);
-    ni[4] = tap_slot(t, L, i, j, k - 1);
-    ni[5] = tap_slot(t, L, i, j, k + 1);
+    face_slots(L, s, v.n, ni);  // x-1, x+1, y-1, y+1, z-1, z+1
+#pragma unroll
+    for (int q = 0; q < 6; ++q) ni[q] = ni[q] < 0 ? I(0) : ni[q];  // outside the domain: slot 0
     float mn[kCount], mx[kCount], po[kCount];
 #pragma unroll
     for (int c = 0; c < kCount; ++c) po[c] = rec_s(o, c), mn[c] = po[c], mx[c] = po[c];
@@ -319,8 +317,21 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_records_kernel(TopoVi
 #pragma unroll
     for (int c = 0; c < kCount; ++c) {
         const float corr = __fmaf_rn(0.5f, po[c] - pb[c], pf[c]);
-        sstore(f.out[c], s, fmaxf(fminf(mn[c], pf[c]), fminf(corr, fmaxf(mx[c], pf[c]))));
+        sstore(f.out[c], (int64_t)s, fmaxf(fminf(mn[c], pf[c]), fminf(corr, fmaxf(mx[c], pf[c]))));
     }
+}
+
+template <typename I>
+void launch_advect_scalars_records(const Context& c, const uint4* rec, const HalfFields& f, float sdt) {
+    const dim3 g = leaf_blocks(c);
+    switch (f.count) {
+        case 1: advect_scalars_records_kernel<1, I><<<g, kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+        case 2: advect_scalars_records_kernel<2, I><<<g, kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+        case 3: advect_scalars_records_kernel<3, I><<<g, kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+        case 4: advect_scalars_records_kernel<4, I><<<g, kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+        default: advect_scalars_records_kernel<5, I><<<g, kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
+    }
+    HNS_LAUNCHED();
 }
 
 // One substep's arrays: BF16 velocity and the five FP16 scalars (null: absent).
@@ -455,14 +466,10 @@ RefinePlan run_advance_mixed(Context& c, const hns_fire_fields& in, const hns_fi
             pack_fire_records_kernel<<<pg, kThreads, 0, c.stream>>>(nxt.vel, f, rec, (int64_t)n);
             HNS_LAUNCHED();
             const float sdt = dt_sub * inv_dx;
-            switch (f.count) {
-                case 1: advect_scalars_records_kernel<1><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
-                case 2: advect_scalars_records_kernel<2><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
-                case 3: advect_scalars_records_kernel<3><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
-                case 4: advect_scalars_records_kernel<4><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
-                default: advect_scalars_records_kernel<5><<<leaf_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, rec, f, sdt); break;
-            }
-            HNS_LAUNCHED();
+            if (c.topo.num_leaves < (int64_t(1) << 22))
+                launch_advect_scalars_records<int32_t>(c, rec, f, sdt);
+            else
+                launch_advect_scalars_records<int64_t>(c, rec, f, sdt);
         }
         c.phase_end();
         cur = nxt;

@@ -114,9 +114,9 @@ __device__ __forceinline__ uint2 relax_row(uint2 XP, uint2 XM, uint2 YP, uint2 Y
 // zero leaf. Offsets are 32-bit element counts (fewer than 2^22 leaves).
 constexpr int kLeavesPerGroup = kLeavesPerBlock * kLeavesPerThread;
 
-template <bool kZero, bool kShared, bool kPdl>
+template <bool kZero, bool kShared, bool kPdl, typename Mid>
 __device__ __forceinline__ void relax_group(const int* __restrict__ nb8, const __half* __restrict__ rhs, __half* e,
-                                            int num_leaves, int g, int colour, float omega) {
+                                            int num_leaves, int g, int colour, float omega, Mid&& mid) {
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
     const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
     const int p = (w + colour) & 1;  // z parity of this colour in the warp's rows
@@ -135,6 +135,7 @@ __device__ __forceinline__ void relax_group(const int* __restrict__ nb8, const _
 #pragma unroll
     for (int k = 0; k < kLeavesPerThread; ++k) B[k] = ld8(rhs + own[k]);
     if constexpr (kZero) {
+        mid();
 #pragma unroll
         for (int k = 0; k < kLeavesPerThread; ++k) {
             float v[4];
@@ -177,6 +178,7 @@ __device__ __forceinline__ void relax_group(const int* __restrict__ nb8, const _
             const __half* zq = e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1);
             ZC[k] = kShared ? (uint32_t)*reinterpret_cast<const unsigned short*>(zq) : (uint32_t)__half_as_ushort(__ldg(zq));
         }
+        mid();  // every load of the pass is in flight
 #pragma unroll
         for (int k = 0; k < kLeavesPerThread; ++k)
             out[k] = p ? relax_row<1>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega)
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int groups = (num_leaves + kLeavesPerGroup - 1) / kLeavesPerGroup;
     for (int g = blockIdx.x; g < groups; g += gridDim.x)
-        relax_group<kZero, false, true>(nb8, rhs, e, num_leaves, g, colour, omega);
+        relax_group<kZero, false, true>(nb8, rhs, e, num_leaves, g, colour, omega, [] {});
 }
 
 // ---- FP32 ---------------------------------------------------------------------------------
@@ -247,9 +249,9 @@ __device__ __forceinline__ float4 relax_row_f32(float4 XP, float4 XM, float4 YP,
 // scales the right-hand side.
 constexpr int kF32LeavesPerGroup = kF32LeavesPerBlock * kF32LeavesPerThread;
 
-template <bool kZero, bool kShared, bool kPdl>
+template <bool kZero, bool kShared, bool kPdl, typename Mid>
 __device__ __forceinline__ void relax_group_f32(const int* __restrict__ nb8, const float* __restrict__ rhs, float* e,
-                                                int num_leaves, int g, int colour, float omega, float dx2) {
+                                                int num_leaves, int g, int colour, float omega, float dx2, Mid&& mid) {
     const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) & 1;
     const int a = lane >> 2, b = 2 * (lane & 3) + ((a + w) & 1);
     const int p = (w + colour) & 1;
@@ -268,6 +270,7 @@ __device__ __forceinline__ void relax_group_f32(const int* __restrict__ nb8, con
 #pragma unroll
     for (int k = 0; k < kF32LeavesPerThread; ++k) B[k] = ldf4(rhs + own[k]);
     if constexpr (kZero) {
+        mid();
 #pragma unroll
         for (int k = 0; k < kF32LeavesPerThread; ++k) {
             float v[4];
@@ -307,6 +310,7 @@ __device__ __forceinline__ void relax_group_f32(const int* __restrict__ nb8, con
             const float* zq = e + ((nz[k] << 9) | ((own[k] ^ 256u) & 511u)) + 3u * (uint32_t)(p ^ 1);
             ZC[k] = kShared ? *zq : __ldg(zq);
         }
+        mid();  // every load of the pass is in flight
 #pragma unroll
         for (int k = 0; k < kF32LeavesPerThread; ++k)
             out[k] = p ? relax_row_f32<1>(XP[k], XM[k], YP[k], YM[k], K[k], ZC[k], B[k], C[k], omega, dx2)
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(kF32Threads, kF32ShortGridCtasPerSm)
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int groups = (num_leaves + kF32LeavesPerGroup - 1) / kF32LeavesPerGroup;
     for (int g = blockIdx.x; g < groups; g += gridDim.x)
-        relax_group_f32<kZero, false, true>(nb8, rhs, e, num_leaves, g, colour, omega, dx2);
+        relax_group_f32<kZero, false, true>(nb8, rhs, e, num_leaves, g, colour, omega, dx2, [] {});
 }
 
 // ---- The persistent solve -------------------------------------------------------------------
@@ -338,12 +342,16 @@ __global__ void __launch_bounds__(kF32Threads, kF32ShortGridCtasPerSm)
 // c, c + G, c + 2G, ... in order (G CTAs, all resident). Before item (h, g) the CTA waits until
 // progress[x] >= h for g itself and for every group x that holds a face neighbour of g's leaves:
 // those groups have finished half-sweep h - 1, so the other colour the item reads is current and
-// no neighbour still has to read the colour the item overwrites. After the item it publishes
-// progress[g] = h + 1 (its stores fenced first). The values are those of the launch-per-colour
-// kernel to the bit: each voxel sees the same operands in the same order.
+// no neighbour still has to read the colour the item overwrites. A done item is published as
+// progress[g] = h + 1 (its stores fenced first) by its CTA during the CTA's next pass, once that
+// pass's loads are in flight, so that the fence costs no time of its own; or at once, before the
+// CTA waits for anything. The next item's dependencies are polled during the current pass too.
+// The values are those of the launch-per-colour kernel to the bit: each voxel sees the same
+// operands in the same order.
 //
-// Every wait ends: an item waits only on smaller items, and the CTA of the smallest unfinished
-// item has finished its own earlier items, so that item's dependencies are all done. Waits are
+// Every wait ends: an item waits only on smaller items; a CTA publishes its done items before it
+// waits, and one that does not wait publishes them during its next pass; so the smallest item
+// not yet published belongs to a CTA that is working on it or about to publish it. Waits are
 // bounded all the same (kSolveMaxPolls polls with a short sleep, about a second): one that gives
 // up raises the device error flag (counters[1]) and the abort word progress[groups], which every
 // other wait watches, and every CTA returns, leaving e unfinished. `unreachable` (0 but in the
@@ -364,8 +372,7 @@ __device__ __forceinline__ void st_relaxed_u32(unsigned* p, uint32_t v) {
 // T = __half: the FP16 inner solve (relax_group, unit spacing); T = float: the FP32 solve
 // (relax_group_f32, dx2). Groups of kLeavesPerGroup or kF32LeavesPerGroup leaves.
 template <typename T, bool kZeroFirst>
-__global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? kShortGridCtasPerSm : kF32ShortGridCtasPerSm)
-    rbgs_split_solve_kernel(
+__global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_solve_kernel(
     const int* __restrict__ nb8, const T* __restrict__ rhs, T* e, int num_leaves, int half_sweeps, float omega, float dx2,
     const double* __restrict__ check, double tol2, unsigned long long* __restrict__ counters, unsigned* progress,
     uint32_t max_polls, uint32_t unreachable) {
@@ -379,25 +386,40 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? kShortGridCtasPerSm
     unsigned* abort_word = progress + groups;
     const int64_t items = (int64_t)half_sweeps * groups;
     // The dependency this thread watches: face df of leaf dl of the item's group (threads 64 ...),
-    // or the group itself (the thread after them).
+    // or the group itself (the thread after them); -1: none (and none in half-sweep 0).
     const int dt = tid - 64, dl = dt / 6, df = dt - 6 * dl;
     const bool watches_face = dt >= 0 && dt < kDepThreads, watches_self = dt == kDepThreads;
+    auto dependency = [&](int h, int g) -> int {
+        if (h == 0) return -1;
+        if (watches_face) {
+            const int leaf = g * kPerGroup + dl;
+            if (leaf >= num_leaves) return -1;
+            const int n = __ldg(nb8 + 8 * leaf + df);
+            return n < num_leaves ? n / kPerGroup : -1;  // the zero leaf is never written
+        }
+        return watches_self ? g : -1;
+    };
+    auto publish = [&](int h, int g) {  // thread 0, after a CTA barrier that follows the item's stores
+        __threadfence();
+        st_relaxed_u32(progress + g, (uint32_t)(h + 1));
+    };
     int h = (int)(blockIdx.x / (unsigned)groups), g = (int)(blockIdx.x % (unsigned)groups);
     const int step_h = (int)(gridDim.x / (unsigned)groups), step_g = (int)(gridDim.x % (unsigned)groups);
+    int x = dependency(h, g);
+    bool ok = x < 0 || ld_acquire_u32(progress + x) >= (uint32_t)h + unreachable;
+    // The CTA's previous item, done but not yet published (ph < 0: none). Its publication waits
+    // for a fence; it is deferred into the next item's pass, after that pass's loads are issued,
+    // unless the next item has to wait (then it comes first: another CTA may wait for it).
+    int ph = -1, pg = 0;
     for (int64_t i = blockIdx.x; i < items; i += gridDim.x) {
-        if (h > 0) {
-            int x = -1;
-            if (watches_face) {
-                const int leaf = g * kPerGroup + dl;
-                if (leaf < num_leaves) {
-                    const int n = __ldg(nb8 + 8 * leaf + df);
-                    if (n < num_leaves) x = n / kPerGroup;  // the zero leaf is never written
-                }
-            } else if (watches_self) {
-                x = g;
-            }
+        // The previous item of this CTA is complete for this CTA's threads (its stores precede
+        // the barrier below): a dependency on it needs no wait.
+        if (!ok && x == pg && h - 1 == ph) ok = true;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0 && ph >= 0) publish(ph, pg);
+            ph = -1;
             bool failed = false;
-            if (x >= 0) {
+            if (!ok) {
                 uint32_t polls = 0;
                 while (ld_acquire_u32(progress + x) < (uint32_t)h + unreachable) {
                     if (++polls >= max_polls) {
@@ -415,26 +437,32 @@ __global__ void __launch_bounds__(kThreads, sizeof(T) == 2 ? kShortGridCtasPerSm
             }
             if (__syncthreads_or(failed)) return;
         }
+        // The next item, and this thread's dependency of it, polled while this pass's loads are
+        // in flight.
+        int nh = h + step_h, ng = g + step_g;
+        if (ng >= groups) ng -= groups, ++nh;
+        const int nx = i + gridDim.x < items ? dependency(nh, ng) : -1;
+        bool nok = true;
+        auto mid = [&] {
+            if (tid == 0 && ph >= 0) publish(ph, pg);
+            if (nx >= 0) nok = ld_acquire_u32(progress + nx) >= (uint32_t)nh + unreachable;
+        };
         if constexpr (kHalf) {
             if (kZeroFirst && h == 0)
-                relax_group<true, true, false>(nb8, rhs, e, num_leaves, g, 0, omega);
+                relax_group<true, true, false>(nb8, rhs, e, num_leaves, g, 0, omega, mid);
             else
-                relax_group<false, true, false>(nb8, rhs, e, num_leaves, g, h & 1, omega);
+                relax_group<false, true, false>(nb8, rhs, e, num_leaves, g, h & 1, omega, mid);
         } else {
             if (kZeroFirst && h == 0)
-                relax_group_f32<true, true, false>(nb8, rhs, e, num_leaves, g, 0, omega, dx2);
+                relax_group_f32<true, true, false>(nb8, rhs, e, num_leaves, g, 0, omega, dx2, mid);
             else
-                relax_group_f32<false, true, false>(nb8, rhs, e, num_leaves, g, h & 1, omega, dx2);
+                relax_group_f32<false, true, false>(nb8, rhs, e, num_leaves, g, h & 1, omega, dx2, mid);
         }
-        __syncthreads();
-        if (tid == 0) {
-            __threadfence();
-            st_relaxed_u32(progress + g, (uint32_t)(h + 1));
-        }
-        h += step_h;
-        g += step_g;
-        if (g >= groups) g -= groups, ++h;
+        ph = h, pg = g;
+        h = nh, g = ng, x = nx, ok = nok;
     }
+    __syncthreads();
+    if (tid == 0 && ph >= 0) publish(ph, pg);
 }
 
 // Entry base of the half row (z = 4h .. 4h + 3) that starts at slot q (a multiple of 4), in the
@@ -623,8 +651,9 @@ void launch_split_solve(Context& c, const int* nb8, const T* rhs, T* e, int half
     int per_sm = 0;
     HNS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0));
     if (per_sm < 1) fail(HNS_ERR_CUDA, "the persistent solve does not fit on an SM");
-    const int64_t items = (int64_t)half_sweeps * groups;
-    const unsigned blocks = (unsigned)std::min<int64_t>(items, (int64_t)per_sm * c.sm_count());
+    // At most one CTA per group: a CTA beyond that could only hold an item of a later half-sweep
+    // and wait for it.
+    const unsigned blocks = (unsigned)std::min<int64_t>(groups, (int64_t)per_sm * c.sm_count());
     // The test hook: every wait gives up after first_wait_polls polls, its target out of reach.
     const bool stall = c.first_wait_polls >= 0;
     const uint32_t max_polls = stall ? (uint32_t)c.first_wait_polls : kSolveMaxPolls;

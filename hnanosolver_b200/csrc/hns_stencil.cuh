@@ -234,6 +234,45 @@ __device__ __forceinline__ void interp_setup(const TopoView& t, const LeafNbhd& 
     idx[7] = tap_slot(t, L, i1, j1, k1);
 }
 
+// interp_setup with the taps' slots in I (int32_t where the grid has fewer than 2^22 leaves):
+// the same weights and the same slots, the cell's planes resolved once as in taps_at when both
+// lie in the CTA leaf's neighbourhood.
+template <typename I>
+__device__ __forceinline__ void interp_setup_fast(const TopoView& t, const LeafNbhd& L, float x, float y, float z,
+                                                  I idx[8], float w[8]) {
+    const int i0 = __float2int_rd(x), j0 = __float2int_rd(y), k0 = __float2int_rd(z);
+    const int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+    const float tx = x - (float)i0, ty = y - (float)j0, tz = z - (float)k0;
+    const float itx = 1.0f - tx, ity = 1.0f - ty, itz = 1.0f - tz;
+    const float w00 = itx * ity, w10 = tx * ity, w01 = itx * ty, w11 = tx * ty;
+    w[0] = w00 * itz;
+    w[1] = w10 * itz;
+    w[2] = w01 * itz;
+    w[3] = w11 * itz;
+    w[4] = w00 * tz;
+    w[5] = w10 * tz;
+    w[6] = w01 * tz;
+    w[7] = w11 * tz;
+    const int a0 = (i0 >> 3) - L.lx + 1, a1 = (i1 >> 3) - L.lx + 1;
+    const int b0 = (j0 >> 3) - L.ly + 1, b1 = (j1 >> 3) - L.ly + 1;
+    const int c0 = (k0 >> 3) - L.lz + 1, c1 = (k1 >> 3) - L.lz + 1;
+    if ((unsigned)a0 < 3u && (unsigned)a1 < 3u && (unsigned)b0 < 3u && (unsigned)b1 < 3u && (unsigned)c0 < 3u &&
+        (unsigned)c1 < 3u) {
+        const int na[2] = {a0 * 9, a1 * 9}, nb[2] = {b0 * 3, b1 * 3}, nc[2] = {c0, c1};
+        const int la[2] = {(i0 & 7) << 6, (i1 & 7) << 6}, lb[2] = {(j0 & 7) << 3, (j1 & 7) << 3};
+        const int lc[2] = {k0 & 7, k1 & 7};
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int A = q & 1, B = (q >> 1) & 1, C = q >> 2;  // interp_setup's order: x fastest
+            const int l = L.nb[na[A] + nb[B] + nc[C]];
+            idx[q] = l < 0 ? I(0) : (I(l) << 9) + I(la[A] | lb[B] | lc[C]);  // outside: slot 0
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) idx[q] = (I)tap_slot(t, L, (q & 1) ? i1 : i0, (q & 2) ? j1 : j0, (q & 4) ? k1 : k0);
+    }
+}
+
 // |curl u| at a voxel (computeVorticityMag, src/Cuda/Utils.cuh:226-243).
 __device__ __forceinline__ float vort_mag(const TopoView& t, const LeafNbhd& L, const float* __restrict__ v, int i, int j, int k, float factor) {
     const float3 px = near_v(t, L, v, i + 1, j, k), mx = near_v(t, L, v, i - 1, j, k);
