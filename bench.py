@@ -57,8 +57,12 @@ RBGS_BYTES_PER_VOXEL = 12  # one fused red+black iteration: read p, read div, wr
 # bytes, counted by the library's device counter of red-black sweeps that ran.
 F32_HALF_SWEEP_BYTES = RBGS_BYTES_PER_VOXEL // 2
 F16_HALF_SWEEP_BYTES = 3  # read e, read r, write e at 2 bytes each, halved
-F32_KERNEL = "rbgs_split_solve_kernel<float> (FP32 solve, colour-split leaves, persistent: one launch per run of half-sweeps between checks)"
-F16_KERNEL = "rbgs_split_solve_kernel<__half> (FP16 inner solve, colour-split leaves, persistent: one launch per inner solve)"
+KERNELS = {("f32", "per-colour"): "rbgs_split_half_f32_kernel (FP32 solve, colour-split leaves, one launch per colour)",
+           ("f16", "per-colour"): "rbgs_split_half_kernel (FP16 inner solve, colour-split leaves, one launch per colour)",
+           ("f32", "persistent"): "rbgs_split_solve_kernel<float> (FP32 solve, colour-split leaves, persistent: one "
+                                  "launch per run of half-sweeps between checks)",
+           ("f16", "persistent"): "rbgs_split_solve_kernel<__half> (FP16 inner solve, colour-split leaves, persistent: "
+                                  "one launch per inner solve)"}
 
 # The fire step (HNS_Advance with the configurations' forces): the sparse plume runs it in FP32
 # with a fixed 100 red-black iterations per step, the large sparse fire on BF16/FP16 storage with
@@ -97,7 +101,7 @@ def measured_peak_gbs():
 
 def apply_options(g, hl, args):
     """The library options the command line selects."""
-    form = getattr(args, "split_solve", "persistent")
+    form = getattr(args, "split_solve", "per-colour")
     g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT if form == "persistent" else hl.SPLIT_PER_COLOUR)
 
 
@@ -317,6 +321,45 @@ def cpu_baseline(args, wl, iters):
                       f"{iters} red-black iterations", "cpu": binding.cpu_model()}
 
 
+def field_error_vs_fp64(torch, origins, wl, vel_in, dens_in, vel_out, dens_out, dev):
+    """Field error of one step's result against the same step in FP64 from the same stored
+    inputs: MacCormack advection of velocity and density, then the projection with the exact
+    solve (conjugate gradients to an FP64 residual of 1e-12). The checker is the torch FP64
+    restatement tests/fp64_box.py on a dense box holding the grid's active voxels, pinned there
+    against the FP64 oracle. Errors are max |step - fp64| / max |fp64| per field, after the
+    timed region and outside it."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from fp64_box import Box, active_mask, from_dense, to_dense
+
+    from hnanosolver_b200 import synth
+
+    t0 = time.perf_counter()
+    coords = torch.from_numpy(synth.leaf_dense_coords(origins)).to(dev)
+    lo = coords.min(dim=0).values.cpu().numpy()
+    shape = tuple(int(v) for v in (coords.max(dim=0).values.cpu().numpy() - lo + 1))
+    box = Box(shape, lo, wl["dx"], dev, active=active_mask(coords, lo, shape, dev))
+    v64 = to_dense(vel_in.double(), coords, lo, shape, dev)
+    d64 = to_dense(dens_in.double(), coords, lo, shape, dev)
+    v_adv, (d_adv,), _ = box.advect(v64, [d64], wl["dt"])
+    del v64, d64
+    v_prj, cg_iterations, cg_residual = box.project_exact(v_adv)
+    del v_adv
+    torch.cuda.empty_cache()
+
+    def rel(got, ref):
+        return float((got.double() - ref).abs().max() / ref.abs().max().clamp_min(1e-300))
+
+    ref_v = from_dense(v_prj[0], coords, lo, numpy=False)
+    ref_d = from_dense(d_adv[0], coords, lo, numpy=False)
+    err = {"velocity": rel(vel_out.reshape(-1, 3), ref_v), "density": rel(dens_out.reshape(-1), ref_d),
+           "checker": "torch FP64 restatement (tests/fp64_box.py) of advection + exact projection from the step's "
+                      "stored inputs; max |step - fp64| / max |fp64|",
+           "fp64_solve": {"cg_iterations": cg_iterations, "residual": cg_residual}, "seconds": time.perf_counter() - t0}
+    del box, v_prj, d_adv, ref_v, ref_d, coords
+    torch.cuda.empty_cache()
+    return err
+
+
 def _timed_steps(torch, stream, fn, steps):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -508,12 +551,12 @@ def ours(args, wl):
         # record packing, advection, divergence, first residual, convergence log, gradient; per
         # outer iteration scale, 2 half-sweeps per inner iteration, update, residual (the face
         # table is made once per context).
-        kernel_bytes, kernel_name, phase = F16_HALF_SWEEP_BYTES, F16_KERNEL, "inner"
+        kernel_bytes, kernel_name, phase = F16_HALF_SWEEP_BYTES, KERNELS[("f16", args.split_solve)], "inner"
     else:
         info, outer = info32, None
         st = plain_desc(cap32)
         step = step32(st)
-        kernel_bytes, kernel_name, phase = F32_HALF_SWEEP_BYTES, F32_KERNEL, "solve"
+        kernel_bytes, kernel_name, phase = F32_HALF_SWEEP_BYTES, KERNELS[("f32", args.split_solve)], "solve"
 
     for _ in range(args.warmup):
         step()
@@ -563,6 +606,15 @@ def ours(args, wl):
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     e2e_s = replicas.max_over_ranks(R, e2e_s, dev)
 
+    # The last timed step's result against FP64 (its inputs are the other buffer of the pair).
+    field_error = None
+    if rank == 0 and not args.no_field_error:
+        out_i = ms_state[0] if mixed else state[0]
+        if mixed:
+            field_error = field_error_vs_fp64(torch, origins, wl, vb[1 - out_i], dh[1 - out_i], vb[out_i], dh[out_i], dev)
+        else:
+            field_error = field_error_vs_fp64(torch, origins, wl, v[1 - out_i], d[1 - out_i], v[out_i], d[out_i], dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args, wl, wl["fp32_iterations"])
@@ -578,7 +630,7 @@ def ours(args, wl):
                "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
                "timed_solves_logged": logged, "worst_residual_timed_steps": worst,
-               "timed_steps_above_tolerance": not_converged}
+               "timed_steps_above_tolerance": not_converged, "field_error_vs_fp64": field_error}
         if mixed:
             det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
                         "omega_inner": wl["omega_refined"], "inner_iterations": wl["inner"], "outer_cap": outer,
@@ -874,7 +926,7 @@ def ours_fire(args, wl):
         # record packing, velocity advection, confinement, divergence/burn/buoyancy, first residual,
         # convergence log, gradient, scalar advection; per outer iteration scale, 2 half-sweeps per
         # inner iteration, update, residual.
-        kernel_bytes, kernel_name, phase = F16_HALF_SWEEP_BYTES, F16_KERNEL, "inner"
+        kernel_bytes, kernel_name, phase = F16_HALF_SWEEP_BYTES, KERNELS[("f16", args.split_solve)], "inner"
     else:
         load_fp32()
         iters = wl["iterations"]
@@ -885,7 +937,7 @@ def ours_fire(args, wl):
 
         # velocity advection, confinement and sources, divergence/burn/buoyancy, the red-black
         # iterations, gradient, scalar advection.
-        kernel_bytes, kernel_name, phase = F32_HALF_SWEEP_BYTES, F32_KERNEL, "solve"
+        kernel_bytes, kernel_name, phase = F32_HALF_SWEEP_BYTES, KERNELS[("f32", args.split_solve)], "solve"
 
     for _ in range(args.warmup):
         step()
@@ -1134,7 +1186,9 @@ def main():
                     help="mixed (default for the SOP chain and fire1024) or fp32 (default for plume256 --forces)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout measured beside the step")
-    ap.add_argument("--split-solve", choices=["persistent", "per-colour"], default="persistent",
+    ap.add_argument("--no-field-error", action="store_true",
+                    help="skip the FP64 check of the last timed step's fields (shell512 and plume256 steps)")
+    ap.add_argument("--split-solve", choices=["persistent", "per-colour"], default="per-colour",
                     help="launch form of the colour-split red-black solves (same results to the bit)")
     ap.add_argument("--no-fp32-comparison", action="store_true",
                     help="skip the FP32 forms measured beside the mixed one (profiling runs)")

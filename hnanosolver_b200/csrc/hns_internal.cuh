@@ -174,7 +174,7 @@ struct Context {
     int rbgs_kernel = HNS_RBGS_SPLIT;     // hns_set_option(HNS_OPT_RBGS_KERNEL)
     int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
-    int split_solve = HNS_SPLIT_PERSISTENT;  // hns_set_option(HNS_OPT_SPLIT_SOLVE)
+    int split_solve = HNS_SPLIT_PER_COLOUR;  // hns_set_option(HNS_OPT_SPLIT_SOLVE)
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;

@@ -493,11 +493,12 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
                                     gives up after `value` polls, raising the flag; every CTA then
                                     returns, leaving the solve unfinished. */
 #define HNS_OPT_SPLIT_SOLVE 4   /* how the colour-split solves (HNS_RBGS_SPLIT, HNS_INNER_SPLIT) launch: */
-#define HNS_SPLIT_PER_COLOUR 0  /*   one launch per half-sweep (programmatic dependent launches) */
+#define HNS_SPLIT_PER_COLOUR 0  /*   one launch per half-sweep (programmatic dependent launches;
+                                     default: the faster of the two on a B200) */
 #define HNS_SPLIT_PERSISTENT 1  /*   one cooperative launch per inner solve, or per run of iterations
                                      between convergence checks, leaf groups ordered by per-group
-                                     progress counters instead of launch boundaries (default). Both
-                                     give the same results to the bit. */
+                                     progress counters instead of launch boundaries. Both give the
+                                     same results to the bit. */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */

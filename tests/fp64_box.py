@@ -1,14 +1,18 @@
-"""FP64 restatement, in torch, of the plain step on a FULLY ACTIVE box: MacCormack advection
+"""FP64 restatement, in torch, of the plain step on a box of voxels: MacCormack advection
 of the velocity (advect_vector, src/Cuda/Kernel.cu:349-426) and of scalars (advect_scalar,
 src/Cuda/Kernel.cu:294-344), divergence (Kernel.cu:432-453), red-black SOR from p = 0
 (Kernel.cu:459-489, driven as in src/Cuda/HNanoSolver.cu:366-373) and gradient subtraction
-(Kernel.cu:495-541), with every read outside the box 0.
+(Kernel.cu:495-541), with every read outside the box 0. The box is fully active, or holds a
+sparse grid as a mask of its active voxels (`active`), every read of an inactive voxel 0 as the
+reference reads outside its index grid.
 
 Test infrastructure only: it is the checker that makes central finite differences of long
 rollouts affordable (a batch of perturbed states steps at once on the device), and it follows
 the FP64 oracle (oracle/hns_oracle_impl.h) formula for formula; test_oracle pins it against
-that oracle. Every voxel of the box is active, so a field is a dense array: scalars
-(B, X, Y, Z), velocity (B, 3, X, Y, Z), index (x, y, z) = coordinate - box origin.
+that oracle. A field is a dense array over the box, 0 at inactive voxels: scalars (B, X, Y, Z),
+velocity (B, 3, X, Y, Z), index (x, y, z) = coordinate - box origin. `solve_exact` (conjugate
+gradients to an FP64 residual of 1e-12) gives the projection the iterative solves approach, the
+reference point of the field error of a step solved to a tolerance.
 """
 import numpy as np
 import torch
@@ -18,10 +22,19 @@ PAD = 4  # taps up to PAD voxels outside the box read the zero padding; further 
 NBRS = ((-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0), (0, 0, -1), (0, 0, 1))  # the clamp's neighbour order
 
 
-def to_dense(values: np.ndarray, coords: np.ndarray, lo, shape, device, dtype=torch.float64) -> torch.Tensor:
-    """Slot-ordered values ((N,) or (N, 3)) -> (1, X, Y, Z) or (1, 3, X, Y, Z)."""
-    v = torch.as_tensor(np.asarray(values, dtype=np.float64), device=device, dtype=dtype)
-    c = torch.as_tensor(np.asarray(coords, dtype=np.int64) - np.asarray(lo, dtype=np.int64), device=device)
+def _index(coords, lo, device) -> torch.Tensor:
+    if isinstance(coords, torch.Tensor):
+        return coords.to(device=device, dtype=torch.int64) - torch.as_tensor(np.asarray(lo, dtype=np.int64), device=device)
+    return torch.as_tensor(np.asarray(coords, dtype=np.int64) - np.asarray(lo, dtype=np.int64), device=device)
+
+
+def to_dense(values, coords, lo, shape, device, dtype=torch.float64) -> torch.Tensor:
+    """Slot-ordered values ((N,) or (N, 3), numpy or torch) -> (1, X, Y, Z) or (1, 3, X, Y, Z)."""
+    if isinstance(values, torch.Tensor):
+        v = values.to(device=device, dtype=dtype)
+    else:
+        v = torch.as_tensor(np.asarray(values, dtype=np.float64), device=device, dtype=dtype)
+    c = _index(coords, lo, device)
     if v.ndim == 1:
         out = torch.zeros((1,) + tuple(shape), device=device, dtype=dtype)
         out[0, c[:, 0], c[:, 1], c[:, 2]] = v
@@ -31,18 +44,28 @@ def to_dense(values: np.ndarray, coords: np.ndarray, lo, shape, device, dtype=to
     return out
 
 
-def from_dense(d: torch.Tensor, coords: np.ndarray, lo) -> np.ndarray:
-    """(X, Y, Z) or (3, X, Y, Z) -> slot-ordered (N,) or (N, 3) float64."""
-    c = torch.as_tensor(np.asarray(coords, dtype=np.int64) - np.asarray(lo, dtype=np.int64), device=d.device)
-    if d.ndim == 3:
-        return d[c[:, 0], c[:, 1], c[:, 2]].cpu().numpy()
-    return d[:, c[:, 0], c[:, 1], c[:, 2]].T.cpu().numpy()
+def from_dense(d: torch.Tensor, coords, lo, numpy: bool = True):
+    """(X, Y, Z) or (3, X, Y, Z) -> slot-ordered (N,) or (N, 3) float64 (numpy, or a tensor on
+    d's device)."""
+    c = _index(coords, lo, d.device)
+    out = d[c[:, 0], c[:, 1], c[:, 2]] if d.ndim == 3 else d[:, c[:, 0], c[:, 1], c[:, 2]].T
+    return out.cpu().numpy() if numpy else out
+
+
+def active_mask(coords, lo, shape, device) -> torch.Tensor:
+    """The box's active voxels (X, Y, Z) bool, from the grid's voxel coordinates."""
+    c = _index(coords, lo, device)
+    m = torch.zeros(tuple(shape), dtype=torch.bool, device=device)
+    m[c[:, 0], c[:, 1], c[:, 2]] = True
+    return m
 
 
 class Box:
-    """Operators on a dense box of the given shape whose first voxel has coordinate `lo`."""
+    """Operators on a dense box of the given shape whose first voxel has coordinate `lo`;
+    `active` (X, Y, Z) bool marks the grid's voxels (None: all). Inputs are 0 at inactive
+    voxels, and so are the outputs."""
 
-    def __init__(self, shape, lo, dx: float, device):
+    def __init__(self, shape, lo, dx: float, device, active=None):
         self.shape = tuple(int(s) for s in shape)
         self.lo = tuple(int(v) for v in lo)
         self.dx = float(dx)
@@ -52,7 +75,11 @@ class Box:
         ax = [torch.arange(n, device=device, dtype=torch.float64) + o for n, o in zip(self.shape, self.lo)]
         self.gx, self.gy, self.gz = torch.meshgrid(ax[0], ax[1], ax[2], indexing="ij")
         par = (self.gx + self.gy + self.gz).long() & 1
-        self.colour = [par == 0, par == 1]
+        self.active = active
+        self.colour = [par == 0, par == 1] if active is None else [(par == 0) & active, (par == 1) & active]
+
+    def _mask(self, f):
+        return f if self.active is None else torch.where(self.active, f, torch.zeros((), dtype=f.dtype, device=f.device))
 
     # ---- reads ----
     @staticmethod
@@ -145,7 +172,8 @@ class Box:
             o, sc = self._clamp(s, self._sample(s, tb), self._sample(s, tf), fr["scalars"][q] if fr else None)
             souts.append(o)
             ssel.append(sc)
-        return torch.stack(vout, dim=1), souts, {"back": fb, "fwd": ff, "vel": vsel, "scalars": ssel}
+        souts = [self._mask(o) for o in souts]
+        return self._mask(torch.stack(vout, dim=1)), souts, {"back": fb, "fwd": ff, "vel": vsel, "scalars": ssel}
 
     # ---- projection ----
     def divergence(self, vel):
@@ -156,7 +184,7 @@ class Box:
             p = (u + self._nbr(up, *d)) * 0.5
             m = (u + self._nbr(up, -d[0], -d[1], -d[2])) * 0.5
             out = out + (p - m)
-        return out * self.inv_dx
+        return self._mask(out * self.inv_dx)
 
     def rbgs(self, div, iterations, omega):
         """Red-black SOR from p = 0 (colour 0 first), p + omega (pgs - p) written as
@@ -181,10 +209,47 @@ class Box:
         pp = self._pad1(p)
         g = [(self._nbr(pp, *d) - self._nbr(pp, -d[0], -d[1], -d[2])) * h
              for d in ((1, 0, 0), (0, 1, 0), (0, 0, 1))]
-        return vel - torch.stack(g, dim=1)
+        return self._mask(vel - torch.stack(g, dim=1))
 
     def project(self, vel, iterations, omega):
         return self.subtract_gradient(vel, self.rbgs(self.divergence(vel), iterations, omega))
+
+    def laplacian(self, p):
+        """L p = the six face neighbours' sum - 6 p (0 outside the grid), at the active voxels."""
+        pp = self._pad1(p)
+        s = self._nbr(pp, 1, 0, 0) + self._nbr(pp, -1, 0, 0) + self._nbr(pp, 0, 1, 0) + self._nbr(pp, 0, -1, 0)
+        s = s + self._nbr(pp, 0, 0, 1) + self._nbr(pp, 0, 0, -1)
+        return self._mask(s - 6.0 * p)
+
+    def solve_exact(self, div, tol: float = 1e-12, max_iterations: int = 20000):
+        """p with L p = div dx^2 to a relative FP64 residual |b - L p| / |b| <= tol, by conjugate
+        gradients on -L (symmetric positive definite with p = 0 outside the grid), from p = 0.
+        Returns (p, iterations, relative residual)."""
+        b = -div * (self.dx * self.dx)
+        p = torch.zeros_like(b)
+        r = b.clone()
+        d = r.clone()
+        bb = float((b * b).sum())
+        if bb == 0.0:
+            return p, 0, 0.0
+        rr = bb
+        it = 0
+        while it < max_iterations and rr > tol * tol * bb:
+            q = -self.laplacian(d)
+            a = rr / float((d * q).sum())
+            p.add_(d, alpha=a)
+            r.sub_(q, alpha=a)
+            rr_new = float((r * r).sum())
+            d.mul_(rr_new / rr).add_(r)
+            rr = rr_new
+            it += 1
+        res = self.laplacian(p) - div * (self.dx * self.dx)
+        return p, it, float(torch.sqrt((res * res).sum() / bb))
+
+    def project_exact(self, vel, tol: float = 1e-12):
+        """The projection with the exact solve. Returns (velocity, iterations, residual)."""
+        p, it, res = self.solve_exact(self.divergence(vel), tol)
+        return self.subtract_gradient(vel, p), it, res
 
     def step(self, vel, scalars, dt, iterations, omega, frozen=None):
         """The plain step: advect (velocity and scalars along the incoming velocity), project.

@@ -164,7 +164,7 @@ def test_rbgs_kernels_bit_exact(case, dev, kernel, form, iters, zero):
 
     g, t = case["grid"], case["topo"]
     g.set_option(hl.OPT_RBGS_KERNEL, kernel)
-    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT if form is None else form)
+    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PER_COLOUR if form is None else form)
     div = t.divergence(case["vel"], 10.0)
     p0 = np.zeros_like(div) if zero else (case["dens"] * 0.01).astype(np.float32)
     p = T(p0, dev)
@@ -172,7 +172,7 @@ def test_rbgs_kernels_bit_exact(case, dev, kernel, form, iters, zero):
     g.device_status()
     assert bit_exact(H(p), t.rbgs(div, p0, 0.1, iters, 1.8))
     g.set_option(hl.OPT_RBGS_KERNEL, hl.RBGS_SPLIT)
-    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT)
+    g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PER_COLOUR)
 
 
 def test_rbgs_unaligned_pointers_fall_back(case, dev):

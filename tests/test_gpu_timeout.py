@@ -91,11 +91,13 @@ def test_persistent_inner_solve_wait_gives_up_then_recovers(dev):
         return vo.cpu(), p.cpu()
 
     clean = hl.Grid(origins, voxel_size=0.1)
+    clean.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT)
     ref = step(clean)
     assert hl.lib.hns_device_status(clean._h) == 0
     clean.close()
 
     grid = hl.Grid(origins, voxel_size=0.1)
+    grid.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT)
     grid.set_option(hl.OPT_WAIT_POLLS, 0)
     step(grid)
     s = hl.lib.hns_device_status(grid._h)
