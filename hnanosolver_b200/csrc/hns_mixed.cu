@@ -766,8 +766,10 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         const TI* src = nullptr;
         const void* src_faces = nullptr;
         c.phase_begin(HNS_PHASE_INNER);
-        // The persistent form: the whole inner solve in one launch.
-        const bool persistent = layout == HNS_INNER_SPLIT && c.split_solve == HNS_SPLIT_PERSISTENT;
+        // The persistent form: the whole inner solve in one launch. An outer iteration past the
+        // forecast takes it whatever the option: it most likely returns at once, and one launch
+        // then costs a few microseconds where 2 * inner returning half-sweeps cost 2.3 us each.
+        const bool persistent = layout == HNS_INNER_SPLIT && (c.split_solve == HNS_SPLIT_PERSISTENT || spare);
         if (persistent) {
             if constexpr (sizeof(TI) == 2)
                 launch_rbgs_split_solve(c, nb8, rhat, e_split, 2 * plan.inner, true, omega, chk, tol2);
@@ -946,6 +948,123 @@ __global__ void __launch_bounds__(kThreads, 4) advect_records_kernel(TopoView t,
     }
 }
 
+// ---- advection from a leaf tile in shared memory --------------------------------------------
+// advect_records_kernel with the leaf's voxel records and a kTileHalo-voxel halo around it
+// unpacked once into shared memory as FP32 (u, v, w, s), a tile of kTileSide^3 cells at local
+// coordinates [-kTileHalo, 8 + kTileHalo). A trace cell whose eight corners lie in the tile is
+// eight shared-memory loads at fixed offsets from one base index (a back trace shorter than a
+// voxel per axis, and a forward trace that ends within a voxel of the start); other cells take
+// the leaf-table path of the records kernel. The clamp's six face neighbours always lie in the
+// tile. Same values, same lerps in the same order, same clamps: the records kernel's results
+// to the bit. One CTA of 256 threads per leaf, two voxels per thread (x and x + 4), four CTAs
+// per SM so that one CTA's tile fill overlaps the others' sampling; cells of missing leaves
+// hold 0, as the records kernel reads outside the domain.
+constexpr int kTileHalo = 1;
+constexpr int kTileSide = 8 + 2 * kTileHalo;
+constexpr int kTileCells = kTileSide * kTileSide * kTileSide;
+constexpr int kTileThreads = 256;
+constexpr int kTileFill = (kTileCells + kTileThreads - 1) / kTileThreads;  // cells a thread fills
+
+__device__ __forceinline__ float4 unpack_rec(uint2 r) {
+    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xFFFF0000u), __uint_as_float(r.y << 16),
+                       __half2float(__ushort_as_half((unsigned short)(r.y >> 16))));
+}
+
+// Trilinear sample of the four channels at (x, y, z) (global voxel units), lerps along z, then
+// y, then x (tri_lerp's order).
+__device__ __forceinline__ float4 tile_sample(const float4* __restrict__ tile, const TopoView& t, const LeafNbhd& L,
+                                              const uint2* __restrict__ rec, float x, float y, float z) {
+    const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
+    const float tx = x - (float)i, ty = y - (float)j, tz = z - (float)k;
+    const int cx = i - (L.lx << 3) + kTileHalo, cy = j - (L.ly << 3) + kTileHalo, cz = k - (L.lz << 3) + kTileHalo;
+    float4 c[8];
+    if ((unsigned)cx <= (unsigned)(kTileSide - 2) && (unsigned)cy <= (unsigned)(kTileSide - 2) &&
+        (unsigned)cz <= (unsigned)(kTileSide - 2)) {
+        const float4* b = tile + (cx * kTileSide + cy) * kTileSide + cz;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) c[q] = b[(q >> 2) * kTileSide * kTileSide + ((q >> 1) & 1) * kTileSide + (q & 1)];
+    } else {
+        TapsT<int32_t> tp;
+        taps_at(tp, t, L, x, y, z);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) c[q] = tp.s[q] < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : unpack_rec(__ldg(rec + (uint32_t)tp.s[q]));
+    }
+    auto tri = [&](float v0, float v1, float v2, float v3, float v4, float v5, float v6, float v7) {
+        const float z0 = lerp1(v0, v1, tz), z1 = lerp1(v2, v3, tz), z2 = lerp1(v4, v5, tz), z3 = lerp1(v6, v7, tz);
+        return lerp1(lerp1(z0, z1, ty), lerp1(z2, z3, ty), tx);
+    };
+    return make_float4(tri(c[0].x, c[1].x, c[2].x, c[3].x, c[4].x, c[5].x, c[6].x, c[7].x),
+                       tri(c[0].y, c[1].y, c[2].y, c[3].y, c[4].y, c[5].y, c[6].y, c[7].y),
+                       tri(c[0].z, c[1].z, c[2].z, c[3].z, c[4].z, c[5].z, c[6].z, c[7].z),
+                       tri(c[0].w, c[1].w, c[2].w, c[3].w, c[4].w, c[5].w, c[6].w, c[7].w));
+}
+
+__global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t, const uint2* __restrict__ rec,
+                                                                       __nv_bfloat16* __restrict__ vel_out,
+                                                                       __half* __restrict__ s0_out, float sdt) {
+    __shared__ float4 tile[kTileCells];
+    __shared__ LeafNbhd L;
+    const int64_t leaf = blockIdx.x;
+    load_nbhd(L, t, leaf);
+    __syncthreads();
+    // The fill: every load of the thread's cells is issued before any is unpacked.
+    uint2 raw[kTileFill];
+#pragma unroll
+    for (int m = 0; m < kTileFill; ++m) {
+        const int q = threadIdx.x + m * kTileThreads;
+        raw[m] = make_uint2(0u, 0u);
+        if (q < kTileCells) {
+            const int lx = q / (kTileSide * kTileSide) - kTileHalo, ly = (q / kTileSide) % kTileSide - kTileHalo,
+                      lz = q % kTileSide - kTileHalo;
+            const int r = (lx < 0 ? 0 : lx > 7 ? 18 : 9) + (ly < 0 ? 0 : ly > 7 ? 6 : 3) + (lz < 0 ? 0 : lz > 7 ? 2 : 1);
+            const int l = L.nb[r];
+            if (l >= 0) raw[m] = __ldg(rec + (((uint32_t)l << 9) | (uint32_t)(((lx & 7) << 6) | ((ly & 7) << 3) | (lz & 7))));
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < kTileFill; ++m) {
+        const int q = threadIdx.x + m * kTileThreads;
+        if (q < kTileCells) tile[q] = unpack_rec(raw[m]);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int half = 0; half < 2; ++half) {
+        const int n = (int)threadIdx.x + half * kTileThreads;
+        const int a = n >> 6, b = (n >> 3) & 7, cz = n & 7;
+        const int i = (L.lx << 3) + a, j = (L.ly << 3) + b, k = (L.lz << 3) + cz;
+        const float4* centre = tile + ((a + kTileHalo) * kTileSide + (b + kTileHalo)) * kTileSide + (cz + kTileHalo);
+        const float4 o = *centre;
+        const float bx = (float)i - o.x * sdt, by = (float)j - o.y * sdt, bz = (float)k - o.z * sdt;
+        const float4 f = tile_sample(tile, t, L, rec, bx, by, bz);
+        const float4 g = tile_sample(tile, t, L, rec, bx + f.x * sdt, by + f.y * sdt, bz + f.z * sdt);
+        float3 corr = make_float3(f.x + 0.5f * (o.x - g.x), f.y + 0.5f * (o.y - g.y), f.z + 0.5f * (o.z - g.z));
+        float3 mn = make_float3(o.x, o.y, o.z), mx = mn;
+        float dmn = o.w, dmx = o.w;
+        constexpr int kOff[6] = {-kTileSide * kTileSide, kTileSide * kTileSide, -kTileSide, kTileSide, -1, 1};
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const float4 e = centre[kOff[q]];
+            mn.x = fminf(mn.x, e.x), mn.y = fminf(mn.y, e.y), mn.z = fminf(mn.z, e.z);
+            mx.x = fmaxf(mx.x, e.x), mx.y = fmaxf(mx.y, e.y), mx.z = fmaxf(mx.z, e.z);
+            dmn = fminf(dmn, e.w);
+            dmx = fmaxf(dmx, e.w);
+        }
+        mn.x = fminf(mn.x, f.x), mn.y = fminf(mn.y, f.y), mn.z = fminf(mn.z, f.z);
+        mx.x = fmaxf(mx.x, f.x), mx.y = fmaxf(mx.y, f.y), mx.z = fmaxf(mx.z, f.z);
+        corr.x = fmaxf(mn.x, fminf(corr.x, mx.x));
+        corr.y = fmaxf(mn.y, fminf(corr.y, mx.y));
+        corr.z = fmaxf(mn.z, fminf(corr.z, mx.z));
+        const int64_t s = (leaf << 9) + n;
+        vstore(vel_out, s, corr);
+        if (s0_out != nullptr) {
+            const float dcorr = f.w + 0.5f * (o.w - g.w);
+            dmn = fminf(dmn, f.w);
+            dmx = fmaxf(dmx, f.w);
+            sstore(s0_out, s, fmaxf(dmn, fminf(dcorr, dmx)));
+        }
+    }
+}
+
 }  // namespace
 
 void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void* const* sin, void* const* sout, int ns,
@@ -960,6 +1079,14 @@ void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void*
         pack_records_kernel<<<stream_blocks(c, n), kThreads, 0, c.stream>>>(
             static_cast<const __nv_bfloat16*>(vel), ns > 0 ? static_cast<const __half*>(sin[0]) : nullptr, rec, n);
         HNS_LAUNCHED();
+        if (ns <= 1) {
+            // Velocity and at most one scalar: the shared-memory leaf tile.
+            advect_tile_kernel<<<(unsigned)c.topo.num_leaves, kTileThreads, 0, c.stream>>>(
+                c.topo.view, reinterpret_cast<const uint2*>(rec), static_cast<__nv_bfloat16*>(vel_out),
+                ns > 0 ? static_cast<__half*>(sout[0]) : nullptr, sdt);
+            HNS_LAUNCHED();
+            return;
+        }
         FieldSetT<__half> f{};
         f.count = std::max(0, ns - 1);
         for (int q = 0; q < f.count; ++q) {

@@ -152,6 +152,33 @@ def test_mixed_step_scalar_counts(dev, oracle, shell, nscalars):
     g.close()
 
 
+def test_mixed_advection_long_traces(dev, oracle, shell):
+    """Traces of up to four voxels per axis leave the shared-memory leaf tile of the advection
+    (the leaf and a one-voxel halo) and take the leaf-table path: the density is still the
+    oracle's FP32 MacCormack step of its FP16 input to the bit, and the velocity and density
+    equal those of the records kernel (the path of a step with three scalars)."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    vb, dh, vo, do, _ = _mixed(g, dev, dens, vel * 4.0, tol=1e-3)
+    t = oracle.topo(origins)
+    v_in = vb.float().cpu().numpy()
+    assert np.abs(v_in).max() > 3.0  # traces longer than the tile's halo
+    expect_d = torch.from_numpy(t.advect_scalar(v_in, dh.float().cpu().numpy(), 0.1, 10.0)).to(torch.float16)
+    assert torch.equal(do.cpu(), expect_d)
+    hs = [dh, dh.clone(), dh.clone()]
+    outs = [torch.empty_like(dh) for _ in hs]
+    vo3 = torch.empty_like(vb)
+    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-3, max_outer=8, inner_iterations=40, flags=0)
+    torch.cuda.synchronize()
+    g.step_mixed(vb, vo3, hs, outs, desc)
+    torch.cuda.synchronize()
+    assert torch.equal(vo3.cpu(), vo.cpu())
+    assert torch.equal(outs[0].cpu(), do.cpu())
+    g.close()
+
+
 def test_unaligned_arrays_match_aligned(dev, shell):
     """Velocity and scalar arrays that are only element-aligned (2 bytes for BF16/FP16, 4 for
     FP32) take element-wise loads in the advection, divergence and gradient kernels instead of
