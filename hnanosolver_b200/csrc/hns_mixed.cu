@@ -949,31 +949,36 @@ __global__ void __launch_bounds__(kThreads, 4) advect_records_kernel(TopoView t,
 }
 
 // ---- advection from a leaf tile in shared memory --------------------------------------------
-// advect_records_kernel with the leaf's voxel records and a kTileHalo-voxel halo around it
-// unpacked once into shared memory as FP32 (u, v, w, s), a tile of kTileSide^3 cells at local
-// coordinates [-kTileHalo, 8 + kTileHalo). A trace cell whose eight corners lie in the tile is
-// eight shared-memory loads at fixed offsets from one base index (a back trace shorter than a
-// voxel per axis, and a forward trace that ends within a voxel of the start); other cells take
-// the leaf-table path of the records kernel. The clamp's six face neighbours always lie in the
-// tile. Same values, same lerps in the same order, same clamps: the records kernel's results
-// to the bit. One CTA of 256 threads per leaf, two voxels per thread (x and x + 4), four CTAs
-// per SM so that one CTA's tile fill overlaps the others' sampling; cells of missing leaves
-// hold 0, as the records kernel reads outside the domain.
+// The advection of the velocity and at most one scalar (advect_records_kernel's arithmetic)
+// with the leaf's voxels and a kTileHalo-voxel halo around it read once from the BF16 velocity
+// and FP16 scalar arrays into shared memory as FP32 (u, v, w, s), a tile of kTileSide^3 cells
+// at local coordinates [-kTileHalo, 8 + kTileHalo), with no record-packing pass. A trace cell
+// whose eight corners lie in the tile is eight shared-memory loads at fixed offsets from one
+// base index (a back trace shorter than a voxel per axis, and a forward trace that ends within
+// a voxel of the start); other cells take the leaf-table path, reading the arrays. The clamp's
+// six face neighbours always lie in the tile. Same values, same lerps in the same order, same
+// clamps: the records kernel's results to the bit. One CTA of 256 threads per leaf, two voxels
+// per thread (x and x + 4), four CTAs per SM so that one CTA's tile fill overlaps the others'
+// sampling; cells of missing leaves hold 0, as the records kernel reads outside the domain.
 constexpr int kTileHalo = 1;
 constexpr int kTileSide = 8 + 2 * kTileHalo;
 constexpr int kTileCells = kTileSide * kTileSide * kTileSide;
 constexpr int kTileThreads = 256;
 constexpr int kTileFill = (kTileCells + kTileThreads - 1) / kTileThreads;  // cells a thread fills
 
-__device__ __forceinline__ float4 unpack_rec(uint2 r) {
-    return make_float4(__uint_as_float(r.x << 16), __uint_as_float(r.x & 0xFFFF0000u), __uint_as_float(r.y << 16),
-                       __half2float(__ushort_as_half((unsigned short)(r.y >> 16))));
-}
-
 // Trilinear sample of the four channels at (x, y, z) (global voxel units), lerps along z, then
 // y, then x (tri_lerp's order).
+// The FP32 (u, v, w, s) of the voxel at slot s from the BF16 velocity and FP16 scalar arrays
+// (s0 null: s = 0).
+__device__ __forceinline__ float4 voxel4(const __nv_bfloat16* __restrict__ vel, const __half* __restrict__ s0, uint32_t s) {
+    const unsigned short* v = reinterpret_cast<const unsigned short*>(vel) + 3 * (size_t)s;
+    return make_float4(__uint_as_float((uint32_t)__ldg(v) << 16), __uint_as_float((uint32_t)__ldg(v + 1) << 16),
+                       __uint_as_float((uint32_t)__ldg(v + 2) << 16), s0 != nullptr ? __half2float(__ldg(s0 + s)) : 0.f);
+}
+
 __device__ __forceinline__ float4 tile_sample(const float4* __restrict__ tile, const TopoView& t, const LeafNbhd& L,
-                                              const uint2* __restrict__ rec, float x, float y, float z) {
+                                              const __nv_bfloat16* __restrict__ vel, const __half* __restrict__ s0,
+                                              float x, float y, float z) {
     const int i = __float2int_rd(x), j = __float2int_rd(y), k = __float2int_rd(z);
     const float tx = x - (float)i, ty = y - (float)j, tz = z - (float)k;
     const int cx = i - (L.lx << 3) + kTileHalo, cy = j - (L.ly << 3) + kTileHalo, cz = k - (L.lz << 3) + kTileHalo;
@@ -987,7 +992,7 @@ __device__ __forceinline__ float4 tile_sample(const float4* __restrict__ tile, c
         TapsT<int32_t> tp;
         taps_at(tp, t, L, x, y, z);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) c[q] = tp.s[q] < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : unpack_rec(__ldg(rec + (uint32_t)tp.s[q]));
+        for (int q = 0; q < 8; ++q) c[q] = tp.s[q] < 0 ? make_float4(0.f, 0.f, 0.f, 0.f) : voxel4(vel, s0, (uint32_t)tp.s[q]);
     }
     auto tri = [&](float v0, float v1, float v2, float v3, float v4, float v5, float v6, float v7) {
         const float z0 = lerp1(v0, v1, tz), z1 = lerp1(v2, v3, tz), z2 = lerp1(v4, v5, tz), z3 = lerp1(v6, v7, tz);
@@ -999,7 +1004,8 @@ __device__ __forceinline__ float4 tile_sample(const float4* __restrict__ tile, c
                        tri(c[0].w, c[1].w, c[2].w, c[3].w, c[4].w, c[5].w, c[6].w, c[7].w));
 }
 
-__global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t, const uint2* __restrict__ rec,
+__global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t, const __nv_bfloat16* __restrict__ vel,
+                                                                       const __half* __restrict__ s0,
                                                                        __nv_bfloat16* __restrict__ vel_out,
                                                                        __half* __restrict__ s0_out, float sdt) {
     __shared__ float4 tile[kTileCells];
@@ -1008,23 +1014,33 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
     load_nbhd(L, t, leaf);
     __syncthreads();
     // The fill: every load of the thread's cells is issued before any is unpacked.
-    uint2 raw[kTileFill];
+    const unsigned short* vb = reinterpret_cast<const unsigned short*>(vel);
+    const unsigned short* sb = reinterpret_cast<const unsigned short*>(s0);
+    uint32_t raw[kTileFill][4];
 #pragma unroll
     for (int m = 0; m < kTileFill; ++m) {
         const int q = threadIdx.x + m * kTileThreads;
-        raw[m] = make_uint2(0u, 0u);
+        raw[m][0] = raw[m][1] = raw[m][2] = raw[m][3] = 0u;
         if (q < kTileCells) {
             const int lx = q / (kTileSide * kTileSide) - kTileHalo, ly = (q / kTileSide) % kTileSide - kTileHalo,
                       lz = q % kTileSide - kTileHalo;
             const int r = (lx < 0 ? 0 : lx > 7 ? 18 : 9) + (ly < 0 ? 0 : ly > 7 ? 6 : 3) + (lz < 0 ? 0 : lz > 7 ? 2 : 1);
             const int l = L.nb[r];
-            if (l >= 0) raw[m] = __ldg(rec + (((uint32_t)l << 9) | (uint32_t)(((lx & 7) << 6) | ((ly & 7) << 3) | (lz & 7))));
+            if (l >= 0) {
+                const uint32_t sl = ((uint32_t)l << 9) | (uint32_t)(((lx & 7) << 6) | ((ly & 7) << 3) | (lz & 7));
+                raw[m][0] = __ldg(vb + 3 * (size_t)sl);
+                raw[m][1] = __ldg(vb + 3 * (size_t)sl + 1);
+                raw[m][2] = __ldg(vb + 3 * (size_t)sl + 2);
+                if (sb != nullptr) raw[m][3] = __ldg(sb + sl);
+            }
         }
     }
 #pragma unroll
     for (int m = 0; m < kTileFill; ++m) {
         const int q = threadIdx.x + m * kTileThreads;
-        if (q < kTileCells) tile[q] = unpack_rec(raw[m]);
+        if (q < kTileCells)
+            tile[q] = make_float4(__uint_as_float(raw[m][0] << 16), __uint_as_float(raw[m][1] << 16),
+                                  __uint_as_float(raw[m][2] << 16), __half2float(__ushort_as_half((unsigned short)raw[m][3])));
     }
     __syncthreads();
 #pragma unroll 1
@@ -1035,8 +1051,8 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
         const float4* centre = tile + ((a + kTileHalo) * kTileSide + (b + kTileHalo)) * kTileSide + (cz + kTileHalo);
         const float4 o = *centre;
         const float bx = (float)i - o.x * sdt, by = (float)j - o.y * sdt, bz = (float)k - o.z * sdt;
-        const float4 f = tile_sample(tile, t, L, rec, bx, by, bz);
-        const float4 g = tile_sample(tile, t, L, rec, bx + f.x * sdt, by + f.y * sdt, bz + f.z * sdt);
+        const float4 f = tile_sample(tile, t, L, vel, s0, bx, by, bz);
+        const float4 g = tile_sample(tile, t, L, vel, s0, bx + f.x * sdt, by + f.y * sdt, bz + f.z * sdt);
         float3 corr = make_float3(f.x + 0.5f * (o.x - g.x), f.y + 0.5f * (o.y - g.y), f.z + 0.5f * (o.z - g.z));
         float3 mn = make_float3(o.x, o.y, o.z), mx = mn;
         float dmn = o.w, dmx = o.w;
@@ -1072,6 +1088,14 @@ void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void*
     const int64_t n = c.num_voxels();
     const float sdt = dt * (1.0f / c.dx);
     auto aligned8 = [](const void* q) { return ((uintptr_t)q & 7u) == 0; };
+    if (n > 0 && c.topo.num_leaves < (int64_t(1) << 22) && ns <= 1) {
+        // Velocity and at most one scalar: the shared-memory leaf tile, filled from the arrays.
+        advect_tile_kernel<<<(unsigned)c.topo.num_leaves, kTileThreads, 0, c.stream>>>(
+            c.topo.view, static_cast<const __nv_bfloat16*>(vel), ns > 0 ? static_cast<const __half*>(sin[0]) : nullptr,
+            static_cast<__nv_bfloat16*>(vel_out), ns > 0 ? static_cast<__half*>(sout[0]) : nullptr, sdt);
+        HNS_LAUNCHED();
+        return;
+    }
     if (n > 0 && c.topo.num_leaves < (int64_t(1) << 22) && aligned8(vel) && (ns == 0 || aligned8(sin[0])) &&
         ns <= kMaxAdvectFields) {
         // Voxel records: velocity and the first scalar interleaved, then one load per tap.
@@ -1079,14 +1103,6 @@ void launch_advect_mixed(Context& c, const void* vel, void* vel_out, const void*
         pack_records_kernel<<<stream_blocks(c, n), kThreads, 0, c.stream>>>(
             static_cast<const __nv_bfloat16*>(vel), ns > 0 ? static_cast<const __half*>(sin[0]) : nullptr, rec, n);
         HNS_LAUNCHED();
-        if (ns <= 1) {
-            // Velocity and at most one scalar: the shared-memory leaf tile.
-            advect_tile_kernel<<<(unsigned)c.topo.num_leaves, kTileThreads, 0, c.stream>>>(
-                c.topo.view, reinterpret_cast<const uint2*>(rec), static_cast<__nv_bfloat16*>(vel_out),
-                ns > 0 ? static_cast<__half*>(sout[0]) : nullptr, sdt);
-            HNS_LAUNCHED();
-            return;
-        }
         FieldSetT<__half> f{};
         f.count = std::max(0, ns - 1);
         for (int q = 0; q < f.count; ++q) {
