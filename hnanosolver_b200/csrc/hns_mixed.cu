@@ -960,9 +960,16 @@ __global__ void __launch_bounds__(kThreads, 4) advect_records_kernel(TopoView t,
 // clamps: the records kernel's results to the bit. One CTA of 256 threads per leaf, two voxels
 // per thread (x and x + 4), four CTAs per SM so that one CTA's tile fill overlaps the others'
 // sampling; cells of missing leaves hold 0, as the records kernel reads outside the domain.
+//
+// Tile layout: cell (x, y, z) at x * kTileSX + y * kTileSY + z, both strides multiples of 8 cells
+// (16-byte cells): the 8 lanes of a quarter-warp, one z-row of voxels, then read cells whose
+// bank group is set by z alone, so a row whose traces straddle a y or x cell boundary still
+// reads distinct bank groups (an unpadded 10-cell stride measured 38 % bank conflicts).
 constexpr int kTileHalo = 1;
 constexpr int kTileSide = 8 + 2 * kTileHalo;
-constexpr int kTileCells = kTileSide * kTileSide * kTileSide;
+constexpr int kTileSY = 16, kTileSX = kTileSide * kTileSY;
+constexpr int kTileCells = kTileSide * kTileSide * kTileSide;  // cells filled
+constexpr int kTileStore = kTileSide * kTileSX;                // cells allocated (padding included)
 constexpr int kTileThreads = 256;
 constexpr int kTileFill = (kTileCells + kTileThreads - 1) / kTileThreads;  // cells a thread fills
 
@@ -985,9 +992,9 @@ __device__ __forceinline__ float4 tile_sample(const float4* __restrict__ tile, c
     float4 c[8];
     if ((unsigned)cx <= (unsigned)(kTileSide - 2) && (unsigned)cy <= (unsigned)(kTileSide - 2) &&
         (unsigned)cz <= (unsigned)(kTileSide - 2)) {
-        const float4* b = tile + (cx * kTileSide + cy) * kTileSide + cz;
+        const float4* b = tile + cx * kTileSX + cy * kTileSY + cz;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) c[q] = b[(q >> 2) * kTileSide * kTileSide + ((q >> 1) & 1) * kTileSide + (q & 1)];
+        for (int q = 0; q < 8; ++q) c[q] = b[(q >> 2) * kTileSX + ((q >> 1) & 1) * kTileSY + (q & 1)];
     } else {
         TapsT<int32_t> tp;
         taps_at(tp, t, L, x, y, z);
@@ -1008,7 +1015,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
                                                                        const __half* __restrict__ s0,
                                                                        __nv_bfloat16* __restrict__ vel_out,
                                                                        __half* __restrict__ s0_out, float sdt) {
-    __shared__ float4 tile[kTileCells];
+    __shared__ float4 tile[kTileStore];
     __shared__ LeafNbhd L;
     const int64_t leaf = blockIdx.x;
     load_nbhd(L, t, leaf);
@@ -1038,9 +1045,11 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
 #pragma unroll
     for (int m = 0; m < kTileFill; ++m) {
         const int q = threadIdx.x + m * kTileThreads;
-        if (q < kTileCells)
-            tile[q] = make_float4(__uint_as_float(raw[m][0] << 16), __uint_as_float(raw[m][1] << 16),
-                                  __uint_as_float(raw[m][2] << 16), __half2float(__ushort_as_half((unsigned short)raw[m][3])));
+        if (q < kTileCells) {
+            const int at = (q / (kTileSide * kTileSide)) * kTileSX + ((q / kTileSide) % kTileSide) * kTileSY + q % kTileSide;
+            tile[at] = make_float4(__uint_as_float(raw[m][0] << 16), __uint_as_float(raw[m][1] << 16),
+                                   __uint_as_float(raw[m][2] << 16), __half2float(__ushort_as_half((unsigned short)raw[m][3])));
+        }
     }
     __syncthreads();
 #pragma unroll 1
@@ -1048,7 +1057,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
         const int n = (int)threadIdx.x + half * kTileThreads;
         const int a = n >> 6, b = (n >> 3) & 7, cz = n & 7;
         const int i = (L.lx << 3) + a, j = (L.ly << 3) + b, k = (L.lz << 3) + cz;
-        const float4* centre = tile + ((a + kTileHalo) * kTileSide + (b + kTileHalo)) * kTileSide + (cz + kTileHalo);
+        const float4* centre = tile + (a + kTileHalo) * kTileSX + (b + kTileHalo) * kTileSY + (cz + kTileHalo);
         const float4 o = *centre;
         const float bx = (float)i - o.x * sdt, by = (float)j - o.y * sdt, bz = (float)k - o.z * sdt;
         const float4 f = tile_sample(tile, t, L, vel, s0, bx, by, bz);
@@ -1056,7 +1065,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
         float3 corr = make_float3(f.x + 0.5f * (o.x - g.x), f.y + 0.5f * (o.y - g.y), f.z + 0.5f * (o.z - g.z));
         float3 mn = make_float3(o.x, o.y, o.z), mx = mn;
         float dmn = o.w, dmx = o.w;
-        constexpr int kOff[6] = {-kTileSide * kTileSide, kTileSide * kTileSide, -kTileSide, kTileSide, -1, 1};
+        constexpr int kOff[6] = {-kTileSX, kTileSX, -kTileSY, kTileSY, -1, 1};
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
             const float4 e = centre[kOff[q]];

@@ -41,10 +41,13 @@ using namespace relax16;
 // Measured on a 45,198-leaf grid (us per half-sweep): 4 x 2 (256 threads) 18.3, 4 x 3 17.4,
 // 2 x 3 17.1, 1 x 5 16.8, 2 x 4 16.7, 2 x 6 17.4, 1 x 1 22.2: more leaves per thread keep more
 // loads in flight, and small blocks leave a shorter tail to the last wave.
+// Register limit: 80 registers give 6 CTAs per SM; 64 registers (8 per SM) measured 19.8 us with
+// four leaves per thread (spills), 16.2 with three, 17.5 with two: no gain over 6 x 4.
 constexpr int kLeavesPerBlock = 2;   // leaves whose rows one block's threads cover
 constexpr int kLeavesPerThread = 4;  // leaves a thread relaxes its row in
 constexpr int kThreads = 64 * kLeavesPerBlock;
 constexpr int kShortGridCtasPerSm = 6;  // the register limit at 80 registers and 128 threads
+constexpr int kHalfCtasPerSm = 6;       // the half-sweep kernel's launch bound
 
 // nbr27 indices of the six face neighbours: (dx+1)*9 + (dy+1)*3 + (dz+1).
 constexpr int kNbXp = 22, kNbXm = 4, kNbYp = 16, kNbYm = 10, kNbZp = 14, kNbZm = 12;
@@ -193,7 +196,7 @@ __device__ __forceinline__ void relax_group(const int* __restrict__ nb8, const _
 // a launch a thread reads and writes only its own rows of the launch's colour and only reads the
 // other colour, so the passes of a CTA are independent.
 template <bool kZero>
-__global__ void __launch_bounds__(kThreads, kShortGridCtasPerSm) rbgs_split_half_kernel(const int* __restrict__ nb8,
+__global__ void __launch_bounds__(kThreads, kHalfCtasPerSm) rbgs_split_half_kernel(const int* __restrict__ nb8,
                                                                     const __half* __restrict__ rhs, __half* e,
                                                                     int num_leaves, int colour, float omega,
                                                                     const double* __restrict__ check, double tol2,
@@ -603,7 +606,7 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     unsigned blocks = (unsigned)((L + per_block - 1) / per_block);
     // A launch that will most likely return at once (the refinement expected to have converged)
     // uses one wave of CTAs: its cost is then the launch, not the scheduling of every CTA.
-    if (short_grid) blocks = std::min(blocks, (unsigned)(c.sm_count() * kShortGridCtasPerSm));
+    if (short_grid) blocks = std::min(blocks, (unsigned)(c.sm_count() * kHalfCtasPerSm));
     const auto* r = static_cast<const __half*>(rhs);
     auto* x = static_cast<__half*>(e);
     cudaLaunchConfig_t cfg = {};
