@@ -922,7 +922,7 @@ __global__ void __launch_bounds__(kThreads, 4) advect_records_kernel(TopoView t,
     corr.x = fmaxf(mn.x, fminf(corr.x, mx.x));
     corr.y = fmaxf(mn.y, fminf(corr.y, mx.y));
     corr.z = fmaxf(mn.z, fminf(corr.z, mx.z));
-    vstore(vel_out, wide(s), corr);
+    if (vel_out != nullptr) vstore(vel_out, wide(s), corr);
     if (s0_out != nullptr) {
         const float dcorr = pf + 0.5f * (o.d - pb);
         dmn = fminf(dmn, pf);
@@ -1080,7 +1080,7 @@ __global__ void __launch_bounds__(kTileThreads, 4) advect_tile_kernel(TopoView t
         corr.y = fmaxf(mn.y, fminf(corr.y, mx.y));
         corr.z = fmaxf(mn.z, fminf(corr.z, mx.z));
         const int64_t s = (leaf << 9) + n;
-        vstore(vel_out, s, corr);
+        if (vel_out != nullptr) vstore(vel_out, s, corr);
         if (s0_out != nullptr) {
             const float dcorr = f.w + 0.5f * (o.w - g.w);
             dmn = fminf(dmn, f.w);
@@ -1205,15 +1205,14 @@ hns_status mixed_info(Context& c, const RefinePlan& plan, const hns_mixed_desc& 
     return HNS_OK;
 }
 
-// after_advect, when given, runs on the host once the advection is enqueued (the scalars'
-// outputs are final from then on; the velocity is not).
+// The mixed step on device arrays: advection (velocity and the ns scalars), divergence, the
+// refined solve, the gradient.
 RefinePlan mixed_step_device(Context& c, const void* vel_in, void* vel_out, const void* const* sin, void* const* sout, int ns,
-                             const hns_mixed_desc& d, const std::function<void()>& after_advect = {}) {
+                             const hns_mixed_desc& d) {
     const size_t n = (size_t)c.num_voxels();
     c.phase_begin(HNS_PHASE_ADVECT);
     launch_advect_mixed(c, vel_in, vel_out, sin, sout, ns, d.dt);
     c.phase_end();
-    if (after_advect) after_advect();
     float* div = c.scratch_f32("project_div", n);
     double* p = reinterpret_cast<double*>(c.scratch_f32("refine_p", 2 * n));
     c.phase_begin(HNS_PHASE_DIVERGENCE);
@@ -1277,30 +1276,30 @@ HNS_API hns_status hns_step_mixed_host(hns_ctx* ctx, float* vel, float* const* s
         DeviceGuard dg(c->device);
         const size_t n = (size_t)c->num_voxels();
         // Host data is FP32 (the reference's GridIndexedData); it is staged in FP32, converted
-        // to BF16/FP16 on the device, stepped, and converted back.
+        // to BF16/FP16 on the device, stepped, and converted back. The host link is the bound:
+        // only the velocity's upload and download are on the critical path. The scalars are
+        // uploaded, advected along the incoming velocity, converted and downloaded on the
+        // auxiliary stream while the main stream projects the velocity (the same kernels and
+        // values as the device form, which advects them together with the velocity).
+        for (int q = 0; q < nscalars; ++q)
+            if (!scalars[q]) fail(HNS_ERR_INVALID_ARG, "null scalar field");
         float* stage = c->scratch_f32("mixed_host_stage", 3 * n);
         void* v_in = c->scratch_f32("mixed_vel_in", (3 * n + 1) / 2);
         void* v_out = c->scratch_f32("mixed_vel_out", (3 * n + 1) / 2);
         std::vector<const void*> sin((size_t)nscalars);
         std::vector<void*> sout((size_t)nscalars);
-        HNS_CUDA(cudaMemcpyAsync(stage, vel, 3 * n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-        convert_array(*c, stage, HNS_DTYPE_F32, v_in, HNS_DTYPE_BF16, (int64_t)(3 * n));
         for (int q = 0; q < nscalars; ++q) {
-            if (!scalars[q]) fail(HNS_ERR_INVALID_ARG, "null scalar field");
-            void* a = c->scratch_f32("mixed_scalar_in_" + std::to_string(q), (n + 1) / 2);
+            sin[q] = c->scratch_f32("mixed_scalar_in_" + std::to_string(q), (n + 1) / 2);
             sout[q] = c->scratch_f32("mixed_scalar_out_" + std::to_string(q), (n + 1) / 2);
-            sin[q] = a;
-            HNS_CUDA(cudaMemcpyAsync(stage, scalars[q], n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-            convert_array(*c, stage, HNS_DTYPE_F32, a, HNS_DTYPE_F16, (int64_t)n);
         }
-        // The advected scalars are final before the pressure solve: they are converted and
-        // downloaded on the auxiliary stream while the main stream projects the velocity.
         float* stage_aux = nscalars > 0 ? c->scratch_f32("mixed_host_stage_aux", n) : nullptr;
         if (nscalars > 0) c->ensure_aux();
-        auto download_scalars = [&] {
-            HNS_CUDA(cudaEventRecord(c->aux_ready, c->stream));
+        HNS_CUDA(cudaMemcpyAsync(stage, vel, 3 * n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        convert_array(*c, stage, HNS_DTYPE_F32, v_in, HNS_DTYPE_BF16, (int64_t)(3 * n));
+        if (nscalars > 0) {
+            HNS_CUDA(cudaEventRecord(c->aux_ready, c->stream));  // v_in is converted
             HNS_CUDA(cudaStreamWaitEvent(c->aux_stream, c->aux_ready, 0));
-            // The conversions below launch on the auxiliary stream; the main one is restored on exit.
+            // The launches below go to the auxiliary stream; the main one is restored on exit.
             struct StreamSwap {
                 Context& ctx;
                 cudaStream_t saved;
@@ -1308,13 +1307,16 @@ HNS_API hns_status hns_step_mixed_host(hns_ctx* ctx, float* vel, float* const* s
             } swap{*c, c->stream};
             c->stream = c->aux_stream;
             for (int q = 0; q < nscalars; ++q) {
+                HNS_CUDA(cudaMemcpyAsync(stage_aux, scalars[q], n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+                convert_array(*c, stage_aux, HNS_DTYPE_F32, const_cast<void*>(sin[q]), HNS_DTYPE_F16, (int64_t)n);
+            }
+            launch_advect_mixed(*c, v_in, nullptr, sin.data(), sout.data(), nscalars, desc->dt);
+            for (int q = 0; q < nscalars; ++q) {
                 convert_array(*c, sout[q], HNS_DTYPE_F16, stage_aux, HNS_DTYPE_F32, (int64_t)n);
                 HNS_CUDA(cudaMemcpyAsync(scalars[q], stage_aux, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
             }
-        };
-        const RefinePlan plan = mixed_step_device(*c, v_in, v_out, sin.data(), sout.data(), nscalars, *desc,
-                                                  nscalars > 0 ? std::function<void()>(download_scalars)
-                                                               : std::function<void()>());
+        }
+        const RefinePlan plan = mixed_step_device(*c, v_in, v_out, nullptr, nullptr, 0, *desc);
         convert_array(*c, v_out, HNS_DTYPE_BF16, stage, HNS_DTYPE_F32, (int64_t)(3 * n));
         HNS_CUDA(cudaMemcpyAsync(vel, stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
         if (nscalars > 0) HNS_CUDA(cudaStreamSynchronize(c->aux_stream));
