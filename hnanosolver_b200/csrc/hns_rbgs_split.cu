@@ -42,7 +42,10 @@ using namespace relax16;
 // 2 x 3 17.1, 1 x 5 16.8, 2 x 4 16.7, 2 x 6 17.4, 1 x 1 22.2: more leaves per thread keep more
 // loads in flight, and small blocks leave a shorter tail to the last wave.
 // Register limit: 80 registers give 6 CTAs per SM; 64 registers (8 per SM) measured 19.8 us with
-// four leaves per thread (spills), 16.2 with three, 17.5 with two: no gain over 6 x 4.
+// four leaves per thread (spills), 16.2 with three, 17.5 with two: no gain over 6 x 4 (16.1).
+// A thread per row quad (the four same-parity rows at one x: 16-byte loads, 15 loads for 16
+// updates instead of 36, same values) measured 18.6 us at 6 CTAs per SM and 16.8 at 8: fewer
+// instructions, but fewer bytes in flight, and the kernel is bound by memory latency.
 constexpr int kLeavesPerBlock = 2;   // leaves whose rows one block's threads cover
 constexpr int kLeavesPerThread = 4;  // leaves a thread relaxes its row in
 constexpr int kThreads = 64 * kLeavesPerBlock;
