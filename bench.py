@@ -535,11 +535,14 @@ def ours(args, wl):
         dh = [torch.from_numpy(dens).to(dev).to(torch.float16).contiguous(), torch.empty(n, dtype=torch.float16, device=dev)]
 
         def mdesc(outer):
+            if args.multigrid:
+                return hl.MixedDesc(dt=wl["dt"], omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
+                                    inner_iterations=args.cycles, flags=hl.SOLVE_MULTIGRID)
             return hl.MixedDesc(dt=wl["dt"], omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
                                 inner_iterations=wl["inner"], flags=0)
 
         info = solve_once(lambda: g.step_mixed(vb[0], vb[1], [dh[0]], [dh[1]], mdesc(16), info=True), g.last_refine)
-        outer = max(1, info.iterations // wl["inner"]) + 1
+        outer = max(1, info.iterations // (args.cycles if args.multigrid else wl["inner"])) + 1
         st = mdesc(outer)
         ms_state = [0]
 
@@ -1188,6 +1191,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout measured beside the step")
     ap.add_argument("--no-field-error", action="store_true",
                     help="skip the FP64 check of the last timed step's fields (shell512 and plume256 steps)")
+    ap.add_argument("--multigrid", action="store_true",
+                    help="mixed SOP step: V-cycles (HNS_SOLVE_MULTIGRID) as the inner solve of the refinement")
+    ap.add_argument("--cycles", type=int, default=2, help="V-cycles per outer refinement step with --multigrid")
     ap.add_argument("--split-solve", choices=["persistent", "per-colour"], default="per-colour",
                     help="launch form of the colour-split red-black solves (same results to the bit)")
     ap.add_argument("--no-fp32-comparison", action="store_true",

@@ -280,6 +280,8 @@ void copy_h2d(Context& c, void* dev, const void* host, size_t bytes);
 void copy_d2h(Context& c, void* host, const void* dev, size_t bytes);
 // One multigrid V-cycle (hns_multigrid.cu): u0 (n FP32) ~ A^-1 b0 for the unit-spacing system.
 void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, double tol2);
+// One V-cycle of the FP16 inner solve on the colour-split layout (e in place; e_zero: e = 0 before).
+void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_zero, const double* check, double tol2);
 // The FP16 inner solve on colour-split leaves (hns_rbgs_split.cu): the face-neighbour table
 // (8 ints per leaf, missing neighbours = the zero leaf L) and one in-place half-sweep (colour 0
 // red, 1 black). e holds L + 1 leaves, the last all zeros. e_zero: e = 0 before this red

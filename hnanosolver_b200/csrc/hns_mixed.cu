@@ -734,7 +734,11 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         const double* chk = plan.slots + 2 * k;
         const bool spare = forecast > 0 && k >= forecast;
         const unsigned gk = spare ? std::min(g, (unsigned)(c.sm_count() * 4)) : g;
-        if (flags & HNS_SOLVE_MULTIGRID) {
+        // Multigrid on the FP16 colour-split layout: `inner` V-cycles per outer iteration, the
+        // colour-split half-sweep as the fine smoother (mg16_vcycle); other layouts and the FP32
+        // inner solve take the FP32 V-cycle in slot order below.
+        const bool mg16 = (flags & HNS_SOLVE_MULTIGRID) && sizeof(TI) == 2 && layout == HNS_INNER_SPLIT;
+        if ((flags & HNS_SOLVE_MULTIGRID) && !mg16) {
             // One V-cycle on the scaled residual in FP32 (slot order), then p += s e.
             float* rm = c.scratch_f32("mg_rhat", (size_t)n);
             float* em = c.scratch_f32("mg_e", (size_t)n);
@@ -769,8 +773,11 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         // The persistent form: the whole inner solve in one launch. An outer iteration past the
         // forecast takes it whatever the option: it most likely returns at once, and one launch
         // then costs a few microseconds where 2 * inner returning half-sweeps cost 2.3 us each.
-        const bool persistent = layout == HNS_INNER_SPLIT && (c.split_solve == HNS_SPLIT_PERSISTENT || spare);
-        if (persistent) {
+        const bool persistent = !mg16 && layout == HNS_INNER_SPLIT && (c.split_solve == HNS_SPLIT_PERSISTENT || spare);
+        if (mg16) {
+            for (int cyc = 0; cyc < plan.inner; ++cyc) mg16_vcycle(c, nb8, rhat, e_split, cyc == 0, chk, tol2);
+            src = e_split;
+        } else if (persistent) {
             if constexpr (sizeof(TI) == 2)
                 launch_rbgs_split_solve(c, nb8, rhat, e_split, 2 * plan.inner, true, omega, chk, tol2);
             else
@@ -778,7 +785,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                                             2 * plan.inner, true, omega, 1.0f, chk, tol2);
             src = e_split;
         }
-        for (int it = 0; it < (persistent ? 0 : plan.inner); ++it) {
+        for (int it = 0; it < (persistent || mg16 ? 0 : plan.inner); ++it) {
             TI* dst = e[it & 1];
             if constexpr (sizeof(TI) == 2) {
                 if (layout == HNS_INNER_SPLIT) {

@@ -15,6 +15,7 @@
 // FP32 throughout; the FP64 outer refinement around it measures the residual exactly, so the
 // cycle only has to reduce the error. Every kernel returns at once when the refinement has
 // converged.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -151,6 +152,225 @@ __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(TopoView t, const 
 
 unsigned blocks(int64_t cells) { return (unsigned)((cells + kThreads - 1) / kThreads); }
 
+// ---- V-cycle of the FP16 inner solve (colour-split fine level) ------------------------------
+// Coarse levels as above (2^LG cells per leaf side, cell (x, y, z) of leaf l at
+// (l << 3 LG) + ((x << LG) + y << LG) + z, FP32), with the operator corrected at the walls: the
+// fine system's p = 0 sits at the ghost cell's centre, half a fine cell past the wall, and a
+// coarse ghost value of 0 would put it half a coarse cell past it. The coarse ghost value is
+// instead extrapolated linearly through that point, -gamma u with gamma = (2^l - 1) / (2^l + 1)
+// at level l, which adds gamma to the diagonal for each missing face neighbour. A numpy model of
+// the cycle on a 160^3 shell gives 0.16 per cycle with the correction against 0.54-1.1 without.
+// Face neighbours come from the colour-split face table nb8 ({+x, -x, +y, -y, +z, -z, the leaf,
+// 0}, a missing leaf = num_leaves).
+
+template <int LG>
+struct LevelCell {
+    int leaf, x, y, z;
+};
+
+template <int LG>
+__device__ __forceinline__ LevelCell<LG> level_cell(int64_t q) {
+    constexpr int m = (1 << LG) - 1;
+    LevelCell<LG> c;
+    c.leaf = (int)(q >> (3 * LG));
+    c.x = (int)(q >> (2 * LG)) & m;
+    c.y = (int)(q >> LG) & m;
+    c.z = (int)q & m;
+    return c;
+}
+
+// Sum of the face neighbours of cell (x, y, z) of `leaf` at level LG present in the domain, and
+// the number missing.
+template <int LG>
+__device__ __forceinline__ float level_nsum(const int4* __restrict__ nb8, const float* __restrict__ u, int leaf, int x,
+                                            int y, int z, int num_leaves, int& missing) {
+    constexpr int s = 1 << LG, m = s - 1;
+    const int4 f0 = __ldg(nb8 + 2 * leaf), f1 = __ldg(nb8 + 2 * leaf + 1);
+    auto at = [&](int l, int a, int b, int c) -> float {
+        if (l >= num_leaves) {
+            ++missing;
+            return 0.f;
+        }
+        return u[((int64_t)l << (3 * LG)) + (((a << LG) + b) << LG) + c];
+    };
+    missing = 0;
+    float sum = at(x < m ? leaf : f0.x, (x + 1) & m, y, z);
+    sum += at(x > 0 ? leaf : f0.y, (x - 1) & m, y, z);
+    sum += at(y < m ? leaf : f0.z, x, (y + 1) & m, z);
+    sum += at(y > 0 ? leaf : f0.w, x, (y - 1) & m, z);
+    sum += at(z < m ? leaf : f1.x, x, y, (z + 1) & m);
+    sum += at(z > 0 ? leaf : f1.y, x, y, (z - 1) & m);
+    return sum;
+}
+
+// One colour of SOR at level LG: u += omega ((sum - h2 b) / (6 + gamma missing) - u). Colour:
+// the global cell parity, which for LG >= 1 is that of the local coordinates (leaf origins are
+// even in cells) and for LG = 0 that of the leaf.
+template <int LG>
+__global__ void __launch_bounds__(kThreads) mgl_smooth_kernel(TopoView t, const int4* __restrict__ nb8, float* u,
+                                                              const float* __restrict__ b, int colour, float omega,
+                                                              float h2, float gamma, const double* __restrict__ check,
+                                                              double tol2) {
+    if (done(check, tol2)) return;
+    const int num_leaves = (int)t.num_leaves;
+    const int64_t t0 = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    LevelCell<LG> c;
+    int64_t q;
+    if constexpr (LG == 0) {
+        // One cell per leaf: the leaf's parity decides.
+        if (t0 >= num_leaves) return;
+        q = t0;
+        c = level_cell<0>(q);
+        const int4 o = t.origin[c.leaf];
+        if ((((o.x + o.y + o.z) >> 3) & 1) != colour) return;
+    } else {
+        // One thread per cell of the colour: the z pair (2k, 2k + 1) of row (x, y) holds one.
+        constexpr int m = (1 << LG) - 1, hz = (1 << (LG - 1)) - 1;
+        if (t0 >= ((int64_t)num_leaves << (3 * LG - 1))) return;
+        c.leaf = (int)(t0 >> (3 * LG - 1));
+        c.x = (int)(t0 >> (2 * LG - 1)) & m;
+        c.y = (int)(t0 >> (LG - 1)) & m;
+        c.z = 2 * ((int)t0 & hz) + ((c.x + c.y + colour) & 1);
+        q = ((int64_t)c.leaf << (3 * LG)) + (((c.x << LG) + c.y) << LG) + c.z;
+    }
+    int missing;
+    const float sum = level_nsum<LG>(nb8, u, c.leaf, c.x, c.y, c.z, num_leaves, missing);
+    const float uq = u[q];
+    u[q] = uq + omega * ((sum - h2 * __ldg(b + q)) / (6.0f + gamma * (float)missing) - uq);
+}
+
+// bc (level LG - 1) = the mean of the residuals b - (sum - (6 + gamma missing) u) / h2 of each
+// coarse cell's 8 children at level LG.
+template <int LG>
+__global__ void __launch_bounds__(kThreads) mgl_restrict_kernel(const int4* __restrict__ nb8, const float* __restrict__ u,
+                                                                const float* __restrict__ b, float* __restrict__ bc,
+                                                                int num_leaves, float inv_h2, float gamma,
+                                                                const double* __restrict__ check, double tol2) {
+    if (done(check, tol2)) return;
+    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (q >= ((int64_t)num_leaves << (3 * (LG - 1)))) return;
+    const LevelCell<LG - 1> cc = level_cell<LG - 1>(q);
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int x = 2 * cc.x + (k >> 2), y = 2 * cc.y + ((k >> 1) & 1), z = 2 * cc.z + (k & 1);
+        const int64_t f = ((int64_t)cc.leaf << (3 * LG)) + (((x << LG) + y) << LG) + z;
+        int missing;
+        const float ns = level_nsum<LG>(nb8, u, cc.leaf, x, y, z, num_leaves, missing);
+        sum += __ldg(b + f) - (ns - (6.0f + gamma * (float)missing) * u[f]) * inv_h2;
+    }
+    bc[q] = 0.125f * sum;
+}
+
+// Prolongation, one thread per coarse cell (level LC, 2^LC cells per leaf side): the coarse
+// correction at the cell and its 26 neighbours (across faces, edges and corners of the leaf from
+// the 27-neighbour table, 0 outside the domain), then each of the cell's 8 children at level
+// LC + 1 takes the trilinear interpolation between cell centres: along each axis 3/4 of the
+// parent and 1/4 of the parent's neighbour on the child's side.
+template <int LC>
+__device__ __forceinline__ void gather27(const TopoView& t, const float* __restrict__ uc, int leaf, int X, int Y, int Z,
+                                         float v[27]) {
+    constexpr int sc = 1 << LC;
+#pragma unroll
+    for (int k = 0; k < 27; ++k) {
+        int cx = X + k / 9 - 1, cy = Y + (k / 3) % 3 - 1, cz = Z + k % 3 - 1;
+        const int ox = cx < 0 ? -1 : (cx >= sc ? 1 : 0), oy = cy < 0 ? -1 : (cy >= sc ? 1 : 0),
+                  oz = cz < 0 ? -1 : (cz >= sc ? 1 : 0);
+        int l = leaf;
+        if (ox | oy | oz) l = __ldg(t.nbr27 + (int64_t)leaf * 27 + (ox + 1) * 9 + (oy + 1) * 3 + (oz + 1));
+        cx -= ox * sc, cy -= oy * sc, cz -= oz * sc;
+        v[k] = l < 0 ? 0.f : __ldg(uc + ((int64_t)l << (3 * LC)) + (((cx << LC) + cy) << LC) + cz);
+    }
+}
+
+// The interpolated value of child (i, j, k) (each 0 or 1) from the gathered neighbourhood.
+__device__ __forceinline__ float interp8(const float v[27], int i, int j, int k) {
+    const int sx = i ? 1 : -1, sy = j ? 1 : -1, sz = k ? 1 : -1;
+    float sum = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int a = q >> 2, bb = (q >> 1) & 1, e = q & 1;
+        const float w = (a ? 0.25f : 0.75f) * (bb ? 0.25f : 0.75f) * (e ? 0.25f : 0.75f);
+        sum += w * v[(1 + a * sx) * 9 + (1 + bb * sy) * 3 + (1 + e * sz)];
+    }
+    return sum;
+}
+
+// Position of local voxel (x, y, z) of leaf l in the colour-split FP16 layout of the inner solve
+// (a leaf's colour-0 values, then its colour-1 values; row (x, y) at R = 32 ((x + y) & 1) + 4 x +
+// (y >> 1) within a colour, entry z >> 1 of the row).
+__device__ __forceinline__ uint32_t split_at(int l, int x, int y, int z) {
+    return ((uint32_t)l << 9) | ((uint32_t)((x + y + z) & 1) << 8) |
+           (uint32_t)(4 * (32 * ((x + y) & 1) + 4 * x + (y >> 1)) + (z >> 1));
+}
+
+__device__ __forceinline__ float h16(const __half* p, uint32_t i) { return __half2float(p[i]); }
+
+// Fine level of the FP16 cycle: b1 (4^3 cells per leaf) = the mean of the residuals
+// r^ - (sum - 6 e) (unit spacing; a missing leaf is the zero leaf past the last one, p = 0 outside
+// the domain) of each level-1 cell's 8 voxels, e and r^ in the colour-split layout.
+__global__ void __launch_bounds__(kThreads) mg16_restrict_kernel(const int4* __restrict__ nb8, const __half* e,
+                                                                 const __half* __restrict__ rhat, float* __restrict__ b1,
+                                                                 int num_leaves, const double* __restrict__ check,
+                                                                 double tol2) {
+    if (done(check, tol2)) return;
+    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (q >= ((int64_t)num_leaves << 6)) return;
+    const LevelCell<2> cc = level_cell<2>(q);
+    const int4 f0 = __ldg(nb8 + 2 * cc.leaf), f1 = __ldg(nb8 + 2 * cc.leaf + 1);
+    float sum = 0.f;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int x = 2 * cc.x + (k >> 2), y = 2 * cc.y + ((k >> 1) & 1), z = 2 * cc.z + (k & 1);
+        float ns = h16(e, split_at(x < 7 ? cc.leaf : f0.x, (x + 1) & 7, y, z));
+        ns += h16(e, split_at(x > 0 ? cc.leaf : f0.y, (x - 1) & 7, y, z));
+        ns += h16(e, split_at(y < 7 ? cc.leaf : f0.z, x, (y + 1) & 7, z));
+        ns += h16(e, split_at(y > 0 ? cc.leaf : f0.w, x, (y - 1) & 7, z));
+        ns += h16(e, split_at(z < 7 ? cc.leaf : f1.x, x, y, (z + 1) & 7));
+        ns += h16(e, split_at(z > 0 ? cc.leaf : f1.y, x, y, (z - 1) & 7));
+        const uint32_t o = split_at(cc.leaf, x, y, z);
+        sum += __half2float(rhat[o]) - (ns - 6.0f * h16(e, o));
+    }
+    b1[q] = 0.125f * sum;
+}
+
+// e (FP16, colour-split) += the level-1 correction interpolated trilinearly, one rounding; one
+// thread per level-1 cell.
+__global__ void __launch_bounds__(kThreads) mg16_prolong_kernel(TopoView t, const float* __restrict__ u1, __half* e,
+                                                                const double* __restrict__ check, double tol2) {
+    if (done(check, tol2)) return;
+    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (q >= (t.num_leaves << 6)) return;
+    const LevelCell<2> c = level_cell<2>(q);
+    float v[27];
+    gather27<2>(t, u1, c.leaf, c.x, c.y, c.z, v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int i = k >> 2, j = (k >> 1) & 1, l = k & 1;
+        const uint32_t o = split_at(c.leaf, 2 * c.x + i, 2 * c.y + j, 2 * c.z + l);
+        e[o] = __float2half_rn(__half2float(e[o]) + interp8(v, i, j, l));
+    }
+}
+
+// u (level LG) += the correction uc (level LG - 1), one thread per coarse cell.
+template <int LG>
+__global__ void __launch_bounds__(kThreads) mgl_prolong_kernel(TopoView t, const float* __restrict__ uc,
+                                                               float* __restrict__ u, const double* __restrict__ check,
+                                                               double tol2) {
+    if (done(check, tol2)) return;
+    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (q >= (t.num_leaves << (3 * (LG - 1)))) return;
+    const LevelCell<LG - 1> c = level_cell<LG - 1>(q);
+    float v[27];
+    gather27<LG - 1>(t, uc, c.leaf, c.x, c.y, c.z, v);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int i = k >> 2, j = (k >> 1) & 1, l = k & 1;
+        const int64_t f = ((int64_t)c.leaf << (3 * LG)) + ((((2 * c.x + i) << LG) + 2 * c.y + j) << LG) + 2 * c.z + l;
+        u[f] += interp8(v, i, j, l);
+    }
+}
+
 }  // namespace
 
 // One V-cycle on rhs b0 (n FP32 values, slot order) into u0 (n FP32, overwritten; starts at 0).
@@ -202,6 +422,81 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
         HNS_LAUNCHED();
         smooth(l, kPostSmooth, 1.0f);
     }
+}
+
+// One V-cycle of the FP16 inner solve L e = r^ (unit spacing) on the colour-split layout: e is
+// refined in place (e_zero: e = 0 before the cycle). Fine level: kMgNu red-black iterations of
+// the colour-split half-sweep at omega = 1 before and after the coarse correction; levels with
+// 4, 2 and 1 cells per leaf side in FP32 with the wall-corrected operator, kMgNu iterations
+// before and after at the first two, kMgCoarseIters SOR iterations at the last.
+namespace {
+// Coarsest sweeps: on shell512 (about six leaves thick) 10 keep the cycle at about 0.15; 2 (which
+// suffice on a thinner shell) doubled the cycles.
+constexpr int kMgNu = 2, kMgCoarseIters = 10;
+constexpr float kMgCoarseOmega = 1.5f;
+
+template <int LG>
+void smooth_level(Context& c, const int4* nb8, float* u, const float* b, int iters, float omega, int l,
+                  const double* check, double tol2) {
+    const float h2 = (float)(1 << (2 * l)), gamma = (float)((1 << l) - 1) / (float)((1 << l) + 1);
+    int64_t threads = c.topo.num_leaves;  // LG = 0: one thread per leaf
+    if constexpr (LG > 0) threads <<= 3 * LG - 1;  // one thread per cell of the colour
+    const unsigned g = blocks(threads);
+    for (int it = 0; it < iters; ++it)
+        for (int colour = 0; colour < 2; ++colour) {
+            mgl_smooth_kernel<LG><<<g, kThreads, 0, c.stream>>>(c.topo.view, nb8, u, b, colour, omega, h2, gamma, check, tol2);
+            HNS_LAUNCHED();
+        }
+}
+}  // namespace
+
+void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_zero, const double* check, double tol2) {
+    const int64_t L = c.topo.num_leaves;
+    if (L == 0) return;
+    const TopoView t = c.topo.view;
+    const auto* f8 = reinterpret_cast<const int4*>(nb8);
+    const auto* r = static_cast<const __half*>(rhat);
+    auto* eh = static_cast<__half*>(e);
+    float* u[4] = {nullptr, nullptr, nullptr, nullptr};
+    float* b[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int l = 1; l < 4; ++l) {
+        const size_t cells = (size_t)L << (3 * (3 - l));
+        u[l] = c.scratch_f32("mg16_u" + std::to_string(l), cells);
+        b[l] = c.scratch_f32("mg16_b" + std::to_string(l), cells);
+    }
+    auto fine = [&](bool zero_first) {
+        for (int it = 0; it < kMgNu; ++it) {
+            launch_rbgs_split_half(c, nb8, rhat, e, 0, zero_first && it == 0, 1.0f, check, tol2, false);
+            launch_rbgs_split_half(c, nb8, rhat, e, 1, false, 1.0f, check, tol2, false);
+        }
+    };
+    auto zero = [&](int l) {
+        HNS_CUDA(cudaMemsetAsync(u[l], 0, sizeof(float) * ((size_t)L << (3 * (3 - l))), c.stream));
+    };
+    fine(e_zero);
+    mg16_restrict_kernel<<<blocks(L << 6), kThreads, 0, c.stream>>>(f8, eh, r, b[1], (int)L, check, tol2);
+    HNS_LAUNCHED();
+    zero(1);
+    smooth_level<2>(c, f8, u[1], b[1], kMgNu, 1.0f, 1, check, tol2);
+    mgl_restrict_kernel<2><<<blocks(L << 3), kThreads, 0, c.stream>>>(f8, u[1], b[1], b[2], (int)L, 0.25f, 1.0f / 3.0f,
+                                                                       check, tol2);
+    HNS_LAUNCHED();
+    zero(2);
+    smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, check, tol2);
+    mgl_restrict_kernel<1><<<blocks(L), kThreads, 0, c.stream>>>(f8, u[2], b[2], b[3], (int)L, 1.0f / 16.0f, 0.6f, check,
+                                                                  tol2);
+    HNS_LAUNCHED();
+    zero(3);
+    smooth_level<0>(c, f8, u[3], b[3], kMgCoarseIters, kMgCoarseOmega, 3, check, tol2);
+    mgl_prolong_kernel<1><<<blocks(L), kThreads, 0, c.stream>>>(t, u[3], u[2], check, tol2);
+    HNS_LAUNCHED();
+    smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, check, tol2);
+    mgl_prolong_kernel<2><<<blocks(L << 3), kThreads, 0, c.stream>>>(t, u[2], u[1], check, tol2);
+    HNS_LAUNCHED();
+    smooth_level<2>(c, f8, u[1], b[1], kMgNu, 1.0f, 1, check, tol2);
+    mg16_prolong_kernel<<<blocks(L << 6), kThreads, 0, c.stream>>>(t, u[1], eh, check, tol2);
+    HNS_LAUNCHED();
+    fine(false);
 }
 
 }  // namespace hns

@@ -174,11 +174,15 @@ HNS_API hns_status hns_project_static(hns_ctx* ctx, float* vel, int iterations, 
                                inner solves (max_outer x inner_iterations) instead of one plain
                                FP32 solve; removes the FP32 rounding floor of the residual */
 #define HNS_SOLVE_MULTIGRID 8u /* with refinement (HNS_SOLVE_REFINE in hns_step_desc.flags; always in
-                                    hns_mixed_desc.flags): each outer step's inner solve is one geometric
-                                    multigrid V-cycle (FP32, levels of 8, 4, 2 and 1 cells per leaf side)
-                                    instead of inner_iterations red-black iterations. The reference
-                                    declares this preconditioner (src/Cuda/Kernels.cuh:52-60) but does not
-                                    implement it. */
+                                    hns_mixed_desc.flags): each outer step's inner solve is geometric
+                                    multigrid (levels of 8, 4, 2 and 1 cells per leaf side) instead of
+                                    inner_iterations red-black iterations. The FP16 colour-split inner
+                                    solve (hns_mixed_desc, the default layout) runs inner_iterations
+                                    V-cycles per outer step with the colour-split red-black half-sweep
+                                    as the fine smoother and FP32 coarse levels whose operator is
+                                    corrected at the walls; the FP32 and other FP16 inner solves run
+                                    one FP32 V-cycle. The reference declares this preconditioner
+                                    (src/Cuda/Kernels.cuh:52-60) but does not implement it. */
 
 typedef struct hns_step_desc {
     float dt;
@@ -240,7 +244,7 @@ typedef struct hns_mixed_desc {
     float omega;          /* inner SOR factor; <= 0 selects 1.9 */
     double tolerance;     /* target ||b - L p|| / ||b|| in FP64 (> 0) */
     int max_outer;        /* outer refinement cap */
-    int inner_iterations; /* red-black iterations per outer refinement */
+    int inner_iterations; /* red-black iterations per outer refinement (V-cycles with HNS_SOLVE_MULTIGRID) */
     unsigned flags;       /* 0, or HNS_SOLVE_MULTIGRID */
 } hns_mixed_desc;
 

@@ -339,8 +339,8 @@ def test_outer_forecast_short_grids_bit_exact(dev, shell):
 
 @pytest.mark.parametrize("grid", ["spheres", "box"])
 def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
-    """HNS_SOLVE_MULTIGRID: one V-cycle per outer step in place of the red-black iterations. The
-    FP64 residual of the returned pressure, recomputed by the oracle, is within the tolerance,
+    """HNS_SOLVE_MULTIGRID: V-cycles (two per outer step for the mixed step, one for the FP32
+    refined step) in place of the red-black iterations. The FP64 residual of the returned pressure, recomputed by the oracle, is within the tolerance,
     and the projected velocity agrees with the red-black refinement's to the accuracy that a
     1e-5 relative residual allows; the FP32 refined step takes the flag too."""
     from hnanosolver_b200 import lib as hl
@@ -356,7 +356,8 @@ def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
     outs = {}
     for flags in (0, hl.SOLVE_MULTIGRID):
         vo, do = torch.empty_like(vb), torch.empty_like(dh)
-        desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=40, inner_iterations=30, flags=flags)
+        desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=40, inner_iterations=2 if flags else 30,
+                            flags=flags)
         torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
         info = g.step_mixed(vb, vo, [dh], [do], desc, info=True)
         assert info.residual <= 1e-5
