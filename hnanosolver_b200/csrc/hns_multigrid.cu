@@ -181,7 +181,7 @@ __device__ __forceinline__ LevelCell<LG> level_cell(int64_t q) {
 
 // Sum of the face neighbours of cell (x, y, z) of `leaf` at level LG present in the domain, and
 // the number missing.
-template <int LG>
+template <int LG, bool kRead = true>
 __device__ __forceinline__ float level_nsum(const int4* __restrict__ nb8, const float* __restrict__ u, int leaf, int x,
                                             int y, int z, int num_leaves, int& missing) {
     constexpr int s = 1 << LG, m = s - 1;
@@ -191,7 +191,7 @@ __device__ __forceinline__ float level_nsum(const int4* __restrict__ nb8, const 
             ++missing;
             return 0.f;
         }
-        return u[((int64_t)l << (3 * LG)) + (((a << LG) + b) << LG) + c];
+        return kRead ? u[((int64_t)l << (3 * LG)) + (((a << LG) + b) << LG) + c] : 0.f;
     };
     missing = 0;
     float sum = at(x < m ? leaf : f0.x, (x + 1) & m, y, z);
@@ -208,32 +208,53 @@ __device__ __forceinline__ float level_nsum(const int4* __restrict__ nb8, const 
 // even in cells) and for LG = 0 that of the leaf.
 template <int LG>
 __global__ void __launch_bounds__(kThreads) mgl_smooth_kernel(TopoView t, const int4* __restrict__ nb8, float* u,
-                                                              const float* __restrict__ b, int colour, float omega,
-                                                              float h2, float gamma, const double* __restrict__ check,
-                                                              double tol2) {
+                                                              const float* __restrict__ b, int colour, int zero,
+                                                              float omega, float h2, float gamma,
+                                                              const double* __restrict__ check, double tol2) {
     if (done(check, tol2)) return;
+    // Programmatic dependent launches: the next kernel of the cycle may be scheduled now; u and
+    // b are read after griddepcontrol.wait (a no-op for an ordinary launch).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const int num_leaves = (int)t.num_leaves;
     const int64_t t0 = (int64_t)blockIdx.x * kThreads + threadIdx.x;
     LevelCell<LG> c;
-    int64_t q;
+    int64_t q, other = -1;
     if constexpr (LG == 0) {
-        // One cell per leaf: the leaf's parity decides.
+        // One cell per leaf: the leaf's parity decides; from u = 0 the other colour writes 0.
         if (t0 >= num_leaves) return;
         q = t0;
         c = level_cell<0>(q);
         const int4 o = t.origin[c.leaf];
-        if ((((o.x + o.y + o.z) >> 3) & 1) != colour) return;
+        if ((((o.x + o.y + o.z) >> 3) & 1) != colour) {
+            if (zero) {
+                asm volatile("griddepcontrol.wait;" ::: "memory");
+                u[q] = 0.f;
+            }
+            return;
+        }
     } else {
-        // One thread per cell of the colour: the z pair (2k, 2k + 1) of row (x, y) holds one.
+        // One thread per cell of the colour: the z pair (2k, 2k + 1) of row (x, y) holds one; from
+        // u = 0 the thread also writes the pair's other cell.
         constexpr int m = (1 << LG) - 1, hz = (1 << (LG - 1)) - 1;
         if (t0 >= ((int64_t)num_leaves << (3 * LG - 1))) return;
         c.leaf = (int)(t0 >> (3 * LG - 1));
         c.x = (int)(t0 >> (2 * LG - 1)) & m;
         c.y = (int)(t0 >> (LG - 1)) & m;
-        c.z = 2 * ((int)t0 & hz) + ((c.x + c.y + colour) & 1);
+        const int z0 = 2 * ((int)t0 & hz);
+        c.z = z0 + ((c.x + c.y + colour) & 1);
         q = ((int64_t)c.leaf << (3 * LG)) + (((c.x << LG) + c.y) << LG) + c.z;
+        other = q + (c.z == z0 ? 1 : -1);
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     int missing;
+    if (zero) {
+        // u = 0 before this sweep (the first of a level's cycle): no neighbour is read.
+        float unused = level_nsum<LG, false>(nb8, u, c.leaf, c.x, c.y, c.z, num_leaves, missing);
+        (void)unused;
+        u[q] = omega * (-h2 * __ldg(b + q)) / (6.0f + gamma * (float)missing);
+        if constexpr (LG > 0) u[other] = 0.f;
+        return;
+    }
     const float sum = level_nsum<LG>(nb8, u, c.leaf, c.x, c.y, c.z, num_leaves, missing);
     const float uq = u[q];
     u[q] = uq + omega * ((sum - h2 * __ldg(b + q)) / (6.0f + gamma * (float)missing) - uq);
@@ -247,6 +268,8 @@ __global__ void __launch_bounds__(kThreads) mgl_restrict_kernel(const int4* __re
                                                                 int num_leaves, float inv_h2, float gamma,
                                                                 const double* __restrict__ check, double tol2) {
     if (done(check, tol2)) return;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
     if (q >= ((int64_t)num_leaves << (3 * (LG - 1)))) return;
     const LevelCell<LG - 1> cc = level_cell<LG - 1>(q);
@@ -306,49 +329,132 @@ __device__ __forceinline__ uint32_t split_at(int l, int x, int y, int z) {
 
 __device__ __forceinline__ float h16(const __half* p, uint32_t i) { return __half2float(p[i]); }
 
+// The 8 values of row (x, y) of leaf l, z order, from its two colour blocks (colour c holds
+// z = 2 j + ((x + y + c) & 1) at entries 4 R + j).
+__device__ __forceinline__ void row8(const __half* p, int l, int x, int y, float v[8]) {
+    const uint32_t R = (uint32_t)(32 * ((x + y) & 1) + 4 * x + (y >> 1));
+    const uint2 a = *reinterpret_cast<const uint2*>(p + ((uint32_t)l << 9) + 4 * R);
+    const uint2 b = *reinterpret_cast<const uint2*>(p + ((uint32_t)l << 9) + 256 + 4 * R);
+    const int p0 = (x + y) & 1;
+    const uint32_t ha[4] = {a.x & 0xFFFFu, a.x >> 16, a.y & 0xFFFFu, a.y >> 16};
+    const uint32_t hb[4] = {b.x & 0xFFFFu, b.x >> 16, b.y & 0xFFFFu, b.y >> 16};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float fa = __half2float(__ushort_as_half((unsigned short)ha[j]));
+        const float fb = __half2float(__ushort_as_half((unsigned short)hb[j]));
+        v[2 * j] = p0 ? fb : fa;
+        v[2 * j + 1] = p0 ? fa : fb;
+    }
+}
+
 // Fine level of the FP16 cycle: b1 (4^3 cells per leaf) = the mean of the residuals
 // r^ - (sum - 6 e) (unit spacing; a missing leaf is the zero leaf past the last one, p = 0 outside
-// the domain) of each level-1 cell's 8 voxels, e and r^ in the colour-split layout.
+// the domain) of each level-1 cell's 8 voxels, e and r^ in the colour-split layout. One thread
+// per fine row (thread leaf * 64 + 8 x + y): its 8 residuals from the row, its four neighbour
+// rows (across a face: the neighbour leaf's row) and the two values past its z ends, summed in
+// z pairs; the four rows of a level-1 column (lanes differing in bits 0 and 3) are added with
+// two shuffles and the column's 4 values stored by its first row.
 __global__ void __launch_bounds__(kThreads) mg16_restrict_kernel(const int4* __restrict__ nb8, const __half* e,
                                                                  const __half* __restrict__ rhat, float* __restrict__ b1,
                                                                  int num_leaves, const double* __restrict__ check,
                                                                  double tol2) {
     if (done(check, tol2)) return;
-    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-    if (q >= ((int64_t)num_leaves << 6)) return;
-    const LevelCell<2> cc = level_cell<2>(q);
-    const int4 f0 = __ldg(nb8 + 2 * cc.leaf), f1 = __ldg(nb8 + 2 * cc.leaf + 1);
-    float sum = 0.f;
+    const int64_t tid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (tid >= ((int64_t)num_leaves << 6)) return;  // whole warps: 64 threads per leaf
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int leaf = (int)(tid >> 6), x = (int)(tid >> 3) & 7, y = (int)tid & 7;
+    const int4 f0 = __ldg(nb8 + 2 * leaf), f1 = __ldg(nb8 + 2 * leaf + 1);
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // e is the preceding half-sweep's
+    float c[8], xp[8], xm[8], yp[8], ym[8], rh[8];
+    row8(e, leaf, x, y, c);
+    row8(e, x < 7 ? leaf : f0.x, (x + 1) & 7, y, xp);
+    row8(e, x > 0 ? leaf : f0.y, (x - 1) & 7, y, xm);
+    row8(e, y < 7 ? leaf : f0.z, x, (y + 1) & 7, yp);
+    row8(e, y > 0 ? leaf : f0.w, x, (y - 1) & 7, ym);
+    row8(rhat, leaf, x, y, rh);
+    const float zlo = h16(e, split_at(f1.y, x, y, 7)), zhi = h16(e, split_at(f1.x, x, y, 0));
+    float part[4];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int x = 2 * cc.x + (k >> 2), y = 2 * cc.y + ((k >> 1) & 1), z = 2 * cc.z + (k & 1);
-        float ns = h16(e, split_at(x < 7 ? cc.leaf : f0.x, (x + 1) & 7, y, z));
-        ns += h16(e, split_at(x > 0 ? cc.leaf : f0.y, (x - 1) & 7, y, z));
-        ns += h16(e, split_at(y < 7 ? cc.leaf : f0.z, x, (y + 1) & 7, z));
-        ns += h16(e, split_at(y > 0 ? cc.leaf : f0.w, x, (y - 1) & 7, z));
-        ns += h16(e, split_at(z < 7 ? cc.leaf : f1.x, x, y, (z + 1) & 7));
-        ns += h16(e, split_at(z > 0 ? cc.leaf : f1.y, x, y, (z - 1) & 7));
-        const uint32_t o = split_at(cc.leaf, x, y, z);
-        sum += __half2float(rhat[o]) - (ns - 6.0f * h16(e, o));
+    for (int Z = 0; Z < 4; ++Z) {
+        float sum = 0.f;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int z = 2 * Z + k;
+            const float zm = z > 0 ? c[z > 0 ? z - 1 : 0] : zlo, zpv = z < 7 ? c[z < 7 ? z + 1 : 7] : zhi;
+            sum += rh[z] - (xp[z] + xm[z] + yp[z] + ym[z] + zpv + zm - 6.0f * c[z]);
+        }
+        part[Z] = sum;
     }
-    b1[q] = 0.125f * sum;
+#pragma unroll
+    for (int Z = 0; Z < 4; ++Z) {
+        part[Z] += __shfl_xor_sync(0xffffffffu, part[Z], 1);
+        part[Z] += __shfl_xor_sync(0xffffffffu, part[Z], 8);
+    }
+    if (((x | y) & 1) == 0)
+        *reinterpret_cast<float4*>(b1 + ((int64_t)leaf << 6) + ((((x >> 1) << 2) + (y >> 1)) << 2)) =
+            make_float4(0.125f * part[0], 0.125f * part[1], 0.125f * part[2], 0.125f * part[3]);
 }
 
-// e (FP16, colour-split) += the level-1 correction interpolated trilinearly, one rounding; one
-// thread per level-1 cell.
+// e (FP16, colour-split) += the level-1 correction interpolated trilinearly, one rounding per
+// value. One thread per fine row (x, y), both colours: the 4 voxels of colour c are z = 2 j + p
+// (p = (x + y + c) & 1), 8 contiguous bytes at the row's position R in the colour block; their
+// parents are level-1 cells Z = j, and along z each takes 3/4 of the parent and 1/4 of Z - 1
+// (p = 0) or Z + 1 (p = 1). Both colours use the 4 level-1 columns (X + {0, sx}) x (Y + {0, sy})
+// (4 contiguous floats each, in this leaf or its x, y or xy-edge neighbour) and one value past
+// each column's z ends (in the z neighbours of that leaf); 0 where a leaf is missing. Threads
+// take consecutive R, so a warp's p is uniform.
+template <int P>
+__device__ __forceinline__ uint2 prolong_row(const float (&col)[2][2][4], const float (&lo)[2][2], const float (&hi)[2][2],
+                                             uint2 raw) {
+    uint32_t h[4] = {raw.x & 0xFFFFu, raw.x >> 16, raw.y & 0xFFFFu, raw.y >> 16};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float sum = 0.f;
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const float other = P ? (j < 3 ? col[a][b][j + 1] : hi[a][b]) : (j > 0 ? col[a][b][j - 1] : lo[a][b]);
+                const float w = (a ? 0.25f : 0.75f) * (b ? 0.25f : 0.75f);
+                sum = fmaf(w, fmaf(0.25f, other, 0.75f * col[a][b][j]), sum);
+            }
+        h[j] = __half_as_ushort(__float2half_rn(__half2float(__ushort_as_half((unsigned short)h[j])) + sum));
+    }
+    return make_uint2(h[0] | (h[1] << 16), h[2] | (h[3] << 16));
+}
+
 __global__ void __launch_bounds__(kThreads) mg16_prolong_kernel(TopoView t, const float* __restrict__ u1, __half* e,
                                                                 const double* __restrict__ check, double tol2) {
     if (done(check, tol2)) return;
-    const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-    if (q >= (t.num_leaves << 6)) return;
-    const LevelCell<2> c = level_cell<2>(q);
-    float v[27];
-    gather27<2>(t, u1, c.leaf, c.x, c.y, c.z, v);
+    const int64_t tid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (tid >= (t.num_leaves << 6)) return;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const int leaf = (int)(tid >> 6), R = (int)tid & 63;
+    const int par = R >> 5, x = (R & 31) >> 2, y = 2 * (R & 3) + ((par + x) & 1);
+    const int X = x >> 1, Y = y >> 1, sx = (x & 1) ? 1 : -1, sy = (y & 1) ? 1 : -1;
+    const int* nb = t.nbr27 + (int64_t)leaf * 27;
+    float col[2][2][4], lo[2][2], hi[2][2];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int i = k >> 2, j = (k >> 1) & 1, l = k & 1;
-        const uint32_t o = split_at(c.leaf, 2 * c.x + i, 2 * c.y + j, 2 * c.z + l);
-        e[o] = __float2half_rn(__half2float(e[o]) + interp8(v, i, j, l));
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            int cx = X + a * sx, cy = Y + b * sy;
+            const int ox = cx < 0 ? -1 : (cx > 3 ? 1 : 0), oy = cy < 0 ? -1 : (cy > 3 ? 1 : 0);
+            cx -= 4 * ox, cy -= 4 * oy;
+            const int k = (ox + 1) * 9 + (oy + 1) * 3 + 1;  // nbr27 index of the column's leaf
+            const int l = (ox | oy) ? __ldg(nb + k) : leaf, lm = __ldg(nb + k - 1), lp = __ldg(nb + k + 1);
+            const int64_t off = ((cx << 2) + cy) << 2;
+            const float4 v = l < 0 ? make_float4(0.f, 0.f, 0.f, 0.f)
+                                   : __ldg(reinterpret_cast<const float4*>(u1 + ((int64_t)l << 6) + off));
+            col[a][b][0] = v.x, col[a][b][1] = v.y, col[a][b][2] = v.z, col[a][b][3] = v.w;
+            lo[a][b] = lm < 0 ? 0.f : __ldg(u1 + ((int64_t)lm << 6) + off + 3);
+            hi[a][b] = lp < 0 ? 0.f : __ldg(u1 + ((int64_t)lp << 6) + off);
+        }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        uint2* row = reinterpret_cast<uint2*>(e + ((uint32_t)leaf << 9) + ((uint32_t)c << 8) + 4 * R);
+        *row = ((par + c) & 1) ? prolong_row<1>(col, lo, hi, *row) : prolong_row<0>(col, lo, hi, *row);
     }
 }
 
@@ -358,6 +464,8 @@ __global__ void __launch_bounds__(kThreads) mgl_prolong_kernel(TopoView t, const
                                                                float* __restrict__ u, const double* __restrict__ check,
                                                                double tol2) {
     if (done(check, tol2)) return;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const int64_t q = (int64_t)blockIdx.x * kThreads + threadIdx.x;
     if (q >= (t.num_leaves << (3 * (LG - 1)))) return;
     const LevelCell<LG - 1> c = level_cell<LG - 1>(q);
@@ -435,18 +543,35 @@ namespace {
 constexpr int kMgNu = 2, kMgCoarseIters = 10;
 constexpr float kMgCoarseOmega = 1.5f;
 
+// Kernels of the cycle are programmatic dependent launches: each lets the next be scheduled
+// at its start and reads the data the preceding ones wrote after griddepcontrol.wait.
+template <typename... KArgs, typename... Args>
+void launch_pdl(const Context& c, void (*kern)(KArgs...), int64_t threads, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks(threads));
+    cfg.blockDim = dim3(kThreads);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HNS_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+    HNS_LAUNCHED();
+}
+
+// iters red-black iterations at level l (2^LG cells per leaf side); from_zero: u = 0 before them
+// (the first red sweep writes both colours).
 template <int LG>
-void smooth_level(Context& c, const int4* nb8, float* u, const float* b, int iters, float omega, int l,
+void smooth_level(Context& c, const int4* nb8, float* u, const float* b, int iters, float omega, int l, bool from_zero,
                   const double* check, double tol2) {
     const float h2 = (float)(1 << (2 * l)), gamma = (float)((1 << l) - 1) / (float)((1 << l) + 1);
     int64_t threads = c.topo.num_leaves;  // LG = 0: one thread per leaf
     if constexpr (LG > 0) threads <<= 3 * LG - 1;  // one thread per cell of the colour
-    const unsigned g = blocks(threads);
     for (int it = 0; it < iters; ++it)
-        for (int colour = 0; colour < 2; ++colour) {
-            mgl_smooth_kernel<LG><<<g, kThreads, 0, c.stream>>>(c.topo.view, nb8, u, b, colour, omega, h2, gamma, check, tol2);
-            HNS_LAUNCHED();
-        }
+        for (int colour = 0; colour < 2; ++colour)
+            launch_pdl(c, mgl_smooth_kernel<LG>, threads, c.topo.view, nb8, u, b, colour,
+                       (int)(from_zero && it == 0 && colour == 0), omega, h2, gamma, check, tol2);
 }
 }  // namespace
 
@@ -470,32 +595,20 @@ void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_z
             launch_rbgs_split_half(c, nb8, rhat, e, 1, false, 1.0f, check, tol2, false);
         }
     };
-    auto zero = [&](int l) {
-        HNS_CUDA(cudaMemsetAsync(u[l], 0, sizeof(float) * ((size_t)L << (3 * (3 - l))), c.stream));
-    };
     fine(e_zero);
-    mg16_restrict_kernel<<<blocks(L << 6), kThreads, 0, c.stream>>>(f8, eh, r, b[1], (int)L, check, tol2);
-    HNS_LAUNCHED();
-    zero(1);
-    smooth_level<2>(c, f8, u[1], b[1], kMgNu, 1.0f, 1, check, tol2);
-    mgl_restrict_kernel<2><<<blocks(L << 3), kThreads, 0, c.stream>>>(f8, u[1], b[1], b[2], (int)L, 0.25f, 1.0f / 3.0f,
-                                                                       check, tol2);
-    HNS_LAUNCHED();
-    zero(2);
-    smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, check, tol2);
-    mgl_restrict_kernel<1><<<blocks(L), kThreads, 0, c.stream>>>(f8, u[2], b[2], b[3], (int)L, 1.0f / 16.0f, 0.6f, check,
-                                                                  tol2);
-    HNS_LAUNCHED();
-    zero(3);
-    smooth_level<0>(c, f8, u[3], b[3], kMgCoarseIters, kMgCoarseOmega, 3, check, tol2);
-    mgl_prolong_kernel<1><<<blocks(L), kThreads, 0, c.stream>>>(t, u[3], u[2], check, tol2);
-    HNS_LAUNCHED();
-    smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, check, tol2);
-    mgl_prolong_kernel<2><<<blocks(L << 3), kThreads, 0, c.stream>>>(t, u[2], u[1], check, tol2);
-    HNS_LAUNCHED();
-    smooth_level<2>(c, f8, u[1], b[1], kMgNu, 1.0f, 1, check, tol2);
-    mg16_prolong_kernel<<<blocks(L << 6), kThreads, 0, c.stream>>>(t, u[1], eh, check, tol2);
-    HNS_LAUNCHED();
+    launch_pdl(c, mg16_restrict_kernel, L << 6, f8, (const __half*)eh, r, b[1], (int)L, check, tol2);
+    smooth_level<2>(c, f8, u[1], b[1], kMgNu, 1.0f, 1, true, check, tol2);
+    launch_pdl(c, mgl_restrict_kernel<2>, L << 3, f8, (const float*)u[1], (const float*)b[1], b[2], (int)L, 0.25f,
+               1.0f / 3.0f, check, tol2);
+    smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, true, check, tol2);
+    launch_pdl(c, mgl_restrict_kernel<1>, L, f8, (const float*)u[2], (const float*)b[2], b[3], (int)L, 1.0f / 16.0f,
+               0.6f, check, tol2);
+    smooth_level<0>(c, f8, u[3], b[3], kMgCoarseIters, kMgCoarseOmega, 3, true, check, tol2);
+    launch_pdl(c, mgl_prolong_kernel<1>, L, t, (const float*)u[3], u[2], check, tol2);
+    smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, false, check, tol2);
+    launch_pdl(c, mgl_prolong_kernel<2>, L << 3, t, (const float*)u[2], u[1], check, tol2);
+    smooth_level<2>(c, f8, u[1], b[1], kMgNu, 1.0f, 1, false, check, tol2);
+    launch_pdl(c, mg16_prolong_kernel, L << 6, t, (const float*)u[1], eh, check, tol2);
     fine(false);
 }
 
