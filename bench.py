@@ -471,6 +471,7 @@ def ours(args, wl):
     stream = torch.cuda.Stream(device=dev)
     g.set_stream(stream.cuda_stream)
     mixed = args.precision == "mixed"
+    multigrid = mixed and args.inner == "multigrid"
     tol = wl["tolerance"]
 
     # ---- FP32 forms (always measured: the comparison at equal residual) ----
@@ -534,22 +535,48 @@ def ours(args, wl):
         vb = [torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous(), torch.empty((n, 3), dtype=torch.bfloat16, device=dev)]
         dh = [torch.from_numpy(dens).to(dev).to(torch.float16).contiguous(), torch.empty(n, dtype=torch.float16, device=dev)]
 
-        def mdesc(outer):
-            if args.multigrid:
+        def mdesc(outer, mg):
+            if mg:
                 return hl.MixedDesc(dt=wl["dt"], omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
                                     inner_iterations=args.cycles, flags=hl.SOLVE_MULTIGRID)
             return hl.MixedDesc(dt=wl["dt"], omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
                                 inner_iterations=wl["inner"], flags=0)
 
-        info = solve_once(lambda: g.step_mixed(vb[0], vb[1], [dh[0]], [dh[1]], mdesc(16), info=True), g.last_refine)
-        outer = max(1, info.iterations // (args.cycles if args.multigrid else wl["inner"])) + 1
-        st = mdesc(outer)
         ms_state = [0]
 
-        def step():
-            s0 = ms_state[0]
-            g.step_mixed(vb[s0], vb[1 - s0], [dh[s0]], [dh[1 - s0]], st)
-            ms_state[0] = 1 - s0
+        def mixed_form(mg):
+            """(solve info of a calibration step, the step at an outer cap one above its need)."""
+            info = solve_once(lambda: g.step_mixed(vb[0], vb[1], [dh[0]], [dh[1]], mdesc(16, mg), info=True),
+                              g.last_refine)
+            outer = max(1, info.iterations // (args.cycles if mg else wl["inner"])) + 1
+            st = mdesc(outer, mg)
+
+            def step():
+                s0 = ms_state[0]
+                g.step_mixed(vb[s0], vb[1 - s0], [dh[s0]], [dh[1 - s0]], st)
+                ms_state[0] = 1 - s0
+            return info, outer, st, step
+
+        red_black = None
+        if multigrid:
+            # The red-black inner solve in the same run: its time, and the time of its half-sweep
+            # launches, the kernel that is also the multigrid's fine smoother (the roofline).
+            _, _, _, step_rb = mixed_form(False)
+            for _ in range(2):
+                step_rb()
+            rb_steps = max(1, min(args.steps, 3))
+            g.profile_read()
+            g.profile_enable(True)
+            ms_rb = _timed_steps(torch, stream, step_rb, rb_steps) / rb_steps
+            g.profile_enable(False)
+            prof_rb = g.profile_read()
+            last_rb = g.last_refine()
+            red_black = {"ms_per_step": ms_rb, "value": n / (ms_rb / 1e3), "inner_iterations": wl["inner"],
+                         "omega": wl["omega_refined"], "red_black_iterations": last_rb.iterations,
+                         "residual": last_rb.residual,
+                         "half_sweep_ms": prof_rb.phase_ms[hl.PHASES["inner"]] / max(1, prof_rb.solver_launches),
+                         "half_sweeps_timed": int(prof_rb.solver_launches)}
+        info, outer, st, step = mixed_form(multigrid)
 
         # record packing, advection, divergence, first residual, convergence log, gradient; per
         # outer iteration scale, 2 half-sweeps per inner iteration, update, residual (the face
@@ -585,10 +612,16 @@ def ours(args, wl):
     value = replicas.aggregate_rate(R, n, args.steps, ms)
 
     # Dominant kernel: average duration of its launches inside the timed region (phase
-    # events around them / device counter of launches that ran).
-    kms = prof.phase_ms[hl.PHASES[phase]]
-    launches = max(1, prof.solver_launches)
-    k_ms = kms / launches
+    # events around them / device counter of launches that ran). With the multigrid inner solve
+    # the inner phase also holds the coarse levels: the half-sweep's launches are timed in the
+    # red-black form of the same step, in the same run.
+    if mixed and multigrid:
+        k_ms = red_black["half_sweep_ms"]
+        launches = red_black["half_sweeps_timed"]
+    else:
+        kms = prof.phase_ms[hl.PHASES[phase]]
+        launches = max(1, prof.solver_launches)
+        k_ms = kms / launches
     peak, peak_kind = measured_peak_gbs()
     achieved = kernel_bytes * n / (k_ms / 1e3) / 1e9
     traffic = profiled_traffic(args.workload, "split" if mixed else "f32")
@@ -634,8 +667,16 @@ def ours(args, wl):
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
                "timed_solves_logged": logged, "worst_residual_timed_steps": worst,
                "timed_steps_above_tolerance": not_converged, "field_error_vs_fp64": field_error}
-        if mixed:
+        if mixed and multigrid:
             det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+                        "inner_solve": "multigrid V-cycles: colour-split FP16 red-black half-sweeps (omega 1) as the "
+                                       "fine smoother, FP32 leaf-local levels of 4, 2, 1 cells per leaf side",
+                        "cycles_per_outer": args.cycles, "outer_cap": outer, "cycles": last.iterations,
+                        "residual_reached": last.residual, "mixed_red_black_same_run": red_black,
+                        "mixed_vs_mixed_red_black": red_black["ms_per_step"] / ms_step})
+        elif mixed:
+            det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+                        "inner_solve": "red-black SOR iterations",
                         "omega_inner": wl["omega_refined"], "inner_iterations": wl["inner"], "outer_cap": outer,
                         "red_black_iterations": last.iterations, "residual_reached": last.residual})
         else:
@@ -650,7 +691,7 @@ def ours(args, wl):
             "roofline": {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": kernel_bytes * n, "launch_ms": k_ms,
-                         "launches_timed": int(prof.solver_launches)},
+                         "launches_timed": int(launches)},
             "cpu_baseline": cpu,
             "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 16 * n, "steps": e2e_steps,
@@ -834,6 +875,7 @@ def ours_fire(args, wl):
     g.set_stream(stream.cuda_stream)
     params, model = fire_params(hl)
     mixed = args.precision == "mixed"
+    multigrid = mixed and args.inner == "multigrid"
     dt = wl["dt"]
     tol = wl.get("tolerance")
 
@@ -894,6 +936,7 @@ def ours_fire(args, wl):
                                 "residual": lr.residual}}
 
     # ---- the timed form ----
+    red_black = None
     if mixed:
         def to_dev(d):
             out = {}
@@ -906,25 +949,50 @@ def ours_fire(args, wl):
         bufs = [cur, {k: torch.empty_like(v) for k, v in cur.items()}]
         src = to_dev({"fuel": sources["src_fuel"], "temperature": sources["src_temperature"]})
 
-        def mdesc(outer):
+        def mdesc(outer, mg):
+            if mg:
+                return hl.MixedDesc(dt=0.0, omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
+                                    inner_iterations=args.cycles, flags=hl.SOLVE_MULTIGRID)
             return hl.MixedDesc(dt=0.0, omega=wl["omega_refined"], tolerance=tol, max_outer=outer,
                                 inner_iterations=wl["inner"], flags=0)
 
-        torch.cuda.synchronize()
-        try:
-            info = g.advance_mixed(bufs[0], bufs[1], src, dt, params, model, mdesc(60), info=True)
-        except hl.HnsError as e:
-            if e.status != 6:
-                raise
-            info = g.last_refine()
-        outer = max(1, info.iterations // wl["inner"]) + 2
-        st = mdesc(outer)
         ms_state = [0]
 
-        def step():
-            s0 = ms_state[0]
-            g.advance_mixed(bufs[s0], bufs[1 - s0], src, dt, params, model, st)
-            ms_state[0] = 1 - s0
+        def fire_form(mg):
+            torch.cuda.synchronize()
+            try:
+                info = g.advance_mixed(bufs[0], bufs[1], src, dt, params, model, mdesc(60, mg), info=True)
+            except hl.HnsError as e:
+                if e.status != 6:
+                    raise
+                info = g.last_refine()
+            outer = max(1, info.iterations // (args.cycles if mg else wl["inner"])) + 2
+            st = mdesc(outer, mg)
+
+            def step():
+                s0 = ms_state[0]
+                g.advance_mixed(bufs[s0], bufs[1 - s0], src, dt, params, model, st)
+                ms_state[0] = 1 - s0
+            return info, outer, st, step
+
+        red_black = None
+        if multigrid:
+            # The red-black inner solve in the same run (time, and its half-sweeps for the roofline).
+            _, _, _, step_rb = fire_form(False)
+            step_rb()
+            rb_steps = max(1, min(args.steps, 2))
+            g.profile_read()
+            g.profile_enable(True)
+            ms_rb = _timed_steps(torch, stream, step_rb, rb_steps) / rb_steps
+            g.profile_enable(False)
+            prof_rb = g.profile_read()
+            last_rb = g.last_refine()
+            red_black = {"ms_per_step": ms_rb, "value": n / (ms_rb / 1e3), "inner_iterations": wl["inner"],
+                         "omega": wl["omega_refined"], "red_black_iterations": last_rb.iterations,
+                         "residual": last_rb.residual,
+                         "half_sweep_ms": prof_rb.phase_ms[hl.PHASES["inner"]] / max(1, prof_rb.solver_launches),
+                         "half_sweeps_timed": int(prof_rb.solver_launches)}
+        info, outer, st, step = fire_form(multigrid)
 
         # record packing, velocity advection, confinement, divergence/burn/buoyancy, first residual,
         # convergence log, gradient, scalar advection; per outer iteration scale, 2 half-sweeps per
@@ -960,7 +1028,10 @@ def ours_fire(args, wl):
     worst = max((e.residual for e in entries), default=None)
     ms = replicas.max_over_ranks(R, ms, dev)
     value = replicas.aggregate_rate(R, n, args.steps, ms)
-    k_ms = prof.phase_ms[hl.PHASES[phase]] / max(1, prof.solver_launches)
+    launches = max(1, prof.solver_launches)
+    k_ms = prof.phase_ms[hl.PHASES[phase]] / launches
+    if red_black is not None:  # the multigrid inner phase also holds the coarse levels
+        k_ms, launches = red_black["half_sweep_ms"], red_black["half_sweeps_timed"]
     peak, peak_kind = measured_peak_gbs()
     achieved = kernel_bytes * n / (k_ms / 1e3) / 1e9
 
@@ -993,7 +1064,7 @@ def ours_fire(args, wl):
 
     adjoint = None
     if rank == 0 and world == 1 and mixed and not args.no_adjoint:
-        adjoint = fire_adjoint_rollout(torch, hl, g, stream, bufs[0], src, dt, params, model, mdesc(outer + 4), n)
+        adjoint = fire_adjoint_rollout(torch, hl, g, stream, bufs[0], src, dt, params, model, mdesc(outer + 4, multigrid), n)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1011,8 +1082,15 @@ def ours_fire(args, wl):
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
                "timed_solves_logged": logged, "worst_residual_timed_steps": worst,
                "timed_steps_above_tolerance": (sum(1 for e in entries if e.residual > tol) if tol else None)}
-        if mixed:
+        if mixed and multigrid:
             det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+                        "inner_solve": "multigrid V-cycles: colour-split FP16 red-black half-sweeps (omega 1) as the "
+                                       "fine smoother, FP32 leaf-local levels of 4, 2, 1 cells per leaf side",
+                        "cycles_per_outer": args.cycles, "outer_cap": outer, "mixed_red_black_same_run": red_black,
+                        "mixed_vs_mixed_red_black": red_black["ms_per_step"] / (ms / args.steps)})
+        elif mixed:
+            det.update({"storage": "velocity bf16, scalars f16, divergence f32, pressure f64, inner solve f16",
+                        "inner_solve": "red-black SOR iterations",
                         "omega_inner": wl["omega_refined"], "inner_iterations": wl["inner"], "outer_cap": outer})
         else:
             det.update({"red_black_iterations": wl["iterations"], "omega": "2/(1+sin(3.14159 dx)) (the reference's)"})
@@ -1025,7 +1103,7 @@ def ours_fire(args, wl):
             "roofline": {"kernel": kernel_name, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "algorithmic_bytes_per_launch": kernel_bytes * n, "launch_ms": k_ms,
-                         "launches_timed": int(prof.solver_launches)},
+                         "launches_timed": int(launches)},
             "cpu_baseline": cpu,
             "e2e": {"value": world * n / e2e_s, "unit": "voxel-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps, "path": path},
@@ -1191,9 +1269,10 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint rollout measured beside the step")
     ap.add_argument("--no-field-error", action="store_true",
                     help="skip the FP64 check of the last timed step's fields (shell512 and plume256 steps)")
-    ap.add_argument("--multigrid", action="store_true",
-                    help="mixed SOP step: V-cycles (HNS_SOLVE_MULTIGRID) as the inner solve of the refinement")
-    ap.add_argument("--cycles", type=int, default=2, help="V-cycles per outer refinement step with --multigrid")
+    ap.add_argument("--inner", choices=["multigrid", "red-black"], default="multigrid",
+                    help="inner solve of the mixed-precision refinement: V-cycles with red-black smoothing "
+                         "(HNS_SOLVE_MULTIGRID, default) or red-black SOR iterations")
+    ap.add_argument("--cycles", type=int, default=2, help="V-cycles per outer refinement step (--inner multigrid)")
     ap.add_argument("--split-solve", choices=["persistent", "per-colour"], default="per-colour",
                     help="launch form of the colour-split red-black solves (same results to the bit)")
     ap.add_argument("--no-fp32-comparison", action="store_true",

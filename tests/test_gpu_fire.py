@@ -62,10 +62,11 @@ def _host64(t, n):
     return a.reshape(n, 3) if a.size == 3 * n else a
 
 
-@pytest.mark.parametrize("combustion,alpha,substeps,disturbance,factor",
-                         [(1, 0.1, 1, 0.0, 1.0), (0, 0.1, 1, 0.0, 1.0), (1, 0.0, 2, 1.0, 1.0), (2, 0.1, 1, 0.0, 1.0),
-                          (1, 0.1, 1, 0.0, 2.0)])
-def test_fire_mixed_against_fp64_oracle(dev, oracle, combustion, alpha, substeps, disturbance, factor):
+@pytest.mark.parametrize("combustion,alpha,substeps,disturbance,factor,multigrid",
+                         [(1, 0.1, 1, 0.0, 1.0, False), (0, 0.1, 1, 0.0, 1.0, False), (1, 0.0, 2, 1.0, 1.0, False),
+                          (2, 0.1, 1, 0.0, 1.0, False), (1, 0.1, 1, 0.0, 2.0, False), (1, 0.1, 1, 0.0, 1.0, True),
+                          (0, 0.1, 1, 0.0, 1.0, True), (1, 0.0, 2, 1.0, 1.0, True)])
+def test_fire_mixed_against_fp64_oracle(dev, oracle, combustion, alpha, substeps, disturbance, factor, multigrid):
     from oracle.binding import ForceModel as OM
 
     from hnanosolver_b200 import lib as hl
@@ -92,7 +93,10 @@ def test_fire_mixed_against_fp64_oracle(dev, oracle, combustion, alpha, substeps
             omega=1.9)
     gm = hl.ForceModel(combustion=combustion, burn_rate=0.5, heat_release=1.0, ignition_temp=0.0,
                        density_buoyancy=alpha)
-    desc = hl.MixedDesc(dt=0.0, omega=1.9, tolerance=TOL, max_outer=12, inner_iterations=30, flags=0)
+    if multigrid:  # two V-cycles per outer step
+        desc = hl.MixedDesc(dt=0.0, omega=1.9, tolerance=TOL, max_outer=12, inner_iterations=2, flags=hl.SOLVE_MULTIGRID)
+    else:
+        desc = hl.MixedDesc(dt=0.0, omega=1.9, tolerance=TOL, max_outer=12, inner_iterations=30, flags=0)
     grid = hl.Grid(origins, voxel_size=0.1)
     t = oracle.topo(origins)
     cur = _to_dev(dev, state)

@@ -337,7 +337,7 @@ def test_outer_forecast_short_grids_bit_exact(dev, shell):
         assert torch.equal(got[0], ref[0]) and torch.equal(got[1], ref[1])
 
 
-@pytest.mark.parametrize("grid", ["spheres", "box"])
+@pytest.mark.parametrize("grid", ["spheres", "box", "shell"])
 def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
     """HNS_SOLVE_MULTIGRID: V-cycles (two per outer step for the mixed step, one for the FP32
     refined step) in place of the red-black iterations. The FP64 residual of the returned pressure, recomputed by the oracle, is within the tolerance,
@@ -347,6 +347,8 @@ def test_multigrid_inner_solve_reaches_the_tolerance(dev, oracle, grid):
 
     if grid == "spheres":
         origins = synth.spheres_topology(96, 3, 8.0, 20.0, seed=11)
+    elif grid == "shell":
+        origins = synth.shell_topology(160, 60.0, 8.0, seed=2)
     else:
         origins = synth.topology("box64")
     dens, vel = synth.noise_fields(origins, seed=7)
