@@ -538,8 +538,10 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
 // 4, 2 and 1 cells per leaf side in FP32 with the wall-corrected operator, kMgNu iterations
 // before and after at the first two, kMgCoarseIters SOR iterations at the last.
 namespace {
-// Coarsest sweeps: on shell512 (about six leaves thick) 10 keep the cycle at about 0.15; 2 (which
-// suffice on a thinner shell) doubled the cycles.
+// Coarsest sweeps: 10. On shell512 (about six leaves thick) 5 also gives 6 cycles to 1e-5 (3.76
+// against 3.90 ms per step) and 2 doubles the cycles; on the 1024^3 fire (spheres up to 15 leaves
+// across) 5 made a step 41 against 30 ms and left one solve above the tolerance at the outer cap.
+// One iteration before and after at the fine level instead of 2 took 8 cycles and was slower.
 constexpr int kMgNu = 2, kMgCoarseIters = 10;
 constexpr float kMgCoarseOmega = 1.5f;
 
