@@ -164,6 +164,7 @@ struct Context {
     // Face-connected components of the leaves (hns_neumann.cu), made on the first solve with
     // zero-gradient walls: the component of each leaf, the voxels of each, FP64 sums.
     int num_components = 0;
+    int leaf_depth = -1;  // max_leaf_depth(), computed once (hns_neumann.cu)
     DeviceBuffer d_components, d_component_counts, d_component_sums;
     SolvePlan last_solve;   // schedule of the most recent checked solve (hns_last_solve)
     RefinePlan last_refine; // schedule of the most recent refined solve (hns_last_refine)
@@ -280,6 +281,9 @@ void copy_h2d(Context& c, void* dev, const void* host, size_t bytes);
 void copy_d2h(Context& c, void* host, const void* dev, size_t bytes);
 // One multigrid V-cycle (hns_multigrid.cu): u0 (n FP32) ~ A^-1 b0 for the unit-spacing system.
 void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, double tol2);
+// How many leaves deep the domain is: the largest face-step distance from a leaf to one with a
+// missing face neighbour (host, once per context).
+int max_leaf_depth(Context& c);
 // One V-cycle of the FP16 inner solve on the colour-split layout (e in place; e_zero: e = 0 before).
 void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_zero, const double* check, double tol2);
 // The FP16 inner solve on colour-split leaves (hns_rbgs_split.cu): the face-neighbour table

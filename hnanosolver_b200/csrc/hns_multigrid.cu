@@ -18,6 +18,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 
@@ -536,14 +537,21 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
 // refined in place (e_zero: e = 0 before the cycle). Fine level: kMgNu red-black iterations of
 // the colour-split half-sweep at omega = 1 before and after the coarse correction; levels with
 // 4, 2 and 1 cells per leaf side in FP32 with the wall-corrected operator, kMgNu iterations
-// before and after at the first two, kMgCoarseIters SOR iterations at the last.
+// before and after at the first two, SOR sweeps at the last (coarsest_schedule).
 namespace {
-// Coarsest sweeps: 10. On shell512 (about six leaves thick) 5 also gives 6 cycles to 1e-5 (3.76
-// against 3.90 ms per step) and 2 doubles the cycles; on the 1024^3 fire (spheres up to 15 leaves
-// across) 5 made a step 41 against 30 ms and left one solve above the tolerance at the outer cap.
-// One iteration before and after at the fine level instead of 2 took 8 cycles and was slower.
-constexpr int kMgNu = 2, kMgCoarseIters = 10;
-constexpr float kMgCoarseOmega = 1.5f;
+constexpr int kMgNu = 2;
+
+// SOR sweeps and factor at the coarsest level (one cell per leaf), from how many leaves deep the
+// domain is (D, max_leaf_depth): clamp(2 D + 2, 10, 20) sweeps at clamp(2 / (1 + sin(pi / 2 D)),
+// 1.5, 1.75), the optimal SOR factor for an extent of 2 D cells. Measured (ms per step, cycles
+// per solve 6 on the shell, 8-10 on the fire): shell512 (D = 4) 10 at 1.5: 3.90, 20 at 1.5: 4.17,
+// 5 at 1.5: 3.76 (2 doubled the cycles); fire1024 (D = 15) 10 at 1.5: 29.9, 5 at 1.5: 41 with a
+// solve above the tolerance at the outer cap, 20 at 1.5: 24.3, 20 at 1.75: 21.3, 40 at 1.8: 22.0.
+void coarsest_schedule(Context& c, int& sweeps, float& omega) {
+    const int d = std::max(1, max_leaf_depth(c));
+    sweeps = std::min(20, std::max(10, 2 * d + 2));
+    omega = std::min(1.75f, std::max(1.5f, 2.0f / (1.0f + std::sin(3.14159265f / (2.0f * (float)d)))));
+}
 
 // Kernels of the cycle are programmatic dependent launches: each lets the next be scheduled
 // at its start and reads the data the preceding ones wrote after griddepcontrol.wait.
@@ -605,7 +613,10 @@ void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_z
     smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, true, check, tol2);
     launch_pdl(c, mgl_restrict_kernel<1>, L, f8, (const float*)u[2], (const float*)b[2], b[3], (int)L, 1.0f / 16.0f,
                0.6f, check, tol2);
-    smooth_level<0>(c, f8, u[3], b[3], kMgCoarseIters, kMgCoarseOmega, 3, true, check, tol2);
+    int coarse_sweeps;
+    float coarse_omega;
+    coarsest_schedule(c, coarse_sweeps, coarse_omega);
+    smooth_level<0>(c, f8, u[3], b[3], coarse_sweeps, coarse_omega, 3, true, check, tol2);
     launch_pdl(c, mgl_prolong_kernel<1>, L, t, (const float*)u[3], u[2], check, tol2);
     smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, false, check, tol2);
     launch_pdl(c, mgl_prolong_kernel<2>, L << 3, t, (const float*)u[2], u[1], check, tol2);

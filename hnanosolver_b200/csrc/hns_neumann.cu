@@ -7,6 +7,7 @@
 // the Neumann form are in hns_kernels.cu.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -59,6 +60,51 @@ struct KeyHash {
 };
 
 }  // namespace
+
+// The largest number of face steps, over leaves, from a leaf to the nearest leaf with a missing
+// face neighbour (0 when every leaf has one): how many leaves deep the domain is. Computed on the
+// host once per context by a breadth-first pass from those boundary leaves.
+int max_leaf_depth(Context& c) {
+    if (c.leaf_depth >= 0) return c.leaf_depth;
+    const int64_t L = c.topo.num_leaves;
+    const int32_t* o = c.topo.origins.data();
+    std::unordered_map<Key, int32_t, KeyHash> index;
+    index.reserve((size_t)L * 2);
+    for (int64_t l = 0; l < L; ++l) index.emplace(Key{o[3 * l] >> 3, o[3 * l + 1] >> 3, o[3 * l + 2] >> 3}, (int32_t)l);
+    auto neighbours = [&](int32_t l, int32_t out[6]) {
+        const Key k{o[3 * l] >> 3, o[3 * l + 1] >> 3, o[3 * l + 2] >> 3};
+        const Key nbrs[6] = {{k.x + 1, k.y, k.z}, {k.x - 1, k.y, k.z}, {k.x, k.y + 1, k.z},
+                             {k.x, k.y - 1, k.z}, {k.x, k.y, k.z + 1}, {k.x, k.y, k.z - 1}};
+        for (int q = 0; q < 6; ++q) {
+            const auto it = index.find(nbrs[q]);
+            out[q] = it == index.end() ? -1 : it->second;
+        }
+    };
+    std::vector<int32_t> depth((size_t)L, -1), queue;
+    queue.reserve((size_t)L);
+    for (int64_t l = 0; l < L; ++l) {
+        int32_t n[6];
+        neighbours((int32_t)l, n);
+        if (n[0] < 0 || n[1] < 0 || n[2] < 0 || n[3] < 0 || n[4] < 0 || n[5] < 0) {
+            depth[(size_t)l] = 0;
+            queue.push_back((int32_t)l);
+        }
+    }
+    int deepest = 0;
+    for (size_t h = 0; h < queue.size(); ++h) {
+        const int32_t l = queue[h];
+        int32_t n[6];
+        neighbours(l, n);
+        for (int32_t m : n)
+            if (m >= 0 && depth[(size_t)m] < 0) {
+                depth[(size_t)m] = depth[(size_t)l] + 1;
+                deepest = std::max(deepest, depth[(size_t)m]);
+                queue.push_back(m);
+            }
+    }
+    c.leaf_depth = deepest;
+    return deepest;
+}
 
 // Face-connected components of the context's leaves, labelled on the host once per context
 // (breadth-first over face neighbours) and kept on the device with their voxel counts.
