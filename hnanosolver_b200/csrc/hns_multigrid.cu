@@ -261,6 +261,63 @@ __global__ void __launch_bounds__(kThreads) mgl_smooth_kernel(TopoView t, const 
     u[q] = uq + omega * ((sum - h2 * __ldg(b + q)) / (6.0f + gamma * (float)missing) - uq);
 }
 
+// The same sweep at level 1 (4^3 cells per leaf) by rows: one thread per z-row (4 contiguous
+// floats), which updates its 2 cells of the colour from 16-byte loads of the row, its right-hand
+// side and its 4 x/y neighbour rows (across a face, the neighbour leaf's row; a missing leaf adds
+// gamma to the diagonal) and the values past its z ends, and stores the row back whole (no other
+// thread writes it in this sweep). Neighbours are summed in mgl_smooth_kernel's order, so the
+// values are its values: 8 loads for 2 updates where it makes 20.
+__global__ void __launch_bounds__(kThreads) level1_smooth_rows_kernel(const int4* __restrict__ nb8, float* u,
+                                                                      const float* __restrict__ b, int num_leaves,
+                                                                      int colour, int zero, float omega, float h2,
+                                                                      float gamma, const double* __restrict__ check,
+                                                                      double tol2) {
+    if (done(check, tol2)) return;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int64_t tid = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    if (tid >= ((int64_t)num_leaves << 4)) return;
+    const int leaf = (int)(tid >> 4), x = (int)(tid >> 2) & 3, y = (int)tid & 3;
+    const int4 f0 = __ldg(nb8 + 2 * leaf), f1 = __ldg(nb8 + 2 * leaf + 1);
+    auto row_of = [&](int l, int a, int c2) { return ((int64_t)l << 6) + (((a << 2) + c2) << 2); };
+    const int lxp = x < 3 ? leaf : f0.x, lxm = x > 0 ? leaf : f0.y, lyp = y < 3 ? leaf : f0.z, lym = y > 0 ? leaf : f0.w;
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto ld4 = [&](int l, int64_t off) { return l < num_leaves ? __ldg(reinterpret_cast<const float4*>(u + off)) : z4; };
+    const int64_t own = row_of(leaf, x, y);
+    const float4 bb = __ldg(reinterpret_cast<const float4*>(b + own));
+    float4 c4 = zero ? z4 : __ldg(reinterpret_cast<const float4*>(u + own));
+    const float4 xp = zero ? z4 : ld4(lxp, row_of(lxp, (x + 1) & 3, y));
+    const float4 xm = zero ? z4 : ld4(lxm, row_of(lxm, (x - 1) & 3, y));
+    const float4 yp = zero ? z4 : ld4(lyp, row_of(lyp, x, (y + 1) & 3));
+    const float4 ym = zero ? z4 : ld4(lym, row_of(lym, x, (y - 1) & 3));
+    const float zhi = (zero || f1.x >= num_leaves) ? 0.f : __ldg(u + row_of(f1.x, x, y));
+    const float zlo = (zero || f1.y >= num_leaves) ? 0.f : __ldg(u + row_of(f1.y, x, y) + 3);
+    const int lateral = (lxp >= num_leaves) + (lxm >= num_leaves) + (lyp >= num_leaves) + (lym >= num_leaves);
+    float cv[4] = {c4.x, c4.y, c4.z, c4.w};
+    const float bv[4] = {bb.x, bb.y, bb.z, bb.w};
+    const float xpv[4] = {xp.x, xp.y, xp.z, xp.w}, xmv[4] = {xm.x, xm.y, xm.z, xm.w};
+    const float ypv[4] = {yp.x, yp.y, yp.z, yp.w}, ymv[4] = {ym.x, ym.y, ym.z, ym.w};
+    const float old[4] = {cv[0], cv[1], cv[2], cv[3]};
+#pragma unroll
+    for (int z = 0; z < 4; ++z) {
+        if (((x + y + z) & 1) != colour) continue;  // the other colour keeps its value (0 from zero)
+        const int missing = lateral + (z == 3 && f1.x >= num_leaves) + (z == 0 && f1.y >= num_leaves);
+        const float diag = 6.0f + gamma * (float)missing;
+        if (zero) {
+            cv[z] = omega * (-h2 * bv[z]) / diag;
+        } else {
+            float sum = xpv[z];
+            sum += xmv[z];
+            sum += ypv[z];
+            sum += ymv[z];
+            sum += z < 3 ? old[z < 3 ? z + 1 : 3] : zhi;
+            sum += z > 0 ? old[z > 0 ? z - 1 : 0] : zlo;
+            cv[z] = old[z] + omega * ((sum - h2 * bv[z]) / diag - old[z]);
+        }
+    }
+    *reinterpret_cast<float4*>(u + own) = make_float4(cv[0], cv[1], cv[2], cv[3]);
+}
+
 // bc (level LG - 1) = the mean of the residuals b - (sum - (6 + gamma missing) u) / h2 of each
 // coarse cell's 8 children at level LG.
 template <int LG>
@@ -579,9 +636,15 @@ void smooth_level(Context& c, const int4* nb8, float* u, const float* b, int ite
     int64_t threads = c.topo.num_leaves;  // LG = 0: one thread per leaf
     if constexpr (LG > 0) threads <<= 3 * LG - 1;  // one thread per cell of the colour
     for (int it = 0; it < iters; ++it)
-        for (int colour = 0; colour < 2; ++colour)
-            launch_pdl(c, mgl_smooth_kernel<LG>, threads, c.topo.view, nb8, u, b, colour,
-                       (int)(from_zero && it == 0 && colour == 0), omega, h2, gamma, check, tol2);
+        for (int colour = 0; colour < 2; ++colour) {
+            const int zero = (int)(from_zero && it == 0 && colour == 0);
+            if constexpr (LG == 2)
+                launch_pdl(c, level1_smooth_rows_kernel, c.topo.num_leaves << 4, nb8, u, b, (int)c.topo.num_leaves,
+                           colour, zero, omega, h2, gamma, check, tol2);
+            else
+                launch_pdl(c, mgl_smooth_kernel<LG>, threads, c.topo.view, nb8, u, b, colour, zero, omega, h2, gamma,
+                           check, tol2);
+        }
 }
 }  // namespace
 
