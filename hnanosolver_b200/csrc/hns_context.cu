@@ -436,6 +436,10 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
             if (value != HNS_SPLIT_PER_COLOUR && value != HNS_SPLIT_PERSISTENT)
                 fail(HNS_ERR_INVALID_ARG, "unknown inner-solve launch form");
             c->split_solve = value;
+        } else if (option == HNS_OPT_COARSE_SOLVE) {
+            if (value != HNS_COARSE_LAUNCHES && value != HNS_COARSE_CLUSTER)
+                fail(HNS_ERR_INVALID_ARG, "unknown coarse-level solve");
+            c->coarse_solve = value;
         } else if (option == HNS_OPT_WAIT_POLLS) {
             if (value < -1) fail(HNS_ERR_INVALID_ARG, "the wait limit must be -1 (default) or >= 0");
             c->first_wait_polls = value;

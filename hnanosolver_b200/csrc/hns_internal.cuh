@@ -176,6 +176,9 @@ struct Context {
     int inner_layout = HNS_INNER_SPLIT;  // hns_set_option(HNS_OPT_INNER_LAYOUT)
     int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
     int split_solve = HNS_SPLIT_PER_COLOUR;  // hns_set_option(HNS_OPT_SPLIT_SOLVE)
+    int coarse_solve = HNS_COARSE_CLUSTER;   // hns_set_option(HNS_OPT_COARSE_SOLVE)
+    int coarse_cluster_ok = -1;     // CTAs of the coarsest level's cluster, 0 if none fits (-1: not chosen)
+    int64_t coarse_table_leaves = -1;  // leaves of the coarsest level's cluster records made so far
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;

@@ -261,6 +261,171 @@ __global__ void __launch_bounds__(kThreads) mgl_smooth_kernel(TopoView t, const 
     u[q] = uq + omega * ((sum - h2 * __ldg(b + q)) / (6.0f + gamma * (float)missing) - uq);
 }
 
+// All SOR sweeps of the coarsest level (one cell per leaf) in one launch of a thread-block
+// cluster, in place of two launches per sweep. CTA r of the cluster holds the cells of leaves
+// [r P, r P + P) (P = ceil(L / CTAs)): their values u (and a zero past them, the value of
+// a missing neighbour), right-hand sides b and a 32-byte record per cell, made once per context
+// by coarse_table_kernel: the six face neighbours as (CTA rank << 16) | index in that CTA's u,
+// the diagonal 6 + gamma missing, the cell's index; colour-0 records from the front of the
+// table, colour-1 records from the back. Neighbours' values are read through the cluster's
+// shared memory window (distributed shared memory), and a cluster barrier separates the
+// colours. The arithmetic is mgl_smooth_kernel<0>'s, in its order: the values are its values.
+// The cluster has 16 CTAs (a non-portable size) where the device schedules that, else 8.
+constexpr int kCoarseThreads = 1024, kCoarseUnroll = 3;
+constexpr int kCoarseCellBytes = 32 + 4 + 4;  // the record, u, b (plus 4 bytes: u's zero)
+
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// The shared::cluster address of shared::cta address `a` in the CTA of rank `rank`.
+__device__ __forceinline__ uint32_t cluster_map(uint32_t a, uint32_t rank) {
+    uint32_t d;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(rank));
+    return d;
+}
+
+__device__ __forceinline__ float ld_cluster(uint32_t addr) {
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+// The records of CTA r's cells (block r of one per CTA of the cluster), and its colour counts.
+__global__ void __launch_bounds__(kCoarseThreads) coarse_table_kernel(TopoView t, const int4* __restrict__ nb8,
+                                                                      uint4* __restrict__ table, int* __restrict__ counts,
+                                                                      int per_cta, float gamma) {
+    __shared__ int s_count[2];
+    const int P = per_cta, tid = (int)threadIdx.x, r = (int)blockIdx.x;
+    const int num_leaves = (int)t.num_leaves;
+    const int lo = r * P, n = max(0, min(num_leaves - lo, P));
+    if (tid == 0) s_count[0] = s_count[1] = 0;
+    __syncthreads();
+    uint4* rec = table + (size_t)2 * P * r;
+    for (int i = tid; i < n; i += kCoarseThreads) {
+        const int leaf = lo + i;
+        const int4 f0 = nb8[2 * leaf], f1 = nb8[2 * leaf + 1];
+        const int nbl[6] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y};
+        uint32_t w[6];
+        int missing = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const int m = nbl[k];
+            if (m >= num_leaves) {
+                ++missing;
+                w[k] = ((uint32_t)r << 16) | (uint32_t)P;
+            } else {
+                const int q = m / P;
+                w[k] = ((uint32_t)q << 16) | (uint32_t)(m - q * P);
+            }
+        }
+        const float d = 6.0f + gamma * (float)missing;
+        const int4 o = t.origin[leaf];
+        const int slot = (((o.x + o.y + o.z) >> 3) & 1) == 0 ? atomicAdd(&s_count[0], 1)
+                                                               : P - 1 - atomicAdd(&s_count[1], 1);
+        rec[2 * slot] = make_uint4(w[0], w[1], w[2], w[3]);
+        rec[2 * slot + 1] = make_uint4(w[4], w[5], __float_as_uint(d), (uint32_t)i);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        counts[2 * r] = s_count[0];
+        counts[2 * r + 1] = s_count[1];
+    }
+}
+
+__global__ void __launch_bounds__(kCoarseThreads, 1)
+    coarsest_cluster_kernel(const uint4* __restrict__ table, const int* __restrict__ counts, float* __restrict__ u_out,
+                            const float* __restrict__ b, int num_leaves, int per_cta, int sweeps, float omega, float h2,
+                            const double* __restrict__ check, double tol2) {
+    extern __shared__ __align__(16) unsigned char coarse_smem[];
+    __shared__ float s_skip;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const int P = per_cta, tid = (int)threadIdx.x;
+    uint4* srec = reinterpret_cast<uint4*>(coarse_smem);
+    float* su = reinterpret_cast<float*>(srec + 2 * P);  // P + 1 values, su[P] = 0
+    float* sb = su + P + 1;
+    const uint32_t rank = cluster_ctarank();
+    const int lo = (int)rank * P, n = max(0, min(num_leaves - lo, P));
+    const int c0 = __ldg(counts + 2 * rank), c1 = __ldg(counts + 2 * rank + 1);
+    // The records (the topology only) before the wait on the preceding kernel.
+    const uint4* g = table + (size_t)2 * P * rank;
+    for (int k = tid; k < 2 * P; k += kCoarseThreads) srec[k] = __ldg(g + k);
+    if (tid == 0) {
+        su[P] = 0.f;
+        s_skip = 0.f;
+    }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (rank == 0 && tid == 0 && done(check, tol2)) s_skip = 1.f;
+    for (int i = tid; i < n; i += kCoarseThreads) sb[i] = __ldg(b + lo + i);
+    cluster_barrier();
+    // Every CTA takes rank 0's decision, so all or none reach the sweeps' barriers; rank 0's
+    // memory stays until each has read it.
+    if (ld_cluster(cluster_map((uint32_t)__cvta_generic_to_shared(&s_skip), 0)) != 0.f) {
+        cluster_barrier();
+        return;
+    }
+    const uint32_t su_addr = (uint32_t)__cvta_generic_to_shared(su);
+    for (int it = 0; it < sweeps; ++it) {
+        for (int colour = 0; colour < 2; ++colour) {
+            const int begin = colour ? P - c1 : 0, end = colour ? P : c0;
+            if (it == 0 && colour == 0) {
+                // u = 0 before this sweep: no neighbour is read, the other colour is set to 0.
+                for (int j = begin + tid; j < end; j += kCoarseThreads) {
+                    const uint4 q = srec[2 * j + 1];
+                    su[q.w] = omega * (-h2 * sb[q.w]) / __uint_as_float(q.z);
+                }
+                for (int j = P - c1 + tid; j < P; j += kCoarseThreads) su[srec[2 * j + 1].w] = 0.f;
+            } else {
+                // kCoarseUnroll cells per thread at a time: every load issued before the first use.
+                for (int j0 = begin + tid; j0 < end; j0 += kCoarseUnroll * kCoarseThreads) {
+                    uint4 qa[kCoarseUnroll], qb[kCoarseUnroll];
+                    float v[kCoarseUnroll][6];
+#pragma unroll
+                    for (int k = 0; k < kCoarseUnroll; ++k) {
+                        const int j = j0 + k * kCoarseThreads;
+                        if (j < end) {
+                            qa[k] = srec[2 * j];
+                            qb[k] = srec[2 * j + 1];
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < kCoarseUnroll; ++k) {
+                        if (j0 + k * kCoarseThreads < end) {
+                            const uint32_t w[6] = {qa[k].x, qa[k].y, qa[k].z, qa[k].w, qb[k].x, qb[k].y};
+#pragma unroll
+                            for (int e = 0; e < 6; ++e)
+                                v[k][e] = ld_cluster(cluster_map(su_addr + ((w[e] & 0xffffu) << 2), w[e] >> 16));
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < kCoarseUnroll; ++k) {
+                        if (j0 + k * kCoarseThreads < end) {
+                            float sum = v[k][0];
+                            sum += v[k][1];
+                            sum += v[k][2];
+                            sum += v[k][3];
+                            sum += v[k][4];
+                            sum += v[k][5];
+                            const uint32_t i = qb[k].w;
+                            const float uq = su[i];
+                            su[i] = uq + omega * ((sum - h2 * sb[i]) / __uint_as_float(qb[k].z) - uq);
+                        }
+                    }
+                }
+            }
+            cluster_barrier();
+        }
+    }
+    // After the last barrier no CTA reads another's memory.
+    for (int i = tid; i < n; i += kCoarseThreads) u_out[lo + i] = su[i];
+}
+
 // The same sweep at level 1 (4^3 cells per leaf) by rows: one thread per z-row (4 contiguous
 // floats), which updates its 2 cells of the colour from 16-byte loads of the row, its right-hand
 // side and its 4 x/y neighbour rows (across a face, the neighbour leaf's row; a missing leaf adds
@@ -646,6 +811,81 @@ void smooth_level(Context& c, const int4* nb8, float* u, const float* b, int ite
                            check, tol2);
         }
 }
+
+// The coarsest level's `sweeps` SOR sweeps from u = 0 (level 3, one cell per leaf): one cluster
+// launch where the option allows it, the leaves fit the cluster's shared memory and the device
+// can schedule the cluster, else two launches per sweep. Both give the same values.
+void coarsest_solve(Context& c, const int4* nb8, float* u, const float* b, int sweeps, float omega,
+                    const double* check, double tol2) {
+    const int64_t L = c.topo.num_leaves;
+    const float h2 = 64.0f, gamma = 7.0f / 9.0f;  // level 3: (2^3)^2, (2^3 - 1) / (2^3 + 1)
+    auto per_cta = [&](int ctas) { return (L + ctas - 1) / ctas; };
+    auto smem_of = [&](int ctas) { return (size_t)per_cta(ctas) * kCoarseCellBytes + 4; };
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[2];
+    auto configure = [&](int ctas) {
+        cfg.gridDim = dim3(ctas);
+        cfg.blockDim = dim3(kCoarseThreads);
+        cfg.dynamicSmemBytes = smem_of(ctas);
+        cfg.stream = c.stream;
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    };
+    bool fresh = false;
+    if (c.coarse_solve == HNS_COARSE_CLUSTER && sweeps >= 1 && c.coarse_cluster_ok != 0 &&
+        (c.coarse_cluster_ok < 0 || c.coarse_table_leaves != L)) {
+        // The cluster size: the larger of 16 and 8 that holds the level and that the device schedules.
+        c.coarse_cluster_ok = 0;
+        int optin = 0;
+        HNS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c.device));
+        HNS_CUDA(cudaFuncSetAttribute(coarsest_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+        for (int ctas : {16, 8}) {
+            if (smem_of(ctas) + 16 > (size_t)optin) continue;  // + the kernel's static shared memory
+            HNS_CUDA(cudaFuncSetAttribute(coarsest_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem_of(ctas)));
+            configure(ctas);
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, coarsest_cluster_kernel, &cfg) != cudaSuccess) {
+                (void)cudaGetLastError();  // not schedulable at this size: try the next
+                continue;
+            }
+            if (clusters >= 1) {
+                c.coarse_cluster_ok = ctas;
+                break;
+            }
+        }
+        if (c.coarse_cluster_ok > 0) {
+            const int ctas = c.coarse_cluster_ok;
+            auto* table = reinterpret_cast<uint4*>(c.scratch_f32("mg16_coarse_records", (size_t)8 * L + 8 * ctas));
+            auto* counts = reinterpret_cast<int*>(c.scratch_f32("mg16_coarse_counts", 2 * 16));
+            coarse_table_kernel<<<ctas, kCoarseThreads, 0, c.stream>>>(c.topo.view, nb8, table, counts,
+                                                                       (int)per_cta(ctas), gamma);
+            HNS_LAUNCHED();
+            c.coarse_table_leaves = L;
+            fresh = true;
+        }
+    }
+    if (c.coarse_solve != HNS_COARSE_CLUSTER || sweeps < 1 || c.coarse_cluster_ok <= 0) {
+        smooth_level<0>(c, nb8, u, b, sweeps, omega, 3, true, check, tol2);
+        return;
+    }
+    const int ctas = c.coarse_cluster_ok;
+    configure(ctas);
+    // The kernel reads its records before griddepcontrol.wait: after a table made in this call,
+    // an ordinary launch.
+    cfg.numAttrs = fresh ? 1 : 2;
+    const auto* table = reinterpret_cast<const uint4*>(c.scratch_f32("mg16_coarse_records", (size_t)8 * L + 8 * ctas));
+    const auto* counts = reinterpret_cast<const int*>(c.scratch_f32("mg16_coarse_counts", 2 * 16));
+    HNS_CUDA(cudaLaunchKernelEx(&cfg, coarsest_cluster_kernel, table, counts, u, b, (int)L, (int)per_cta(ctas), sweeps,
+                                omega, h2, check, tol2));
+    HNS_LAUNCHED();
+}
 }  // namespace
 
 void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_zero, const double* check, double tol2) {
@@ -679,7 +919,7 @@ void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_z
     int coarse_sweeps;
     float coarse_omega;
     coarsest_schedule(c, coarse_sweeps, coarse_omega);
-    smooth_level<0>(c, f8, u[3], b[3], coarse_sweeps, coarse_omega, 3, true, check, tol2);
+    coarsest_solve(c, f8, u[3], b[3], coarse_sweeps, coarse_omega, check, tol2);
     launch_pdl(c, mgl_prolong_kernel<1>, L, t, (const float*)u[3], u[2], check, tol2);
     smooth_level<1>(c, f8, u[2], b[2], kMgNu, 1.0f, 2, false, check, tol2);
     launch_pdl(c, mgl_prolong_kernel<2>, L << 3, t, (const float*)u[2], u[1], check, tol2);

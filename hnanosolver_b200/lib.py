@@ -26,6 +26,8 @@ INNER_ROWS, INNER_PACKED, INNER_SPLIT = 0, 1, 2
 OPT_WAIT_POLLS = 3
 OPT_SPLIT_SOLVE = 4
 SPLIT_PER_COLOUR, SPLIT_PERSISTENT = 0, 1
+OPT_COARSE_SOLVE = 5
+COARSE_LAUNCHES, COARSE_CLUSTER = 0, 1
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 

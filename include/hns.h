@@ -503,6 +503,14 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
                                      between convergence checks, leaf groups ordered by per-group
                                      progress counters instead of launch boundaries. Both give the
                                      same results to the bit. */
+#define HNS_OPT_COARSE_SOLVE 5  /* how the FP16 multigrid cycle (HNS_SOLVE_MULTIGRID) solves its coarsest
+                                     level, one cell per leaf: */
+#define HNS_COARSE_LAUNCHES 0   /*   two launches per SOR sweep */
+#define HNS_COARSE_CLUSTER 1    /*   all sweeps in one launch of a 16-CTA thread-block cluster (8 where
+                                     the device cannot schedule 16) that holds the level in shared
+                                     memory (default; up to 5,810 leaves per CTA, 92,960 in all with 16;
+                                     larger domains take HNS_COARSE_LAUNCHES). Both give the same
+                                     results to the bit. */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */
