@@ -192,6 +192,14 @@ float* Context::scratch_f32(const std::string& name, size_t count) {
     return b.as<float>();
 }
 
+void Context::release_spare_graphs() {
+    for (auto& g : spare_graphs) {
+        if (g.exec) (void)cudaGraphExecDestroy(g.exec);
+        if (g.graph) (void)cudaGraphDestroy(g.graph);
+    }
+    spare_graphs.clear();
+}
+
 double* Context::reduce_slots(int count) {
     if (count > kReduceSlots) fail(HNS_ERR_UNSUPPORTED, "more than " + std::to_string(kMaxChecks) + " convergence checks");
     if (!d_reduce.ptr) d_reduce.alloc(sizeof(double) * kReduceSlots);
@@ -390,6 +398,7 @@ HNS_API hns_status hns_destroy(hns_ctx* ctx) {
         if (c.refine_echo_done) (void)cudaEventDestroy(c.refine_echo_done);
         if (c.refine_echo) (void)cudaFreeHost(c.refine_echo);
         c.release_staging();
+        c.release_spare_graphs();
         for (auto& e : c.phase_events) {
             (void)cudaEventDestroy(e.start);
             (void)cudaEventDestroy(e.stop);

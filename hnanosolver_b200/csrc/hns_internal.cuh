@@ -179,6 +179,18 @@ struct Context {
     int coarse_solve = HNS_COARSE_CLUSTER;   // hns_set_option(HNS_OPT_COARSE_SOLVE)
     int coarse_cluster_ok = -1;     // CTAs of the coarsest level's cluster, 0 if none fits (-1: not chosen)
     int64_t coarse_table_leaves = -1;  // leaves of the coarsest level's cluster records made so far
+    // Graphs of the multigrid refinement's outer iterations past the forecast (hns_mixed.cu): a
+    // device-side condition runs the iteration only while the solve has not converged. Made on
+    // first use per set of arguments; 0 in spare_graph_ok after one could not be made (those
+    // iterations then launch as the others do).
+    struct SpareGraph {
+        std::vector<uintptr_t> key;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::vector<SpareGraph> spare_graphs;
+    int spare_graph_ok = -1;
+    void release_spare_graphs();
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;

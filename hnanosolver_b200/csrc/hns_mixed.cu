@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <functional>
 #include <string>
 #include <vector>
@@ -595,6 +596,84 @@ bool capturing(const Context& c) {
     return st != cudaStreamCaptureStatusNone;
 }
 
+// Condition of a spare outer iteration's graph: 1 while the refinement has not converged (the
+// test every kernel of the iteration makes before it does anything).
+__global__ void spare_gate_kernel(cudaGraphConditionalHandle h, const double* __restrict__ check, double tol2) {
+    cudaGraphSetConditional(h, check[0] <= tol2 * check[1] ? 0u : 1u);
+}
+
+// Runs `body` (the launches of one outer iteration whose kernels return at once after
+// convergence) on the stream as a graph whose conditional node skips it on the device after
+// convergence: one gate kernel and a graph launch in place of the iteration's launches. The
+// graph is made on the first call with this key (body captured once) and relaunched after.
+// Returns false, with nothing enqueued, where a graph cannot be made.
+bool run_spare_graph(Context& c, const std::vector<uintptr_t>& key, const double* check, double tol2,
+                     const std::function<void()>& body) {
+    if (c.spare_graph_ok == 0) return false;
+    Context::SpareGraph* found = nullptr;
+    for (auto& g : c.spare_graphs)
+        if (g.key == key) found = &g;
+    if (found == nullptr) {
+        if (c.spare_graphs.size() >= 16) c.release_spare_graphs();
+        Context::SpareGraph sg;
+        sg.key = key;
+        bool ok = cudaGraphCreate(&sg.graph, 0) == cudaSuccess;
+        cudaGraphConditionalHandle h = 0;
+        cudaGraph_t body_graph = nullptr;
+        cudaGraphNode_t gate = nullptr, cond = nullptr;
+        if (ok) ok = cudaGraphConditionalHandleCreate(&h, sg.graph, 0, 0) == cudaSuccess;
+        if (ok) {
+            cudaKernelNodeParams kp = {};
+            void* args[] = {&h, &check, &tol2};
+            kp.func = reinterpret_cast<void*>(spare_gate_kernel);
+            kp.gridDim = dim3(1);
+            kp.blockDim = dim3(1);
+            kp.kernelParams = args;
+            ok = cudaGraphAddKernelNode(&gate, sg.graph, nullptr, 0, &kp) == cudaSuccess;
+        }
+        if (ok) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeIf;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&cond, sg.graph, &gate, 1, &cp) == cudaSuccess;
+            if (ok) body_graph = cp.conditional.phGraph_out[0];
+        }
+        if (ok) {
+            // The body's launches are captured, not run; no phase events inside the graph.
+            const bool prof = c.profiling;
+            c.profiling = false;
+            ok = cudaStreamBeginCaptureToGraph(c.stream, body_graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+                 cudaSuccess;
+            if (ok) {
+                try {
+                    body();
+                } catch (const Error&) {
+                    ok = false;
+                }
+                cudaGraph_t out = nullptr;
+                if (cudaStreamEndCapture(c.stream, &out) != cudaSuccess) ok = false;
+            }
+            c.profiling = prof;
+        }
+        if (ok) ok = cudaGraphInstantiate(&sg.exec, sg.graph, 0) == cudaSuccess;
+        if (!ok) {
+            (void)cudaGetLastError();
+            if (sg.exec) (void)cudaGraphExecDestroy(sg.exec);
+            if (sg.graph) (void)cudaGraphDestroy(sg.graph);
+            c.spare_graph_ok = 0;
+            return false;
+        }
+        c.spare_graph_ok = 1;
+        c.spare_graphs.push_back(sg);
+        found = &c.spare_graphs.back();
+    }
+    HNS_CUDA(cudaGraphLaunch(found->exec, c.stream));
+    HNS_LAUNCHED();  // the gate kernel
+    return true;
+}
+
 // Grid of the grid-stride passes: four values per thread, at most 32 CTAs per SM.
 unsigned stream_blocks(const Context& c, int64_t n) {
     const int64_t b = (n + kThreads * 4 - 1) / (kThreads * 4);
@@ -730,14 +809,46 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
     // refinement has converged they return at once for the cost of the launch alone.
     const bool echo = !capturing(c);
     const int forecast = echo ? refine_forecast(c) : 0;
+    // Multigrid on the FP16 colour-split layout: `inner` V-cycles per outer iteration, the
+    // colour-split half-sweep as the fine smoother (mg16_vcycle); other layouts and the FP32
+    // inner solve take the FP32 V-cycle in slot order below.
+    const bool mg16 = (flags & HNS_SOLVE_MULTIGRID) && sizeof(TI) == 2 && layout == HNS_INNER_SPLIT;
+    auto mg16_iteration = [&](int k, unsigned gk) {
+        const double* chk = plan.slots + 2 * k;
+        refine_scale_split_kernel<<<gk, kThreads, 0, c.stream>>>(r, reinterpret_cast<__half*>(rhat), n, chk, tol2,
+                                                                 scales + k);
+        HNS_LAUNCHED();
+        c.phase_begin(HNS_PHASE_INNER);
+        for (int cyc = 0; cyc < plan.inner; ++cyc) mg16_vcycle(c, nb8, rhat, e_split, cyc == 0, chk, tol2);
+        c.phase_end();
+        refine_update_split_kernel<<<gk, kThreads, 0, c.stream>>>(p, reinterpret_cast<const __half*>(e_split), n,
+                                                                  scales + k, chk, tol2, k == 0);
+        HNS_LAUNCHED();
+        refine_residual_kernel<<<residual_blocks(c), kThreads, 0, c.stream>>>(c.topo.view, div, p, r, h2, chk, tol2,
+                                                                             plan.slots + 2 * (k + 1));
+        HNS_LAUNCHED();
+    };
     for (int k = 0; k < plan.max_outer; ++k) {
         const double* chk = plan.slots + 2 * k;
         const bool spare = forecast > 0 && k >= forecast;
         const unsigned gk = spare ? std::min(g, (unsigned)(c.sm_count() * 4)) : g;
-        // Multigrid on the FP16 colour-split layout: `inner` V-cycles per outer iteration, the
-        // colour-split half-sweep as the fine smoother (mg16_vcycle); other layouts and the FP32
-        // inner solve take the FP32 V-cycle in slot order below.
-        const bool mg16 = (flags & HNS_SOLVE_MULTIGRID) && sizeof(TI) == 2 && layout == HNS_INNER_SPLIT;
+        if (mg16) {
+            // Past the forecast, the iteration most likely finds the solve converged: as a graph
+            // whose device-side condition skips it then (one gate kernel in place of about 100
+            // returning launches), else launched as the others.
+            if (spare) {
+                uint64_t tol_bits = 0;
+                std::memcpy(&tol_bits, &tol2, sizeof tol_bits);
+                const std::vector<uintptr_t> key = {
+                    (uintptr_t)k, (uintptr_t)gk, (uintptr_t)plan.inner, (uintptr_t)p, (uintptr_t)div, (uintptr_t)r,
+                    (uintptr_t)rhat, (uintptr_t)e_split, (uintptr_t)nb8, (uintptr_t)plan.slots, (uintptr_t)n,
+                    (uintptr_t)c.coarse_solve, (uintptr_t)c.coarse_cluster_ok, (uintptr_t)c.split_solve,
+                    (uintptr_t)c.first_wait_polls, (uintptr_t)tol_bits};
+                if (run_spare_graph(c, key, chk, tol2, [&] { mg16_iteration(k, gk); })) continue;
+            }
+            mg16_iteration(k, gk);
+            continue;
+        }
         if ((flags & HNS_SOLVE_MULTIGRID) && !mg16) {
             // One V-cycle on the scaled residual in FP32 (slot order), then p += s e.
             float* rm = c.scratch_f32("mg_rhat", (size_t)n);
@@ -773,11 +884,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         // The persistent form: the whole inner solve in one launch. An outer iteration past the
         // forecast takes it whatever the option: it most likely returns at once, and one launch
         // then costs a few microseconds where 2 * inner returning half-sweeps cost 2.3 us each.
-        const bool persistent = !mg16 && layout == HNS_INNER_SPLIT && (c.split_solve == HNS_SPLIT_PERSISTENT || spare);
-        if (mg16) {
-            for (int cyc = 0; cyc < plan.inner; ++cyc) mg16_vcycle(c, nb8, rhat, e_split, cyc == 0, chk, tol2);
-            src = e_split;
-        } else if (persistent) {
+        const bool persistent = layout == HNS_INNER_SPLIT && (c.split_solve == HNS_SPLIT_PERSISTENT || spare);
+        if (persistent) {
             if constexpr (sizeof(TI) == 2)
                 launch_rbgs_split_solve(c, nb8, rhat, e_split, 2 * plan.inner, true, omega, chk, tol2);
             else
@@ -785,7 +893,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                                             2 * plan.inner, true, omega, 1.0f, chk, tol2);
             src = e_split;
         }
-        for (int it = 0; it < (persistent || mg16 ? 0 : plan.inner); ++it) {
+        for (int it = 0; it < (persistent ? 0 : plan.inner); ++it) {
             TI* dst = e[it & 1];
             if constexpr (sizeof(TI) == 2) {
                 if (layout == HNS_INNER_SPLIT) {

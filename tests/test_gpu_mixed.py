@@ -53,13 +53,13 @@ def test_conversions_round_to_nearest(dev, shell):
     g.close()
 
 
-def _mixed(g, dev, dens, vel, tol=1e-5, inner=40, outer=8):
+def _mixed(g, dev, dens, vel, tol=1e-5, inner=40, outer=8, flags=0):
     from hnanosolver_b200 import lib as hl
 
     vb = torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous()
     dh = torch.from_numpy(dens).to(dev).to(torch.float16).contiguous()
     vo, do = torch.empty_like(vb), torch.empty_like(dh)
-    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=tol, max_outer=outer, inner_iterations=inner, flags=0)
+    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=tol, max_outer=outer, inner_iterations=inner, flags=flags)
     torch.cuda.synchronize()  # uploads on torch's stream finish before the library's stream reads them
     info = g.step_mixed(vb, vo, [dh], [do], desc, info=True)
     return vb, dh, vo, do, info
@@ -302,18 +302,22 @@ def test_inner_solve_layouts_bit_exact(dev, shell, grid):
         assert b[4] <= 1e-5
 
 
-def test_outer_forecast_short_grids_bit_exact(dev, shell):
+@pytest.mark.parametrize("inner_solve", ["red-black", "multigrid"])
+def test_outer_forecast_short_grids_bit_exact(dev, shell, inner_solve):
     """A context forecasts the refinement's outer iterations from the checks of its earlier
     solves; the outer iterations past the forecast run their kernels on short grids (one wave,
-    looping over the leaves). Whether those iterations find the solve converged (a forecast at
-    or above the need) or still have work (a forecast below it), the step is the same to the bit
-    as on a fresh context, which has no forecast."""
+    looping over the leaves), and under multigrid each runs as a graph whose device-side
+    condition skips it after convergence. Whether those iterations find the solve converged (a
+    forecast at or above the need) or still have work (a forecast below it), the step is the
+    same to the bit as on a fresh context, which has no forecast."""
     from hnanosolver_b200 import lib as hl
 
     origins, dens, vel = shell
+    mg = inner_solve == "multigrid"
 
     def solve(g, tol):
-        vb, dh, vo, do, info = _mixed(g, dev, dens, vel, tol=tol, inner=30, outer=12)
+        vb, dh, vo, do, info = _mixed(g, dev, dens, vel, tol=tol, inner=2 if mg else 30, outer=12,
+                                      flags=hl.SOLVE_MULTIGRID if mg else 0)
         p = torch.empty(g.num_voxels, dtype=torch.float64, device=dev)
         outer, res = g.refine_pressure(p)
         torch.cuda.synchronize()
