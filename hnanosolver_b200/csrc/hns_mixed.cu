@@ -841,7 +841,8 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
                 std::memcpy(&tol_bits, &tol2, sizeof tol_bits);
                 const std::vector<uintptr_t> key = {
                     (uintptr_t)k, (uintptr_t)gk, (uintptr_t)plan.inner, (uintptr_t)p, (uintptr_t)div, (uintptr_t)r,
-                    (uintptr_t)rhat, (uintptr_t)e_split, (uintptr_t)nb8, (uintptr_t)plan.slots, (uintptr_t)n,
+                    (uintptr_t)rhat, (uintptr_t)e_split, (uintptr_t)nb8, (uintptr_t)plan.slots, (uintptr_t)scales,
+                    (uintptr_t)plan.max_outer, (uintptr_t)n,
                     (uintptr_t)c.coarse_solve, (uintptr_t)c.coarse_cluster_ok, (uintptr_t)c.split_solve,
                     (uintptr_t)c.first_wait_polls, (uintptr_t)tol_bits};
                 if (run_spare_graph(c, key, chk, tol2, [&] { mg16_iteration(k, gk); })) continue;
