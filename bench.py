@@ -105,6 +105,7 @@ def apply_options(g, hl, args):
     g.set_option(hl.OPT_SPLIT_SOLVE, hl.SPLIT_PERSISTENT if form == "persistent" else hl.SPLIT_PER_COLOUR)
     coarse = getattr(args, "coarse_solve", "cluster")
     g.set_option(hl.OPT_COARSE_SOLVE, hl.COARSE_CLUSTER if coarse == "cluster" else hl.COARSE_LAUNCHES)
+    g.set_option(hl.OPT_L2_PERSIST, 0 if getattr(args, "no_l2_persist", False) else 1)
 
 
 def profiled_traffic(workload: str, kind: str):
@@ -663,7 +664,7 @@ def ours(args, wl):
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
         cfg = workload_config(args, wl, origins)
-        det = {"precision": args.precision, "split_solve": args.split_solve, "coarse_solve": args.coarse_solve, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+        det = {"precision": args.precision, "split_solve": args.split_solve, "coarse_solve": args.coarse_solve, "l2_persist": not args.no_l2_persist, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
                "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 else None,
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
@@ -1078,7 +1079,7 @@ def ours_fire(args, wl):
 
     if rank == 0:
         phase_ms = {k: prof.phase_ms[i] / args.steps for k, i in hl.PHASES.items() if prof.phase_count[i]}
-        det = {"precision": args.precision, "split_solve": args.split_solve, "coarse_solve": args.coarse_solve, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+        det = {"precision": args.precision, "split_solve": args.split_solve, "coarse_solve": args.coarse_solve, "l2_persist": not args.no_l2_persist, "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
                "phase_ms_per_step": phase_ms, "fp32_forms_same_run": fp32,
                "mixed_vs_fp32_plain": (value / world) / fp32["plain"]["value"] if fp32 and "value" in fp32["plain"] else None,
                "mixed_vs_fp32_refined": (value / world) / fp32["refined"]["value"] if fp32 else None,
@@ -1280,6 +1281,9 @@ def main():
     ap.add_argument("--coarse-solve", choices=["cluster", "launches"], default="cluster",
                     help="the multigrid cycle's coarsest level: one thread-block cluster launch or two "
                          "launches per SOR sweep (same results to the bit)")
+    ap.add_argument("--no-l2-persist", action="store_true",
+                    help="ordinary caching for the FP16 inner solve's correction array (HNS_OPT_L2_PERSIST 0; "
+                         "by default it persists in L2 where it fits)")
     ap.add_argument("--no-fp32-comparison", action="store_true",
                     help="skip the FP32 forms measured beside the mixed one (profiling runs)")
     args = ap.parse_args()

@@ -449,6 +449,9 @@ HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value) {
             if (value != HNS_COARSE_LAUNCHES && value != HNS_COARSE_CLUSTER)
                 fail(HNS_ERR_INVALID_ARG, "unknown coarse-level solve");
             c->coarse_solve = value;
+        } else if (option == HNS_OPT_L2_PERSIST) {
+            if (value != 0 && value != 1) fail(HNS_ERR_INVALID_ARG, "HNS_OPT_L2_PERSIST takes 0 or 1");
+            c->l2_persist = value;
         } else if (option == HNS_OPT_WAIT_POLLS) {
             if (value < -1) fail(HNS_ERR_INVALID_ARG, "the wait limit must be -1 (default) or >= 0");
             c->first_wait_polls = value;

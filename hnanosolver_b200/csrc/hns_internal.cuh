@@ -177,6 +177,17 @@ struct Context {
     int first_wait_polls = -1;           // hns_set_option(HNS_OPT_WAIT_POLLS); -1: the kernel's default
     int split_solve = HNS_SPLIT_PER_COLOUR;  // hns_set_option(HNS_OPT_SPLIT_SOLVE)
     int coarse_solve = HNS_COARSE_CLUSTER;   // hns_set_option(HNS_OPT_COARSE_SOLVE)
+    int l2_persist = 1;                      // hns_set_option(HNS_OPT_L2_PERSIST)
+    // The access-policy window of the inner solve's launches while a refined solve runs
+    // (num_bytes 0: none); added to their launch attributes by add_inner_window().
+    cudaAccessPolicyWindow inner_window = {};
+    size_t l2_persist_limit = 0;  // the persisting-L2 limit this context has set
+    unsigned add_inner_window(cudaLaunchAttribute* attr, unsigned n) const {
+        if (inner_window.num_bytes == 0) return n;
+        attr[n].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[n].val.accessPolicyWindow = inner_window;
+        return n + 1;
+    }
     int coarse_cluster_ok = -1;     // CTAs of the coarsest level's cluster, 0 if none fits (-1: not chosen)
     int64_t coarse_table_leaves = -1;  // leaves of the coarsest level's cluster records made so far
     // Graphs of the multigrid refinement's outer iterations past the forecast (hns_mixed.cu): a

@@ -783,11 +783,11 @@ void launch_pdl(const Context& c, void (*kern)(KArgs...), int64_t threads, Args.
     cfg.gridDim = dim3(blocks(threads));
     cfg.blockDim = dim3(kThreads);
     cfg.stream = c.stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = c.add_inner_window(attr, 1);
     HNS_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
     HNS_LAUNCHED();
 }

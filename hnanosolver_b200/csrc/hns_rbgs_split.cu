@@ -617,9 +617,11 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = c.stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     unsigned na = 0;
     if (e_zero) {
+        cfg.numAttrs = c.add_inner_window(attr, 0);
+        cfg.attrs = attr;
         HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<true>, nb8, r, x, (int)L, colour, omega, check, tol2,
                                     c.counters));
         HNS_LAUNCHED();
@@ -632,6 +634,7 @@ void launch_rbgs_split_half(const Context& c, const int* nb8, const void* rhs, v
     attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[na].val.programmaticStreamSerializationAllowed = 1;
     ++na;
+    na = c.add_inner_window(attr, na);
     cfg.attrs = attr;
     cfg.numAttrs = na;
     HNS_CUDA(cudaLaunchKernelEx(&cfg, rbgs_split_half_kernel<false>, nb8, r, x, (int)L, colour, omega, check, tol2,

@@ -28,6 +28,7 @@ OPT_SPLIT_SOLVE = 4
 SPLIT_PER_COLOUR, SPLIT_PERSISTENT = 0, 1
 OPT_COARSE_SOLVE = 5
 COARSE_LAUNCHES, COARSE_CLUSTER = 0, 1
+OPT_L2_PERSIST = 6
 SOLVE_ZERO_INIT = 1
 SOLVE_NEUMANN = 2
 

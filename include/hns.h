@@ -511,6 +511,12 @@ HNS_API hns_status hns_adjoint_advance_mixed(hns_ctx* ctx, const hns_fire_fields
                                      memory (default; up to 5,810 leaves per CTA, 92,960 in all with 16;
                                      larger domains take HNS_COARSE_LAUNCHES). Both give the same
                                      results to the bit. */
+#define HNS_OPT_L2_PERSIST 6    /* 1 (default): where the FP16 inner solve's correction array fits the
+                                     device's persisting-L2 maximum (79 MB on a B200: grids up to about
+                                     41M voxels), it is marked persisting in L2 while a refined solve
+                                     runs (an access-policy window on the inner solve's launches; the
+                                     process's persisting-L2 limit is raised to hold it, once per
+                                     context); 0: ordinary caching. The results are the same to the bit. */
 HNS_API hns_status hns_set_option(hns_ctx* ctx, int option, int value);
 /* Device-side error flags raised since the last call (bounded waits that gave up): returns
  * HNS_ERR_TIMEOUT and clears them if any was raised, else HNS_OK. Synchronizes. */

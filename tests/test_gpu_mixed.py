@@ -428,3 +428,27 @@ def test_multigrid_coarse_cluster_bit_exact(dev, grid):
     assert torch.equal(a[2], b[2])
     assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
     assert b[4] <= 1e-5
+
+
+@pytest.mark.parametrize("flags", [0, 8])
+def test_l2_persistence_same_results(dev, shell, flags):
+    """HNS_OPT_L2_PERSIST (the inner solve's FP16 correction array marked persisting in L2 for
+    the solve's launches; the default where it fits) changes caching only: the mixed step with
+    red-black (flags 0) or multigrid (HNS_SOLVE_MULTIGRID = 8) inner solves gives the same
+    pressure, outer count, velocity and density to the bit as with ordinary caching."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    out = {}
+    for persist in (0, 1):
+        g = hl.Grid(origins, voxel_size=0.1)
+        g.set_option(hl.OPT_L2_PERSIST, persist)
+        vb, dh, vo, do, info = _mixed(g, dev, dens, vel, inner=2 if flags else 30, outer=12, flags=flags)
+        p = torch.empty(g.num_voxels, dtype=torch.float64, device=dev)
+        outer, res = g.refine_pressure(p)
+        torch.cuda.synchronize()
+        out[persist] = (vo.cpu(), do.cpu(), p.cpu(), outer)
+        g.close()
+    a, b = out[0], out[1]
+    assert a[3] == b[3]
+    assert torch.equal(a[2], b[2]) and torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
