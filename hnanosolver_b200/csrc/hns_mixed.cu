@@ -807,7 +807,10 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         HNS_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c.device));
         const size_t bytes = (size_t)n * sizeof(TI);
         const size_t persist = bytes;
-        if (bytes > 0 && bytes <= (size_t)std::max(0, max_window) && bytes <= (size_t)std::max(0, max_persist)) {
+        // Not while the caller captures the stream before this context has raised the limit (a
+        // device-wide call inside a capture).
+        if (bytes > 0 && bytes <= (size_t)std::max(0, max_window) && bytes <= (size_t)std::max(0, max_persist) &&
+            (c.l2_persist_limit >= persist || !capturing(c))) {
             if (c.l2_persist_limit < persist) {
                 HNS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
                 c.l2_persist_limit = persist;

@@ -452,3 +452,35 @@ def test_l2_persistence_same_results(dev, shell, flags):
     a, b = out[0], out[1]
     assert a[3] == b[3]
     assert torch.equal(a[2], b[2]) and torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+
+
+def test_multigrid_step_captured_in_a_graph(dev, shell):
+    """The multigrid mixed step enqueued into a caller's CUDA graph capture (the cluster launch
+    of the coarsest level, the L2 window and the PDL chain captured; no forecast and no spare
+    graphs under capture) and replayed gives the eager step's velocity and density to the bit."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    g = hl.Grid(origins, voxel_size=0.1)
+    s = torch.cuda.Stream()
+    g.set_stream(s.cuda_stream)
+    vb = torch.from_numpy(vel).to(dev).to(torch.bfloat16).contiguous()
+    dh = torch.from_numpy(dens).to(dev).to(torch.float16).contiguous()
+    vo, do = torch.empty_like(vb), torch.empty_like(dh)
+    desc = hl.MixedDesc(dt=0.1, omega=1.9, tolerance=1e-5, max_outer=8, inner_iterations=2,
+                        flags=hl.SOLVE_MULTIGRID)
+    torch.cuda.synchronize()
+    g.step_mixed(vb, vo, [dh], [do], desc)  # eager: scratch, tables and limits made here
+    s.synchronize()
+    want_v, want_d = vo.clone(), do.clone()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s, capture_error_mode="relaxed"):
+        g.step_mixed(vb, vo, [dh], [do], desc)
+    vo.zero_()
+    do.zero_()
+    torch.cuda.synchronize()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(vo, want_v) and torch.equal(do, want_d)
+    del graph
+    g.close()
