@@ -864,7 +864,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         const unsigned gk = spare ? std::min(g, (unsigned)(c.sm_count() * 4)) : g;
         if (mg16) {
             // Past the forecast, the iteration most likely finds the solve converged: as a graph
-            // whose device-side condition skips it then (one gate kernel in place of about 100
+            // whose device-side condition skips it then (one gate kernel in place of 65 or more
             // returning launches), else launched as the others.
             if (spare) {
                 uint64_t tol_bits = 0;
