@@ -310,6 +310,10 @@ void mg_vcycle(Context& c, const float* b0, float* u0, const double* check, doub
 // How many leaves deep the domain is: the largest face-step distance from a leaf to one with a
 // missing face neighbour (host, once per context).
 int max_leaf_depth(Context& c);
+// Process-wide settings of a device that several contexts share, only ever raised so that no
+// context lowers another's: `which` 0 is the coarsest-level cluster kernel's dynamic shared
+// memory limit, 1 the persisting-L2 limit. Returns the value now in force (>= value).
+size_t raise_device_setting(int device, int which, size_t value);
 // One V-cycle of the FP16 inner solve on the colour-split layout (e in place; e_zero: e = 0 before).
 void mg16_vcycle(Context& c, const int* nb8, const void* rhat, void* e, bool e_zero, const double* check, double tol2);
 // The FP16 inner solve on colour-split leaves (hns_rbgs_split.cu): the face-neighbour table

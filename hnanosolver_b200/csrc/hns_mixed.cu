@@ -811,10 +811,7 @@ RefinePlan refine_solve(Context& c, const float* div, double* p, int max_outer, 
         // device-wide call inside a capture).
         if (bytes > 0 && bytes <= (size_t)std::max(0, max_window) && bytes <= (size_t)std::max(0, max_persist) &&
             (c.l2_persist_limit >= persist || !capturing(c))) {
-            if (c.l2_persist_limit < persist) {
-                HNS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
-                c.l2_persist_limit = persist;
-            }
+            if (c.l2_persist_limit < persist) c.l2_persist_limit = raise_device_setting(c.device, 1, persist);
             c.inner_window.base_ptr = e_split;
             c.inner_window.num_bytes = bytes;
             c.inner_window.hitRatio = 1.0f;

@@ -20,7 +20,10 @@
 
 #include <cmath>
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <string>
+#include <utility>
 
 #include "hns_internal.cuh"
 
@@ -812,6 +815,24 @@ void smooth_level(Context& c, const int4* nb8, float* u, const float* b, int ite
         }
 }
 
+}  // namespace
+
+// Settings shared by the contexts of a process on one device (raise_device_setting).
+size_t raise_device_setting(int device, int which, size_t value) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, size_t> in_force;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = in_force[{device, which}];
+    if (value <= cur) return cur;
+    if (which == 0)
+        HNS_CUDA(cudaFuncSetAttribute(coarsest_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)value));
+    else
+        HNS_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, value));
+    cur = value;
+    return cur;
+}
+
+namespace {
 // The coarsest level's `sweeps` SOR sweeps from u = 0 (level 3, one cell per leaf): one cluster
 // launch where the option allows it, the leaves fit the cluster's shared memory and the device
 // can schedule the cluster, else two launches per sweep. Both give the same values.
@@ -847,8 +868,7 @@ void coarsest_solve(Context& c, const int4* nb8, float* u, const float* b, int s
         HNS_CUDA(cudaFuncSetAttribute(coarsest_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
         for (int ctas : {16, 8}) {
             if (smem_of(ctas) + 16 > (size_t)optin) continue;  // + the kernel's static shared memory
-            HNS_CUDA(cudaFuncSetAttribute(coarsest_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem_of(ctas)));
+            raise_device_setting(c.device, 0, smem_of(ctas));
             configure(ctas);
             int clusters = 0;
             if (cudaOccupancyMaxActiveClusters(&clusters, coarsest_cluster_kernel, &cfg) != cudaSuccess) {

@@ -484,3 +484,25 @@ def test_multigrid_step_captured_in_a_graph(dev, shell):
     assert torch.equal(vo, want_v) and torch.equal(do, want_d)
     del graph
     g.close()
+
+
+def test_two_live_grids_of_different_sizes(dev, shell):
+    """Two contexts of different leaf counts on one device, stepped alternately with multigrid
+    inner solves: the cluster kernel's shared-memory limit and the persisting-L2 limit are
+    process-wide settings that a context only raises, so the smaller grid set up second does not
+    break the larger one's next step, which repeats its first to the bit."""
+    from hnanosolver_b200 import lib as hl
+
+    origins, dens, vel = shell
+    small = synth.topology("box64")
+    sd, sv = synth.noise_fields(small, seed=3)
+    big_g = hl.Grid(origins, voxel_size=0.1)
+    small_g = hl.Grid(small, voxel_size=0.1)
+    first = _mixed(big_g, dev, dens, vel, inner=2, outer=12, flags=hl.SOLVE_MULTIGRID)
+    torch.cuda.synchronize()
+    _mixed(small_g, dev, sd, sv, inner=2, outer=12, flags=hl.SOLVE_MULTIGRID)
+    again = _mixed(big_g, dev, dens, vel, inner=2, outer=12, flags=hl.SOLVE_MULTIGRID)
+    torch.cuda.synchronize()
+    assert torch.equal(first[2], again[2]) and torch.equal(first[3], again[3])
+    big_g.close()
+    small_g.close()
