@@ -64,3 +64,20 @@ def test_bad_voxel_size_is_rejected():
     with pytest.raises(hl.HnsError) as e:
         hl.Grid(np.zeros((1, 3), np.int32), voxel_size=0.0)
     assert e.value.status == 1
+
+
+def test_python_constants_mirror_the_header():
+    """Every option, option value and solve flag the header defines has the same value in the
+    Python binding (HNS_OPT_X -> OPT_X, HNS_SOLVE_X -> SOLVE_X, value names without the prefix)."""
+    src = open(os.path.join(ROOT, "include", "hns.h")).read()
+    defs = dict((m.group(1), int(m.group(2))) for m in
+                re.finditer(r"^#define HNS_((?:OPT|RBGS|INNER|SPLIT|COARSE|SOLVE)_\w+)\s+(\d+)u?\b", src, re.M))
+    assert "OPT_COARSE_SOLVE" in defs and "OPT_L2_PERSIST" in defs and "SOLVE_MULTIGRID" in defs
+    for name, value in defs.items():
+        assert getattr(hl, name) == value, name
+
+
+def test_set_option_without_a_context_is_rejected():
+    for opt in (hl.OPT_RBGS_KERNEL, hl.OPT_INNER_LAYOUT, hl.OPT_WAIT_POLLS, hl.OPT_SPLIT_SOLVE,
+                hl.OPT_COARSE_SOLVE, hl.OPT_L2_PERSIST):
+        assert hl.lib.hns_set_option(None, opt, 0) == 1
