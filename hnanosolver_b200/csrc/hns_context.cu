@@ -192,6 +192,12 @@ float* Context::scratch_f32(const std::string& name, size_t count) {
     return b.as<float>();
 }
 
+bool Context::stream_capturing() const {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    HNS_CUDA(cudaStreamIsCapturing(stream, &st));
+    return st != cudaStreamCaptureStatusNone;
+}
+
 void Context::release_spare_graphs() {
     for (auto& g : spare_graphs) {
         if (g.exec) (void)cudaGraphExecDestroy(g.exec);

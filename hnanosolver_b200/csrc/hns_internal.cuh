@@ -202,6 +202,9 @@ struct Context {
     std::vector<SpareGraph> spare_graphs;
     int spare_graph_ok = -1;
     void release_spare_graphs();
+    // Whether the context's stream is being captured into a graph (work enqueued now runs only
+    // when the graph does: a table built under capture is not marked built).
+    bool stream_capturing() const;
     struct PhaseEvent {
         int phase;
         cudaEvent_t start, stop;

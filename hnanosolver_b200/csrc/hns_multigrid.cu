@@ -887,7 +887,7 @@ void coarsest_solve(Context& c, const int4* nb8, float* u, const float* b, int s
             coarse_table_kernel<<<ctas, kCoarseThreads, 0, c.stream>>>(c.topo.view, nb8, table, counts,
                                                                        (int)per_cta(ctas), gamma);
             HNS_LAUNCHED();
-            c.coarse_table_leaves = L;
+            if (!c.stream_capturing()) c.coarse_table_leaves = L;
             fresh = true;
         }
     }

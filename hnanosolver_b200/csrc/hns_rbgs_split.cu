@@ -578,7 +578,7 @@ int* Context::split_faces() {
     int* nb8 = reinterpret_cast<int*>(scratch_f32("split_faces", (size_t)topo.num_leaves * 8));
     if (split_faces_built != nb8) {
         launch_split_face_table(*this, nb8);
-        split_faces_built = nb8;
+        if (!stream_capturing()) split_faces_built = nb8;
     }
     return nb8;
 }
@@ -588,7 +588,7 @@ void* Context::split_e(const char* name, size_t bytes, int which) {
     char* e = reinterpret_cast<char*>(scratch_f32(name, ((n + 512) * bytes + 3) / 4));
     if (split_zero_leaf[which] != e) {
         HNS_CUDA(cudaMemsetAsync(e + n * bytes, 0, 512 * bytes, stream));
-        split_zero_leaf[which] = e;
+        if (!stream_capturing()) split_zero_leaf[which] = e;
     }
     return e;
 }
